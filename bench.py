@@ -1,0 +1,370 @@
+#!/usr/bin/env python3
+"""Benchmark of the HPCG PCG path on B200.
+
+One step = one HPCG CG set (50 preconditioned CG iterations from x = 0, tolerance
+0, as the timed loop of src/main.cpp:334-340) on the 512^3 problem (134M rows,
+4 MG levels, 27-point stencil, FP64), generated on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line on rank 0. Under torchrun each rank (one per GPU) solves
+its own 512^3 problem; the path has no cross-problem exchange on one process
+per GPU, so N ranks are N replicas ("scaling": "weak") and the value is the
+summed work over the slowest rank's time.
+
+value: HPCG GFLOP/s (the reference FLOP model, src/ReportResults.cpp:75-99) with
+b and x resident in HBM. e2e: the same metric through the C ABI with pinned
+host b and x (uploaded, solved, x downloaded every step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "HPCG GFLOP/s & HBM GB/s at 512^3; FP32-MG vs FP64 time to 1e-9 residual"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=512, help="grid side (nx = ny = nz)")
+    ap.add_argument("--iters", type=int, default=50, help="CG iterations per set")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-n", type=int, default=128, help="grid side of the CPU reference sample")
+    ap.add_argument("--ref-seconds", type=float, default=20.0, help="CPU seconds budget of a reference sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference's own CG_ref, OpenMP build, in a subprocess)
+# ---------------------------------------------------------------------------
+
+def reference_timer_path():
+    return os.path.join(HERE, "oracle", "_ref", "hpcg_ref_timer")
+
+
+def run_reference_sample(n, iters, reps, warmup):
+    """Times the reference's CG_ref at n^3 (all host threads). Returns the timer's JSON."""
+    exe = reference_timer_path()
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    out = subprocess.run([exe, str(n), str(n), str(n), str(iters), str(reps), str(warmup)], env=env,
+                         capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference timer failed: {out.stderr[-500:]}")
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def reference_iters_for(n, seconds, reps):
+    """Iterations per call so that reps calls take about `seconds` on this host:
+    the reference runs ~1.5 GFLOP/s per core-bound MG at 128^3 (serial SYMGS)."""
+    from hpcg_b200 import metrics
+    per_iter = metrics.hpcg_flops(n, n, n, 1) - metrics.hpcg_flops(n, n, n, 0)
+    it = int(seconds * 1.5e9 / max(per_iter, 1.0) / max(reps, 1))
+    return max(1, min(50, it))
+
+
+def cpu_baseline(args):
+    exe = reference_timer_path()
+    if os.path.exists(exe):
+        iters = reference_iters_for(args.ref_n, args.ref_seconds, 1)
+        r = run_reference_sample(args.ref_n, iters, 1, 0)
+        return {"value": round(r["flops_per_call"] / r["mean_s"] / 1e9, 4), "unit": "GFLOP/s",
+                "cores": r["threads"], "kind": "reference",
+                "sample": f"CG_ref of the reference (OpenMP build, its own flags), {args.ref_n}^3, "
+                          f"{iters} iterations, 1 call ({r['mean_s']:.2f} s); the reference cannot "
+                          f"generate 512^3 (nnz overflows its int local_int_t)"}
+    # the C restatement (serial), when the reference was not built here
+    from oracle import oracle as O
+    from hpcg_b200 import metrics
+    n = min(args.ref_n, 64)
+    P = O.generate(n)
+    t0 = time.perf_counter()
+    O.cg(P.levels, P.b, P.x, 10, 0.0)
+    dt = time.perf_counter() - t0
+    return {"value": round(metrics.hpcg_flops(n, n, n, 10) / dt / 1e9, 4), "unit": "GFLOP/s", "cores": 1,
+            "kind": "port", "sample": f"C restatement of CG_ref, {n}^3, 10 iterations"}
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    exe = reference_timer_path()
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/hpcg_ref_timer was not built "
+                          "(the reference tree was absent at build time)"}))
+        return 0
+    steps, warm = max(1, args.steps), max(0, args.warmup)
+    iters = reference_iters_for(args.ref_n, 120.0, steps + warm)
+    r = run_reference_sample(args.ref_n, iters, steps, warm)
+    val = r["flops_per_call"] / r["mean_s"] / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GFLOP/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": round(r["mean_s"] * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"HPCG CG_ref, {args.ref_n}^3 sample (the reference cannot generate 512^3: "
+                               f"3.6e9 nonzeros overflow its int local_int_t), {iters} iterations per step",
+                   "grid": [args.ref_n] * 3, "mg_levels": 4, "iters_per_step": iters},
+        "cpu_baseline": {"value": round(val, 4), "unit": "GFLOP/s", "cores": r["threads"], "kind": "reference",
+                         "sample": f"{args.ref_n}^3, {iters} CG_ref iterations per step"},
+        "e2e": {"value": round(val, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(HERE, "profiles", "gs_phase_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+
+def gpu_launches_per_set(iters, nlevels=4):
+    """Kernels the library launches for one CG call (its own kernels only)."""
+    mg = 15 * 2 + 2  # per non-coarsest level: pre and post symmetric sweeps (15 colour phases each),
+    # residual-restriction, prolongation
+    per_mg = mg * (nlevels - 1) + 15
+    per_iter = per_mg + 2 + 1 + 2 + 2  # r'z + finalize, p update (k > 1), SpMV + finalize, x/r update + finalize
+    first_iter_adjust = -1  # k = 1 copies z to p instead of the update kernel
+    loads_stores = 2 + 1    # b and x gathered in, x scattered out
+    preamble = 3            # SpMV, r = b - Ax with r'r, finalize
+    return iters * per_iter + first_iter_adjust + loads_stores + preamble
+
+
+def b200_arm(args, rank, world, local_rank):
+    import torch
+    from hpcg_b200 import binding as B
+    from hpcg_b200 import metrics
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+
+    n = args.n
+    nrow = n ** 3
+    t_setup = time.perf_counter()
+    P = B.Problem.generate(n, n, n, 4, dev)
+    t_setup = time.perf_counter() - t_setup
+    b = torch.empty(nrow, dtype=torch.float64, device=f"cuda:{dev}")
+    x = torch.zeros(nrow, dtype=torch.float64, device=f"cuda:{dev}")
+    P.get_rhs(b)
+    torch.cuda.synchronize()
+    lib_stream = torch.cuda.ExternalStream(B.stream(dev), device=dev)
+
+    def step(bv, xv):
+        if xv.is_cuda:
+            xv.zero_()
+            torch.cuda.current_stream().synchronize()
+        else:
+            xv.zero_()
+        return P.CG(bv, xv, args.iters, 0.0, True)
+
+    for _ in range(args.warmup):
+        step(b, x)
+
+    B.profile(True, dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    res = None
+    for _ in range(args.steps):
+        res = step(b, x)
+    e1.record(lib_stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    gs_ms, gs_launch, gs_rows = B.profile_read(B.PROF_GS_FULL, dev)
+    sp_ms, sp_launch, sp_rows = B.profile_read(B.PROF_SPMV, dev)
+    B.profile(False, dev)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    flops_step = metrics.hpcg_flops(n, n, n, args.iters)
+    value = flops_step * args.steps * world / (ms * 1e-3) / 1e9
+    bytes_iter = metrics.compulsory_bytes(n, n, n)
+    hbm_gbs = bytes_iter * args.iters * args.steps / (ms * 1e-3) / 1e9  # per GPU
+
+    # end to end through the C ABI with pinned host vectors
+    e2e = None
+    if not args.no_e2e:
+        bh = b.cpu().pin_memory()
+        xh = torch.zeros(nrow, dtype=torch.float64).pin_memory()
+        step(bh, xh)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(lib_stream)
+        for _ in range(args.steps):
+            step(bh, xh)
+        f1.record(lib_stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        if dist:
+            t = torch.tensor([ems], dtype=torch.float64, device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": round(flops_step * args.steps * world / (ems * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": 2 * nrow * 8, "d2h_bytes_per_step": nrow * 8 + 64,
+               "ms_per_step": round(ems / args.steps, 3)}
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow)
+        achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
+        tr = committed_traffic()
+        traffic = None
+        if tr and tr.get("n") == n and gs_launch:
+            traffic = tr.get("bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"HPCG CG set: {args.iters} preconditioned CG iterations, {n}^3 grid, "
+                                   f"4 MG levels, 27-point stencil, 8-colour SYMGS, FP64",
+                       "grid": [n, n, n], "rows": nrow, "mg_levels": 4, "iters_per_step": args.iters,
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (43 GB matrix)",
+                       "setup_s": round(t_setup, 3)},
+            "hbm_gbs_compulsory": round(hbm_gbs, 1),
+            "hbm_frac_compulsory": round(hbm_gbs / peak, 4),
+            "bytes_per_iter_compulsory": bytes_iter,
+            "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                         "traffic": traffic, "kernel": "k_gs_phase<double,double,false> (level 0)",
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured"
+                         else peak_kind, "launches": gs_launch, "avg_launch_ms": round(gs_ms / max(gs_launch, 1), 4),
+                         "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
+            "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
+                     "gbs": round((sp_rows * (27 * 12 + 8 + 8)) / (sp_ms * 1e-3) / 1e9, 1) if sp_ms else None},
+            "gpu_launches": gpu_launches_per_set(args.iters) * args.steps,
+            "clocks": clk,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(args)
+            except Exception as ex:  # reported, not fatal
+                line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    P.free()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    return b200_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

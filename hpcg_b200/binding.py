@@ -1,0 +1,310 @@
+"""Python binding of the hpcg_b200 C ABI (include/hpcg_b200.h).
+
+The entry points keep the reference's names and argument meaning
+(src/ComputeSPMV.hpp:20, ComputeSYMGS.hpp:20, ComputeMG.hpp:20, CG.hpp:22-24,
+ComputeDotProduct.hpp:18-19, ComputeWAXPBY.hpp:18-19, ComputeResidual.hpp:18,
+OptimizeProblem.hpp:22-28). Where the reference returns a non-zero int, these
+raise ``HpcgError`` carrying that status.
+
+Vectors are float64 and contiguous: numpy arrays (host) or torch tensors (host
+or CUDA), in the reference's natural row order. The library is loaded from this
+package directory; there is no fallback if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhpcg_b200.so")
+
+OK = 0
+ERR_CUDA = 1
+ERR_ARG = 2
+ERR_UNSUPPORTED = 3
+ERR_NOMEM = 4
+ERR_HANDLE = 5
+ERR_TIMEOUT = 6
+SYMGS_COLOUR = 0
+SYMGS_NATURAL = 1
+
+EXPORTS = (
+    "hpcg_b200_optimize", "hpcg_b200_generate", "hpcg_b200_get_rhs", "hpcg_b200_free",
+    "hpcg_b200_memory_use", "hpcg_b200_set_diagonal", "hpcg_b200_set_values", "hpcg_b200_set_symgs_mode",
+    "hpcg_b200_spmv", "hpcg_b200_symgs", "hpcg_b200_mg", "hpcg_b200_dot", "hpcg_b200_waxpby",
+    "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
+    "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
+    "hpcg_b200_profile_read", "hpcg_b200_last_error",
+)
+
+
+class HpcgError(RuntimeError):
+    def __init__(self, what, status, detail=""):
+        super().__init__(f"{what} failed with status {status}" + (f": {detail}" if detail else ""))
+        self.status = status
+
+
+class LevelDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nrow", C.c_int), ("ncol", C.c_int),
+        ("nonzeros_in_row", C.c_void_p), ("mtx_ind_l", C.c_void_p), ("matrix_values", C.c_void_p),
+        ("f2c", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libhpcg_b200.so (raises if the extension was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C hpcg_b200` "
+                              "(or __graft_entry__.build()); there is no CPU fallback")
+        l = C.CDLL(LIB_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        l.hpcg_b200_optimize.argtypes = [C.POINTER(LevelDesc), i, i, C.POINTER(vp)]
+        l.hpcg_b200_generate.argtypes = [i, i, i, i, i, C.POINTER(vp)]
+        l.hpcg_b200_get_rhs.argtypes = [vp, vp]
+        l.hpcg_b200_free.argtypes = [vp]
+        l.hpcg_b200_memory_use.argtypes = [vp]
+        l.hpcg_b200_memory_use.restype = d
+        l.hpcg_b200_set_diagonal.argtypes = [vp, vp]
+        l.hpcg_b200_set_values.argtypes = [vp, i, vp]
+        l.hpcg_b200_set_symgs_mode.argtypes = [vp, i]
+        l.hpcg_b200_spmv.argtypes = [vp, vp, vp]
+        l.hpcg_b200_symgs.argtypes = [vp, vp, vp]
+        l.hpcg_b200_mg.argtypes = [vp, vp, vp]
+        l.hpcg_b200_dot.argtypes = [i, vp, vp, C.POINTER(d)]
+        l.hpcg_b200_waxpby.argtypes = [i, d, vp, d, vp, vp]
+        l.hpcg_b200_residual.argtypes = [i, vp, vp, C.POINTER(d)]
+        l.hpcg_b200_cg.argtypes = [vp, vp, vp, i, d, i, C.POINTER(i), C.POINTER(d), C.POINTER(d), vp]
+        l.hpcg_b200_cg_mixed.argtypes = [vp, vp, vp, i, d, C.POINTER(i), C.POINTER(d), C.POINTER(d)]
+        l.hpcg_b200_level_info.argtypes = [vp, i, C.POINTER(i), C.POINTER(C.c_int64), vp]
+        l.hpcg_b200_export_level.argtypes = [vp, i, vp, vp, vp, vp]
+        l.hpcg_b200_colour_permutation.argtypes = [i, i, i, vp, vp]
+        l.hpcg_b200_stream.argtypes = [i]
+        l.hpcg_b200_stream.restype = vp
+        l.hpcg_b200_profile.argtypes = [i, i]
+        l.hpcg_b200_profile_read.argtypes = [i, i, C.POINTER(d), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        l.hpcg_b200_last_error.restype = C.c_char_p
+        for name in EXPORTS:
+            f = getattr(l, name)
+            if name not in ("hpcg_b200_memory_use", "hpcg_b200_last_error", "hpcg_b200_stream"):
+                f.restype = C.c_int
+        _lib = l
+    return _lib
+
+
+def last_error() -> str:
+    return lib().hpcg_b200_last_error().decode()
+
+
+def _check(status, what):
+    if status != OK:
+        raise HpcgError(what, status, last_error())
+
+
+def _ptr(v, n=None):
+    """Data pointer of a float64 contiguous numpy array or torch tensor."""
+    if v is None:
+        return None
+    if isinstance(v, np.ndarray):
+        if v.dtype != np.float64 or not v.flags.c_contiguous:
+            raise TypeError("vectors must be contiguous float64")
+        if n is not None and v.shape[0] < n:
+            raise ValueError(f"vector of length {v.shape[0]} shorter than {n}")
+        return v.ctypes.data
+    if hasattr(v, "data_ptr"):
+        import torch
+        if v.dtype != torch.float64 or not v.is_contiguous():
+            raise TypeError("vectors must be contiguous float64")
+        if n is not None and v.numel() < n:
+            raise ValueError(f"vector of length {v.numel()} shorter than {n}")
+        return v.data_ptr()
+    raise TypeError(f"unsupported vector type {type(v)}")
+
+
+def _rowptrs(base_addr, n, row_bytes):
+    return (np.uint64(base_addr) + np.arange(n, dtype=np.uint64) * np.uint64(row_bytes)).astype(np.uint64)
+
+
+class Problem:
+    """A device-resident HPCG hierarchy: the object OptimizeProblem hangs on
+    A.optimizationData (src/OptimizeProblem.cpp:37)."""
+
+    def __init__(self, handle, dims, nlevels):
+        self._h = C.c_void_p(handle)
+        self.dims = dims
+        self.nlevels = nlevels
+
+    # ---- construction ---------------------------------------------------
+    @classmethod
+    def optimize(cls, levels, device=0):
+        """OptimizeProblem from the reference's per-level arrays. Each level is a
+        mapping with nx, ny, nz, nnz [n], cols [n*27] (int32, entry j of row i at
+        i*27+j), vals [n*27] float64 and f2c [n_coarse] int32 (None on the last)."""
+        keep = []
+        descs = (LevelDesc * len(levels))()
+        for i, L in enumerate(levels):
+            n = int(L["nx"] * L["ny"] * L["nz"])
+            nnz8 = np.ascontiguousarray(L["nnz"], dtype=np.int8)
+            cols = np.ascontiguousarray(L["cols"], dtype=np.int32)
+            vals = np.ascontiguousarray(L["vals"], dtype=np.float64)
+            cp = _rowptrs(cols.ctypes.data, n, 27 * 4)
+            vp = _rowptrs(vals.ctypes.data, n, 27 * 8)
+            f2c = L.get("f2c")
+            f2c = None if f2c is None else np.ascontiguousarray(f2c, dtype=np.int32)
+            keep += [nnz8, cols, vals, cp, vp, f2c]
+            descs[i] = LevelDesc(L["nx"], L["ny"], L["nz"], n, n, nnz8.ctypes.data, cp.ctypes.data, vp.ctypes.data,
+                                 f2c.ctypes.data if f2c is not None else None)
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_optimize(descs, len(levels), device, C.byref(h)), "hpcg_b200_optimize")
+        return cls(h.value, (levels[0]["nx"], levels[0]["ny"], levels[0]["nz"]), len(levels))
+
+    @classmethod
+    def generate(cls, nx, ny=None, nz=None, nlevels=4, device=0):
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_generate(nx, ny, nz, nlevels, device, C.byref(h)), "hpcg_b200_generate")
+        return cls(h.value, (nx, ny, nz), nlevels)
+
+    def free(self):
+        if self._h and self._h.value:
+            _check(lib().hpcg_b200_free(self._h), "hpcg_b200_free")
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def nrow(self):
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    # ---- configuration ----------------------------------------------------
+    def memory_use(self) -> float:
+        return lib().hpcg_b200_memory_use(self._h)
+
+    def set_symgs_mode(self, mode):
+        _check(lib().hpcg_b200_set_symgs_mode(self._h, mode), "hpcg_b200_set_symgs_mode")
+
+    def set_diagonal(self, diag):
+        _check(lib().hpcg_b200_set_diagonal(self._h, _ptr(diag, self.nrow)), "hpcg_b200_set_diagonal")
+
+    def set_values(self, level, values27):
+        _check(lib().hpcg_b200_set_values(self._h, level, _ptr(values27)), "hpcg_b200_set_values")
+
+    def get_rhs(self, out=None):
+        out = np.zeros(self.nrow) if out is None else out
+        _check(lib().hpcg_b200_get_rhs(self._h, _ptr(out, self.nrow)), "hpcg_b200_get_rhs")
+        return out
+
+    # ---- the reference's entry points -------------------------------------
+    def ComputeSPMV(self, x, y):
+        _check(lib().hpcg_b200_spmv(self._h, _ptr(x, self.nrow), _ptr(y, self.nrow)), "ComputeSPMV")
+        return 0
+
+    def ComputeSYMGS(self, r, x):
+        _check(lib().hpcg_b200_symgs(self._h, _ptr(r, self.nrow), _ptr(x, self.nrow)), "ComputeSYMGS")
+        return 0
+
+    def ComputeMG(self, r, x):
+        _check(lib().hpcg_b200_mg(self._h, _ptr(r, self.nrow), _ptr(x, self.nrow)), "ComputeMG")
+        return 0
+
+    def CG(self, b, x, max_iter, tolerance, do_preconditioning=True, times=None):
+        """Returns (niters, normr, normr0); x is updated in place."""
+        ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
+        t = None
+        if times is not None:
+            t = np.ascontiguousarray(times, dtype=np.float64)
+        _check(lib().hpcg_b200_cg(self._h, _ptr(b, self.nrow), _ptr(x, self.nrow), max_iter, tolerance,
+                                  int(bool(do_preconditioning)), C.byref(ni), C.byref(nr), C.byref(nr0),
+                                  t.ctypes.data if t is not None else None), "CG")
+        if times is not None:
+            times[:] = t
+        return ni.value, nr.value, nr0.value
+
+    def CG_mixed(self, b, x, max_iter, tolerance):
+        ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
+        _check(lib().hpcg_b200_cg_mixed(self._h, _ptr(b, self.nrow), _ptr(x, self.nrow), max_iter, tolerance,
+                                        C.byref(ni), C.byref(nr), C.byref(nr0)), "CG_mixed")
+        return ni.value, nr.value, nr0.value
+
+    # ---- inspection ------------------------------------------------------------
+    def level_info(self, level):
+        n, pitch = C.c_int(0), C.c_int64(0)
+        starts = np.zeros(9, np.int32)
+        _check(lib().hpcg_b200_level_info(self._h, level, C.byref(n), C.byref(pitch), starts.ctypes.data),
+               "hpcg_b200_level_info")
+        return n.value, pitch.value, starts
+
+    def export_level(self, level):
+        n, pitch, starts = self.level_info(level)
+        n2o = np.zeros(n, np.int32)
+        cols = np.zeros(27 * pitch, np.int32)
+        vals = np.zeros(27 * pitch, np.float64)
+        nc = self.level_info(level + 1)[0] if level + 1 < self.nlevels else 0
+        f2c = np.zeros(max(nc, 1), np.int32)
+        _check(lib().hpcg_b200_export_level(self._h, level, n2o.ctypes.data, cols.ctypes.data, vals.ctypes.data,
+                                            f2c.ctypes.data if nc else None), "hpcg_b200_export_level")
+        return dict(n=n, pitch=pitch, starts=starts, new2old=n2o, cols=cols.reshape(27, pitch),
+                    vals=vals.reshape(27, pitch), f2c=f2c[:nc] if nc else None)
+
+
+def colour_permutation(nx, ny, nz):
+    """(new2old, colour_start) of the library's colour order (host computation)."""
+    n2o = np.zeros(nx * ny * nz, np.int32)
+    starts = np.zeros(9, np.int32)
+    _check(lib().hpcg_b200_colour_permutation(nx, ny, nz, n2o.ctypes.data, starts.ctypes.data),
+           "hpcg_b200_colour_permutation")
+    return n2o, starts
+
+
+PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT = 0, 1, 2, 3
+
+
+def stream(device=0):
+    """The library's cudaStream_t for `device` (an integer handle)."""
+    return lib().hpcg_b200_stream(device)
+
+
+def profile(enable, device=0):
+    _check(lib().hpcg_b200_profile(device, int(bool(enable))), "hpcg_b200_profile")
+
+
+def profile_read(kind, device=0):
+    """(total_ms, launches, rows) of one timed kernel class."""
+    ms, ln, rows = C.c_double(0), C.c_int64(0), C.c_int64(0)
+    _check(lib().hpcg_b200_profile_read(device, kind, C.byref(ms), C.byref(ln), C.byref(rows)),
+           "hpcg_b200_profile_read")
+    return ms.value, ln.value, rows.value
+
+
+def ComputeDotProduct(n, x, y):
+    """ComputeDotProduct_ref.cpp:46-80 semantics; returns the scalar."""
+    out = C.c_double(0)
+    _check(lib().hpcg_b200_dot(n, _ptr(x, n), _ptr(y, n), C.byref(out)), "ComputeDotProduct")
+    return out.value
+
+
+def ComputeWAXPBY(n, alpha, x, beta, y, w):
+    _check(lib().hpcg_b200_waxpby(n, alpha, _ptr(x, n), beta, _ptr(y, n), _ptr(w, n)), "ComputeWAXPBY")
+    return 0
+
+
+def ComputeResidual(n, v1, v2):
+    out = C.c_double(0)
+    _check(lib().hpcg_b200_residual(n, _ptr(v1, n), _ptr(v2, n), C.byref(out)), "ComputeResidual")
+    return out.value

@@ -1,0 +1,211 @@
+// Internal definitions shared by the translation units of libhpcg_b200.so.
+//
+// Device layout of one grid level (all in HBM, allocated once at set-up):
+//   - rows are renumbered into 8 colour blocks by the parity of (ix, iy, iz); the
+//     blocks are stored in sweep order, natural order inside a block;
+//   - the matrix is a 27-slot ELL stored slot-major: val[k*pitch + q], col[k*pitch + q]
+//     for slot k = (sz+1)*9 + (sy+1)*3 + (sx+1), the stencil direction, so slot 13 is
+//     the diagonal and the slot order is the reference's entry order
+//     (GenerateProblem_ref.cpp:152-172); a direction that leaves the grid holds
+//     val = 0 and col = n, the index of a permanently zero vector entry;
+//   - every colour-order vector has `pitch` >= n+1 entries, entry n always 0.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "hpcg_b200.h"
+
+namespace hb {
+
+constexpr int kSlots = 27;
+constexpr int kDiagSlot = 13;
+constexpr int kColours = 8;
+constexpr int kMaxLevels = 4;
+constexpr uint64_t kMagic = 0x48504347b2000001ull;  // "HPCG" + version
+
+// Parity colours in sweep order. The injected (f2c) points, parity colour 0
+// (all coordinates even), are swept last in the forward sweep: swept first they
+// would overwrite the prolonged coarse correction before any other row reads
+// it, and swept last in the backward sweep (i.e. first in the forward sweep) they
+// would hold a zero residual, so restriction would pass nothing down.
+constexpr int kSweepDefault[kColours] = {7, 6, 3, 5, 4, 1, 2, 0};
+
+// The parity bit pattern a stencil direction flips: bit0 for sx = +-1, bit1 for sy, bit2 for sz.
+__host__ __device__ inline int slot_flip(int k) {
+  const int sx = k % 3 - 1, sy = (k / 3) % 3 - 1, sz = k / 9 - 1;
+  return (sx != 0 ? 1 : 0) | (sy != 0 ? 2 : 0) | (sz != 0 ? 4 : 0);
+}
+
+// Geometry of the colour ordering of one (nx, ny, nz) grid.
+struct ColourGrid {
+  int nx, ny, nz;
+  int sweep[kColours];   // parity colour at sweep position s
+  int pos[kColours];     // sweep position of parity colour c
+  int start[kColours + 1];  // first colour-order row of sweep position s
+
+  // points with ix parity b: ix = b, b+2, ... < nx
+  __host__ __device__ static int half(int n, int b) { return (n - b + 1) / 2; }
+
+  __host__ void init(int nx_, int ny_, int nz_, const int* sweep_order) {
+    nx = nx_; ny = ny_; nz = nz_;
+    for (int s = 0; s < kColours; ++s) { sweep[s] = sweep_order[s]; pos[sweep_order[s]] = s; }
+    start[0] = 0;
+    for (int s = 0; s < kColours; ++s) {
+      const int c = sweep[s];
+      start[s + 1] = start[s] + half(nx, c & 1) * half(ny, (c >> 1) & 1) * half(nz, (c >> 2) & 1);
+    }
+  }
+
+  // natural row of (ix, iy, iz) -> colour-order row
+  __host__ __device__ int old2new(int ix, int iy, int iz) const {
+    const int c = (ix & 1) | ((iy & 1) << 1) | ((iz & 1) << 2);
+    const int hx = half(nx, c & 1), hy = half(ny, (c >> 1) & 1);
+    return start[pos[c]] + ((iz >> 1) * hy + (iy >> 1)) * hx + (ix >> 1);
+  }
+
+  // colour-order row -> (ix, iy, iz)
+  __host__ __device__ void coords(int q, int& ix, int& iy, int& iz) const {
+    int s = 0;
+    while (s + 1 < kColours && q >= start[s + 1]) ++s;
+    const int c = sweep[s];
+    const int hx = half(nx, c & 1), hy = half(ny, (c >> 1) & 1);
+    const int m = q - start[s];
+    ix = 2 * (m % hx) + (c & 1);
+    iy = 2 * ((m / hx) % hy) + ((c >> 1) & 1);
+    iz = 2 * (m / (hx * hy)) + ((c >> 2) & 1);
+  }
+};
+
+struct Level {
+  ColourGrid g;
+  int n = 0;                 // rows
+  int64_t pitch = 0;         // slot stride (>= n+1, multiple of 256)
+  double* val = nullptr;     // [27][pitch]
+  int* col = nullptr;        // [27][pitch]
+  float* val32 = nullptr;    // FP32 copy for the mixed-precision V-cycle (built on first use)
+  int* new2old = nullptr;    // [n] colour row -> natural row
+  int* old2new = nullptr;    // [n]
+  int* f2c = nullptr;        // [n of next level] coarse colour row -> fine colour row
+  double* r = nullptr;       // coarse right-hand side (levels > 0), [pitch]
+  double* x = nullptr;       // coarse solution (levels > 0), [pitch]
+  float* r32 = nullptr;      // FP32 V-cycle vectors, [pitch]
+  float* x32 = nullptr;
+  // level-scheduled natural order (built on first use)
+  int* wave_rows = nullptr;  // colour-order rows sorted by ix + 2 iy + 4 iz
+  int nwaves = 0;
+  int* wave_start = nullptr; // host array [nwaves+1]
+};
+
+struct Context;
+
+}  // namespace hb
+
+struct hpcg_b200_problem {
+  uint64_t magic;
+  int device;
+  hb::Context* ctx;
+  int nlev;
+  hb::Level lev[hb::kMaxLevels];
+  int symgs_mode;
+  // level-0 vectors, colour order, [pitch] each
+  double *b, *x, *r, *z, *p, *Ap, *zprev;
+  size_t bytes;  // device bytes held
+};
+
+namespace hb {
+
+// ---- error plumbing ------------------------------------------------------
+void set_error(const char* what, cudaError_t e);
+int status_of(cudaError_t e);
+
+#define HB_CK(call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) {                          \
+      ::hb::set_error(#call, e_);                     \
+      return ::hb::status_of(e_);                     \
+    }                                                 \
+  } while (0)
+
+#define HB_TRY(call)                 \
+  do {                               \
+    int s_ = (call);                 \
+    if (s_ != HPCG_B200_OK) return s_; \
+  } while (0)
+
+// ---- per-device context ------------------------------------------------------
+constexpr int kRedBlocksMax = 4096;  // reduction partial slots
+
+struct Scalars {
+  double rtz, oldrtz, alpha, beta, pAp, normr2, rzprev, tmp;
+};
+
+// Kernel classes timed by the optional launch profiler.
+enum ProfKind : int {
+  kProfGsFull = 0,   // Gauss-Seidel colour phase on level 0, all 27 slots
+  kProfGsFirst = 1,  // first forward sweep on level 0 (x = 0, masked slots)
+  kProfSpmv = 2,     // CG SpMV + p'Ap on level 0
+  kProfRestrict = 3, // residual + restriction, level 0 -> 1
+  kProfKinds = 4,
+};
+
+struct Context {
+  int device = -1;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  double* partials = nullptr;      // [kRedBlocksMax]
+  Scalars* scal = nullptr;         // device scalars
+  Scalars* scal_host = nullptr;    // pinned mirror
+  double* stage[3] = {nullptr, nullptr, nullptr};  // natural-order staging
+  size_t stage_cap = 0;            // entries per staging buffer
+  // launch profiler: CUDA events around selected launches on `stream`
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;                   // free events
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_open[kProfKinds];
+  double prof_ms[kProfKinds] = {0, 0, 0, 0};
+  long prof_launches[kProfKinds] = {0, 0, 0, 0};
+  int64_t prof_rows[kProfKinds] = {0, 0, 0, 0};      // rows processed by the timed launches
+};
+
+// Event pair around one launch of `kind` (no-op unless profiling); prof_end after the launch.
+int prof_begin(Context* c, int kind, cudaEvent_t* start);
+int prof_end(Context* c, int kind, cudaEvent_t start, int64_t rows);
+// Folds finished event pairs into the totals (synchronises the stream).
+int prof_flush(Context* c);
+
+// Context of `device` (created on first use); nullptr on failure (error recorded).
+Context* context_for(int device);
+// Context of the current device.
+Context* current_context();
+// Grows the staging buffers to at least n entries.
+int ensure_stage(Context* c, size_t n);
+
+// Device allocation accounted against the optional budget HPCG_B200_DEVICE_BUDGET (bytes).
+int dev_alloc(void** ptr, size_t bytes, size_t* counter);
+void dev_free(void* ptr);
+
+// true if ptr is device (or managed) memory
+bool is_device_ptr(const void* ptr);
+
+// problem handle validity
+inline bool valid(const hpcg_b200_problem* p) { return p != nullptr && p->magic == kMagic; }
+
+// Grid size for grid-stride kernels: a whole number of waves over the SMs.
+inline int grid_for(const Context* c, int64_t work, int threads, int per_sm) {
+  int64_t blocks = (work + threads - 1) / threads;
+  const int64_t cap = (int64_t)c->sms * per_sm;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+// natural <-> colour order vector movement (solver.cu)
+int load_vector(hpcg_b200_problem* p, int level, const double* src_natural, double* dst_colour);
+int store_vector(hpcg_b200_problem* p, int level, const double* src_colour, double* dst_natural);
+
+}  // namespace hb

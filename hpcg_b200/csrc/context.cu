@@ -1,0 +1,200 @@
+// Per-device context, device allocation accounting and error reporting.
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace hb {
+
+namespace {
+thread_local char g_last_error[512] = "";
+Context* g_ctx[64] = {nullptr};
+std::mutex g_ctx_mu;
+size_t g_budget = 0;        // 0 = unlimited
+size_t g_allocated = 0;
+bool g_budget_read = false;
+
+size_t budget() {
+  if (!g_budget_read) {
+    g_budget_read = true;
+    const char* s = std::getenv("HPCG_B200_DEVICE_BUDGET");
+    if (s && *s) g_budget = (size_t)std::strtoull(s, nullptr, 10);
+  }
+  return g_budget;
+}
+}  // namespace
+
+void set_error(const char* what, cudaError_t e) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+}
+
+int status_of(cudaError_t e) {
+  return e == cudaErrorMemoryAllocation ? HPCG_B200_ERR_NOMEM : HPCG_B200_ERR_CUDA;
+}
+
+int dev_alloc(void** ptr, size_t bytes, size_t* counter) {
+  *ptr = nullptr;
+  if (bytes == 0) return HPCG_B200_OK;
+  const size_t lim = budget();
+  if (lim && g_allocated + bytes > lim) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "device budget of %zu bytes exceeded (%zu requested)",
+                  lim, g_allocated + bytes);
+    return HPCG_B200_ERR_NOMEM;
+  }
+  HB_CK(cudaMalloc(ptr, bytes));
+  g_allocated += bytes;
+  if (counter) *counter += bytes;
+  return HPCG_B200_OK;
+}
+
+// The budget counter is released by the owner of the allocations (free_problem).
+void dev_free(void* ptr) {
+  if (ptr) cudaFree(ptr);
+}
+
+void release_accounted(size_t bytes) { g_allocated = bytes > g_allocated ? 0 : g_allocated - bytes; }
+
+bool is_device_ptr(const void* ptr) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();  // plain pageable host memory on older runtimes
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+Context* context_for(int device) {
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_ctx_mu);
+  if (g_ctx[device]) return g_ctx[device];
+  Context* c = new Context;
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c->partials, sizeof(double) * kRedBlocksMax);
+  if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(Scalars));
+  if (e == cudaSuccess) e = cudaMemset(c->scal, 0, sizeof(Scalars));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->scal_host, sizeof(Scalars));
+  if (e != cudaSuccess) {
+    set_error("context set-up", e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaFree(c->partials);
+    cudaFree(c->scal);
+    delete c;
+    return nullptr;
+  }
+  g_ctx[device] = c;
+  return c;
+}
+
+Context* current_context() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("cudaGetDevice", e);
+    return nullptr;
+  }
+  return context_for(dev);
+}
+
+int ensure_stage(Context* c, size_t n) {
+  if (n <= c->stage_cap) return HPCG_B200_OK;
+  for (int i = 0; i < 3; ++i) {
+    cudaFree(c->stage[i]);
+    c->stage[i] = nullptr;
+  }
+  c->stage_cap = 0;
+  for (int i = 0; i < 3; ++i) HB_CK(cudaMalloc(&c->stage[i], n * sizeof(double)));
+  c->stage_cap = n;
+  return HPCG_B200_OK;
+}
+
+namespace {
+int take_event(Context* c, cudaEvent_t* e) {
+  if (!c->ev_pool.empty()) {
+    *e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return HPCG_B200_OK;
+  }
+  HB_CK(cudaEventCreate(e));
+  return HPCG_B200_OK;
+}
+}  // namespace
+
+int prof_begin(Context* c, int kind, cudaEvent_t* start) {
+  *start = nullptr;
+  if (!c->prof || kind < 0 || kind >= kProfKinds) return HPCG_B200_OK;
+  HB_TRY(take_event(c, start));
+  HB_CK(cudaEventRecord(*start, c->stream));
+  return HPCG_B200_OK;
+}
+
+int prof_end(Context* c, int kind, cudaEvent_t start, int64_t rows) {
+  if (!start) return HPCG_B200_OK;
+  cudaEvent_t stop;
+  HB_TRY(take_event(c, &stop));
+  HB_CK(cudaEventRecord(stop, c->stream));
+  c->ev_open[kind].push_back(std::make_pair(start, stop));
+  c->prof_rows[kind] += rows;
+  return HPCG_B200_OK;
+}
+
+int prof_flush(Context* c) {
+  bool any = false;
+  for (int k = 0; k < kProfKinds; ++k) any = any || !c->ev_open[k].empty();
+  if (!any) return HPCG_B200_OK;
+  HB_CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < kProfKinds; ++k) {
+    for (auto& pr : c->ev_open[k]) {
+      float ms = 0.f;
+      HB_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      c->prof_ms[k] += ms;
+      c->prof_launches[k] += 1;
+      c->ev_pool.push_back(pr.first);
+      c->ev_pool.push_back(pr.second);
+    }
+    c->ev_open[k].clear();
+  }
+  return HPCG_B200_OK;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+const char* hpcg_b200_last_error(void) { return hb::g_last_error; }
+
+void* hpcg_b200_stream(int device) {
+  Context* c = context_for(device);
+  return c ? (void*)c->stream : nullptr;
+}
+
+int hpcg_b200_profile(int device, int enable) {
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_TRY(prof_flush(c));
+  c->prof = enable != 0;
+  for (int k = 0; k < kProfKinds; ++k) {
+    c->prof_ms[k] = 0;
+    c->prof_launches[k] = 0;
+    c->prof_rows[k] = 0;
+  }
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_profile_read(int device, int kind, double* total_ms, int64_t* launches, int64_t* rows) {
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  if (kind < 0 || kind >= kProfKinds) return HPCG_B200_ERR_ARG;
+  HB_TRY(prof_flush(c));
+  if (total_ms) *total_ms = c->prof_ms[kind];
+  if (launches) *launches = c->prof_launches[kind];
+  if (rows) *rows = c->prof_rows[kind];
+  return HPCG_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,289 @@
+// Device kernels of the PCG path. The library is compiled with -fmad=false, so
+// every a*b+c below rounds twice exactly as the reference's C++ does when built
+// without contraction; the per-row summation order is the reference's entry
+// order (slot order). Results of the row kernels are therefore bitwise those of
+// the reference routines on the same ordering; only the dot-product reductions
+// differ (fixed-shape tree instead of a serial loop, deterministic run to run).
+#pragma once
+
+#include "common.cuh"
+
+namespace hb {
+
+constexpr int kThreads = 256;
+
+// Sum of v over the block, valid in thread 0. Fixed shuffle tree: deterministic.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double warp_part[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) warp_part[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (w == 0) {
+    s = lane < (int)(blockDim.x >> 5) ? warp_part[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double warp_part[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) warp_part[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (w == 0) {
+    s = lane < (int)(blockDim.x >> 5) ? warp_part[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
+  }
+  __syncthreads();
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel colour phase: rows [r0, r1) of one colour, updated in parallel
+// (no two rows of a colour are neighbours). Row update as
+// ComputeSYMGS_ref.cpp:72-80: sum = r_i - sum_j a_ij x_j (diagonal included),
+// sum += x_i a_ii, x_i = sum / a_ii.
+// FIRST: the sweep starts from x = 0 (ComputeMG_ref.cpp:42); slots not in `mask`
+// (neighbours not yet swept, and the diagonal) multiply a zero and are skipped,
+// which leaves every sum bitwise unchanged.
+// ---------------------------------------------------------------------------
+template <typename T, typename TR, bool FIRST>
+__global__ void __launch_bounds__(kThreads) k_gs_phase(const T* __restrict__ val, const int* __restrict__ col,
+                                                       int64_t pitch, const TR* __restrict__ rhs, T* x, int r0,
+                                                       int r1, uint32_t mask) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride) {
+    T sum = (T)rhs[q];
+    T xd = (T)0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      if (mask & (1u << k)) {
+        const T a = val[k * pitch + q];
+        const T xv = __ldg(x + col[k * pitch + q]);
+        sum -= a * xv;
+        if (k == kDiagSlot) xd = xv;
+      }
+    }
+    const T d = val[kDiagSlot * pitch + q];
+    if (!FIRST) sum += xd * d;
+    x[q] = sum / d;
+  }
+}
+
+// Natural-order (level-scheduled) Gauss-Seidel: the rows of one wavefront
+// ix + 2 iy + 4 iz = const, which only read rows of other wavefronts.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val, const int* __restrict__ col,
+                                                      int64_t pitch, const T* __restrict__ rhs, T* x,
+                                                      const int* __restrict__ rows, int count) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride) {
+    const int q = rows[t];
+    T sum = rhs[q];
+    T xd = (T)0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const T a = val[k * pitch + q];
+      const T xv = x[col[k * pitch + q]];
+      sum -= a * xv;
+      if (k == kDiagSlot) xd = xv;
+    }
+    const T d = val[kDiagSlot * pitch + q];
+    sum += xd * d;
+    x[q] = sum / d;
+  }
+}
+
+// y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y
+// (the p'Ap of CG.cpp:119, fused).
+template <typename T, bool DOT>
+__global__ void __launch_bounds__(kThreads) k_spmv(const T* __restrict__ val, const int* __restrict__ col,
+                                                   int64_t pitch, const T* __restrict__ x, T* __restrict__ y,
+                                                   int n, double* __restrict__ partials) {
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    T sum = (T)0;
+    T xq = (T)0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const T xv = __ldg(x + col[k * pitch + q]);
+      sum += val[k * pitch + q] * xv;
+      if (k == kDiagSlot) xq = xv;
+    }
+    y[q] = sum;
+    if (DOT) acc += (double)xq * (double)sum;
+  }
+  if (DOT) {
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  }
+}
+
+// Restriction fused with the residual it needs (ComputeMG_ref.cpp:49-51):
+// rc[q] = rf[f] - (A xf)[f] for f = f2c[q]; the residual is formed only at the
+// injected rows (ComputeRestriction_ref.cpp:51 reads no others).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_restrict(const T* __restrict__ val, const int* __restrict__ col,
+                                                       int64_t pitch, const T* __restrict__ rf,
+                                                       const T* __restrict__ xf, const int* __restrict__ f2c,
+                                                       T* __restrict__ rc, int nc) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) {
+    const int f = f2c[q];
+    T sum = (T)0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) sum += val[k * pitch + f] * __ldg(xf + col[k * pitch + f]);
+    rc[q] = rf[f] - sum;
+  }
+}
+
+// ComputeProlongation_ref.cpp:49
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_prolong(const int* __restrict__ f2c, const T* __restrict__ xc,
+                                                      T* __restrict__ xf, int nc) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) xf[f2c[q]] += xc[q];
+}
+
+// ---- vectors ----------------------------------------------------------------
+
+// dst[i] = src[idx[i]]
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gather(T* __restrict__ dst, const T* __restrict__ src,
+                                                     const int* __restrict__ idx, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[idx[i]];
+}
+
+// w = alpha x + beta y (ComputeWAXPBY_ref.cpp:52-67; its alpha == 1 and
+// beta == 1 branches give the same bits, multiplication by 1.0 being exact).
+// NORM: partials of w'w.
+template <bool NORM>
+__global__ void __launch_bounds__(kThreads) k_waxpby(int n, double alpha, const double* __restrict__ x, double beta,
+                                                     const double* __restrict__ y, double* w,
+                                                     double* __restrict__ partials) {
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double v = alpha * x[i] + beta * y[i];
+    w[i] = v;
+    if (NORM) acc += v * v;
+  }
+  if (NORM) {
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  }
+}
+
+// partials of x'y (ComputeDotProduct_ref.cpp:54-64); TWO: also of x'y2 into
+// partials[gridDim.x + block] (the r'z_prev of flexible CG, sharing the read of x).
+template <bool TWO>
+__global__ void __launch_bounds__(kThreads) k_dot(int n, const double* __restrict__ x, const double* __restrict__ y,
+                                                  const double* __restrict__ y2, double* __restrict__ partials) {
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0, acc2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double xi = x[i];
+    acc += xi * y[i];
+    if (TWO) acc2 += xi * y2[i];
+  }
+  const double s = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (TWO) {
+    const double s2 = block_sum(acc2);
+    if (threadIdx.x == 0) partials[gridDim.x + blockIdx.x] = s2;
+  }
+}
+
+// partial maxima of |v1 - v2| (ComputeResidual.cpp:70-75)
+__global__ void __launch_bounds__(kThreads) k_maxdiff(int n, const double* __restrict__ a,
+                                                      const double* __restrict__ b, double* __restrict__ partials) {
+  const int stride = gridDim.x * blockDim.x;
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double d = fabs(a[i] - b[i]);
+    if (d > m) m = d;
+  }
+  const double s = block_max(m);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// ---- CG scalar bookkeeping on the device -----------------------------------
+
+enum FinOp : int {
+  kFinStore = 0,     // *out = sum
+  kFinNormr = 1,     // s->normr2 = sum
+  kFinRtzFirst = 2,  // s->rtz = sum
+  kFinRtz = 3,       // oldrtz = rtz; rtz = sum; beta = rtz / oldrtz   (CG.cpp:112-114)
+  kFinPap = 4,       // pAp = sum; alpha = rtz / pAp                    (CG.cpp:119-120)
+  kFinFlex = 5,      // oldrtz = rtz; rtz = sum; beta = (rtz - sum2) / oldrtz (flexible PR)
+  kFinMax = 6,       // *out = max of partials
+};
+
+// One block: fixed-order reduction of nparts partials (and of the second set
+// at partials[nparts..] for kFinFlex), then the scalar update of `op`.
+__global__ void __launch_bounds__(kThreads) k_finalize(const double* __restrict__ partials, int nparts, int op,
+                                                       Scalars* s, double* out) {
+  double acc = 0.0, acc2 = 0.0;
+  if (op == kFinMax) {
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc = fmax(acc, partials[i]);
+    const double m = block_max(acc);
+    if (threadIdx.x == 0) *out = m;
+    return;
+  }
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += partials[i];
+  if (op == kFinFlex)
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc2 += partials[nparts + i];
+  const double sum = block_sum(acc);
+  const double sum2 = op == kFinFlex ? block_sum(acc2) : 0.0;
+  if (threadIdx.x != 0) return;
+  switch (op) {
+    case kFinStore: *out = sum; break;
+    case kFinNormr: s->normr2 = sum; break;
+    case kFinRtzFirst: s->rtz = sum; break;
+    case kFinRtz: s->oldrtz = s->rtz; s->rtz = sum; s->beta = sum / s->oldrtz; break;
+    case kFinPap: s->pAp = sum; s->alpha = s->rtz / sum; break;
+    case kFinFlex: s->oldrtz = s->rtz; s->rtz = sum; s->rzprev = sum2; s->beta = (sum - sum2) / s->oldrtz; break;
+    default: break;
+  }
+}
+
+// p = z + beta p (CG.cpp:115 as WAXPBY(1, z, beta, p)), beta from the device scalars.
+__global__ void __launch_bounds__(kThreads) k_update_p(int n, const double* __restrict__ z, double* p,
+                                                       const Scalars* __restrict__ s) {
+  const double beta = s->beta;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = z[i] + beta * p[i];
+}
+
+// x = x + alpha p; r = r + (-alpha) Ap (CG.cpp:121-122); partials of r'r (CG.cpp:123).
+__global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const double* __restrict__ p, double* r,
+                                                        const double* __restrict__ Ap, const Scalars* __restrict__ s,
+                                                        double* __restrict__ partials) {
+  const double alpha = s->alpha, malpha = -s->alpha;
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] = x[i] + alpha * p[i];
+    const double ri = r[i] + malpha * Ap[i];
+    r[i] = ri;
+    acc += ri * ri;
+  }
+  const double sum = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+}
+
+// precision conversion for the FP32 V-cycle
+template <typename TO, typename TI>
+__global__ void __launch_bounds__(kThreads) k_convert(TO* __restrict__ dst, const TI* __restrict__ src, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (TO)src[i];
+}
+
+}  // namespace hb

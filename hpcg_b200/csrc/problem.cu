@@ -1,0 +1,419 @@
+// Problem set-up: the device hierarchy built from the reference's host
+// structures (OptimizeProblem) or generated on the device, plus release,
+// accounting and inspection.
+#include <algorithm>
+#include <atomic>
+#include <functional>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hb {
+
+void release_accounted(size_t bytes);
+
+namespace {
+
+int64_t pitch_for(int n) { return ((int64_t)n + 1 + 255) / 256 * 256; }
+
+template <typename T>
+int alloc_n(hpcg_b200_problem* p, T** ptr, int64_t count) {
+  return dev_alloc((void**)ptr, sizeof(T) * (size_t)count, &p->bytes);
+}
+
+hpcg_b200_problem* new_problem(int device, Context* c) {
+  hpcg_b200_problem* p = new hpcg_b200_problem;
+  std::memset(p, 0, sizeof(*p));
+  p->magic = kMagic;
+  p->device = device;
+  p->ctx = c;
+  p->symgs_mode = HPCG_B200_SYMGS_COLOUR;
+  for (int l = 0; l < kMaxLevels; ++l) p->lev[l] = Level();
+  return p;
+}
+
+// Vectors of every level, zeroed so that entry n (the zero sink of padded slots) is 0.
+int alloc_vectors(hpcg_b200_problem* p) {
+  Level& L0 = p->lev[0];
+  double** v0[] = {&p->b, &p->x, &p->r, &p->z, &p->p, &p->Ap, &p->zprev};
+  for (double** v : v0) {
+    HB_TRY(alloc_n(p, v, L0.pitch));
+    HB_CK(cudaMemsetAsync(*v, 0, sizeof(double) * L0.pitch, p->ctx->stream));
+  }
+  for (int l = 1; l < p->nlev; ++l) {
+    Level& L = p->lev[l];
+    HB_TRY(alloc_n(p, &L.r, L.pitch));
+    HB_TRY(alloc_n(p, &L.x, L.pitch));
+    HB_CK(cudaMemsetAsync(L.r, 0, sizeof(double) * L.pitch, p->ctx->stream));
+    HB_CK(cudaMemsetAsync(L.x, 0, sizeof(double) * L.pitch, p->ctx->stream));
+  }
+  return HPCG_B200_OK;
+}
+
+void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)>& body) {
+  unsigned t = std::thread::hardware_concurrency();
+  if (t == 0) t = 1;
+  if (t > 32) t = 32;
+  if (n < 65536 || t == 1) {
+    body(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const int64_t chunk = (n + t - 1) / t;
+  for (unsigned i = 0; i < t; ++i) {
+    const int64_t b = i * chunk, e = std::min<int64_t>(n, b + chunk);
+    if (b < e) pool.emplace_back(body, b, e);
+  }
+  for (auto& th : pool) th.join();
+}
+
+// ---- device generator (GenerateProblem_ref.cpp:131-183 in colour order) -----
+
+__global__ void k_generate(ColourGrid g, int n, int64_t pitch, double* __restrict__ val, int* __restrict__ col,
+                           int* __restrict__ new2old, int* __restrict__ old2new, double* __restrict__ b) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    int ix, iy, iz;
+    g.coords(q, ix, iy, iz);
+    const int i = (iz * g.ny + iy) * g.nx + ix;
+    new2old[q] = i;
+    old2new[i] = q;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const int jx = ix + k % 3 - 1, jy = iy + (k / 3) % 3 - 1, jz = iz + k / 9 - 1;
+      const bool in = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
+      col[k * pitch + q] = in ? g.old2new(jx, jy, jz) : n;
+      val[k * pitch + q] = in ? (k == kDiagSlot ? 26.0 : -1.0) : 0.0;
+      cnt += in ? 1 : 0;
+    }
+    if (b) b[q] = 26.0 - (double)(cnt - 1);
+  }
+}
+
+// f2c (GenerateCoarseProblem.cpp:71-82) between two colour orders
+__global__ void k_generate_f2c(ColourGrid gf, ColourGrid gc, int nc, int* __restrict__ f2c) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) {
+    int ix, iy, iz;
+    gc.coords(q, ix, iy, iz);
+    f2c[q] = gf.old2new(2 * ix, 2 * iy, 2 * iz);
+  }
+}
+
+// scatter of natural-order diagonal values into slot 13
+__global__ void k_set_diag(const double* __restrict__ d, const int* __restrict__ old2new, double* __restrict__ val13,
+                           int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) val13[old2new[i]] = d[i];
+}
+
+// natural-order direction-slot values [n][27] into the colour-order slot-major layout
+__global__ void k_set_values(const double* __restrict__ v, const int* __restrict__ new2old, double* __restrict__ val,
+                             int64_t pitch, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const int64_t i = new2old[q];
+    for (int k = 0; k < kSlots; ++k) val[k * pitch + q] = v[i * kSlots + k];
+  }
+}
+
+int check_dims(int nx, int ny, int nz, int nlevels) {
+  if (nx < 1 || ny < 1 || nz < 1 || nlevels < 1 || nlevels > kMaxLevels) return HPCG_B200_ERR_ARG;
+  if ((int64_t)nx * ny * nz >= (int64_t)1 << 31) return HPCG_B200_ERR_UNSUPPORTED;
+  for (int l = 1; l < nlevels; ++l) {  // GenerateCoarseProblem.cpp:50
+    const int f = 1 << (l - 1);
+    if ((nx / f) % 2 || (ny / f) % 2 || (nz / f) % 2) return HPCG_B200_ERR_UNSUPPORTED;
+  }
+  return HPCG_B200_OK;
+}
+
+}  // namespace
+
+int free_problem(hpcg_b200_problem* p) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  cudaSetDevice(p->device);
+  if (p->ctx) cudaStreamSynchronize(p->ctx->stream);
+  for (int l = 0; l < kMaxLevels; ++l) {
+    Level& L = p->lev[l];
+    void* ptrs[] = {L.val, L.col, L.val32, L.new2old, L.old2new, L.f2c, L.r, L.x, L.r32, L.x32, L.wave_rows};
+    for (void* q : ptrs) dev_free(q);
+    delete[] L.wave_start;
+  }
+  void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
+  for (void* q : vs) dev_free(q);
+  release_accounted(p->bytes);
+  p->magic = 0;
+  delete p;
+  return HPCG_B200_OK;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+int hpcg_b200_optimize(const hpcg_b200_level_desc* desc, int nlevels, int device, hpcg_b200_problem** out) {
+  if (!desc || !out || nlevels < 1 || nlevels > kMaxLevels) return HPCG_B200_ERR_ARG;
+  *out = nullptr;
+  for (int l = 0; l < nlevels; ++l) {
+    const hpcg_b200_level_desc& d = desc[l];
+    if (!d.nonzeros_in_row || !d.mtx_ind_l || !d.matrix_values) return HPCG_B200_ERR_ARG;
+    if ((int64_t)d.nx * d.ny * d.nz != d.nrow || d.ncol != d.nrow || d.nrow < 1) return HPCG_B200_ERR_ARG;
+    if (l + 1 < nlevels) {
+      if (!d.f2c) return HPCG_B200_ERR_ARG;
+      const hpcg_b200_level_desc& c = desc[l + 1];
+      if (c.nx * 2 != d.nx || c.ny * 2 != d.ny || c.nz * 2 != d.nz) return HPCG_B200_ERR_UNSUPPORTED;
+    }
+  }
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_CK(cudaSetDevice(device));
+  hpcg_b200_problem* p = new_problem(device, c);
+  p->nlev = nlevels;
+  std::vector<ColourGrid> grids(nlevels);
+  for (int l = 0; l < nlevels; ++l) {
+    grids[l].init(desc[l].nx, desc[l].ny, desc[l].nz, kSweepDefault);
+    p->lev[l].g = grids[l];
+    p->lev[l].n = desc[l].nrow;
+    p->lev[l].pitch = pitch_for(desc[l].nrow);
+  }
+  int status = HPCG_B200_OK;
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
+    const hpcg_b200_level_desc& d = desc[l];
+    Level& L = p->lev[l];
+    const ColourGrid& g = grids[l];
+    const int n = L.n;
+    const int64_t pitch = L.pitch;
+    std::vector<double> val((size_t)kSlots * pitch, 0.0);
+    std::vector<int> col((size_t)kSlots * pitch, n);
+    std::vector<int> n2o(n), o2n(n);
+    std::atomic<int> bad(0);
+    parallel_for(n, [&](int64_t b, int64_t e) {
+      for (int64_t i = b; i < e; ++i) {
+        const int ix = (int)(i % d.nx), iy = (int)((i / d.nx) % d.ny), iz = (int)(i / ((int64_t)d.nx * d.ny));
+        const int q = g.old2new(ix, iy, iz);
+        n2o[q] = (int)i;
+        o2n[i] = q;
+        const int cnt = d.nonzeros_in_row[i];
+        if (cnt < 1 || cnt > kSlots) { bad = 1; continue; }
+        uint32_t seen = 0;
+        for (int j = 0; j < cnt; ++j) {
+          const int cj = d.mtx_ind_l[i][j];
+          if (cj < 0 || cj >= n) { bad = 1; break; }
+          const int dx = cj % d.nx - ix, dy = (cj / d.nx) % d.ny - iy, dz = cj / (d.nx * d.ny) - iz;
+          if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) { bad = 1; break; }
+          const int k = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+          if (seen & (1u << k)) { bad = 1; break; }
+          seen |= 1u << k;
+          val[(size_t)k * pitch + q] = d.matrix_values[i][j];
+          col[(size_t)k * pitch + q] = g.old2new(ix + dx, iy + dy, iz + dz);
+        }
+        if (!(seen & (1u << kDiagSlot))) bad = 1;
+      }
+    });
+    if (bad) { status = HPCG_B200_ERR_UNSUPPORTED; break; }
+    status = alloc_n(p, &L.val, kSlots * pitch);
+    if (!status) status = alloc_n(p, &L.col, kSlots * pitch);
+    if (!status) status = alloc_n(p, &L.new2old, n);
+    if (!status) status = alloc_n(p, &L.old2new, n);
+    if (status) break;
+    cudaError_t e = cudaMemcpy(L.val, val.data(), sizeof(double) * val.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(L.col, col.data(), sizeof(int) * col.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(L.new2old, n2o.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(L.old2new, o2n.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { set_error("optimize upload", e); status = status_of(e); break; }
+    if (l + 1 < nlevels) {
+      const int nc = desc[l + 1].nrow;
+      const ColourGrid& gc = grids[l + 1];
+      std::vector<int> f(nc);
+      for (int qc = 0; qc < nc && !bad; ++qc) {
+        int cx, cy, cz;
+        gc.coords(qc, cx, cy, cz);
+        const int natc = (cz * desc[l + 1].ny + cy) * desc[l + 1].nx + cx;
+        const int ff = d.f2c[natc];
+        if (ff < 0 || ff >= n) { bad = 1; break; }
+        f[qc] = o2n[ff];
+      }
+      if (bad) { status = HPCG_B200_ERR_ARG; break; }
+      status = alloc_n(p, &L.f2c, nc);
+      if (status) break;
+      e = cudaMemcpy(L.f2c, f.data(), sizeof(int) * nc, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) { set_error("optimize f2c upload", e); status = status_of(e); break; }
+    }
+  }
+  if (status == HPCG_B200_OK) status = alloc_vectors(p);
+  if (status == HPCG_B200_OK) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_error("optimize sync", e); status = status_of(e); }
+  }
+  if (status != HPCG_B200_OK) {
+    free_problem(p);
+    return status;
+  }
+  *out = p;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_generate(int nx, int ny, int nz, int nlevels, int device, hpcg_b200_problem** out) {
+  if (!out) return HPCG_B200_ERR_ARG;
+  *out = nullptr;
+  HB_TRY(check_dims(nx, ny, nz, nlevels));
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_CK(cudaSetDevice(device));
+  hpcg_b200_problem* p = new_problem(device, c);
+  p->nlev = nlevels;
+  int status = HPCG_B200_OK;
+  for (int l = 0; l < nlevels; ++l) {
+    Level& L = p->lev[l];
+    L.g.init(nx >> l, ny >> l, nz >> l, kSweepDefault);
+    L.n = (nx >> l) * (ny >> l) * (nz >> l);
+    L.pitch = pitch_for(L.n);
+  }
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
+    Level& L = p->lev[l];
+    status = alloc_n(p, &L.val, kSlots * L.pitch);
+    if (!status) status = alloc_n(p, &L.col, kSlots * L.pitch);
+    if (!status) status = alloc_n(p, &L.new2old, L.n);
+    if (!status) status = alloc_n(p, &L.old2new, L.n);
+    if (!status && l + 1 < nlevels) status = alloc_n(p, &L.f2c, p->lev[l + 1].n);
+  }
+  if (status == HPCG_B200_OK) status = alloc_vectors(p);
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
+    Level& L = p->lev[l];
+    // padding columns of the tail [n, pitch) are never read; zero them anyway
+    cudaError_t e = cudaMemsetAsync(L.val, 0, sizeof(double) * kSlots * L.pitch, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.col, 0, sizeof(int) * kSlots * L.pitch, c->stream);
+    if (e != cudaSuccess) { set_error("generate memset", e); status = status_of(e); break; }
+    k_generate<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(L.g, L.n, L.pitch, L.val, L.col, L.new2old,
+                                                                  L.old2new, l == 0 ? p->b : nullptr);
+    if (l + 1 < nlevels) {
+      const Level& C = p->lev[l + 1];
+      k_generate_f2c<<<grid_for(c, C.n, 256, 8), 256, 0, c->stream>>>(L.g, C.g, C.n, L.f2c);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_error("generate", e); status = status_of(e); }
+  }
+  if (status != HPCG_B200_OK) {
+    free_problem(p);
+    return status;
+  }
+  *out = p;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_free(hpcg_b200_problem* p) { return free_problem(p); }
+
+int hpcg_b200_colour_permutation(int nx, int ny, int nz, int* new2old, int* colour_start) {
+  if (nx < 1 || ny < 1 || nz < 1 || (int64_t)nx * ny * nz >= ((int64_t)1 << 31)) return HPCG_B200_ERR_ARG;
+  ColourGrid g;
+  g.init(nx, ny, nz, kSweepDefault);
+  if (colour_start)
+    for (int s = 0; s <= kColours; ++s) colour_start[s] = g.start[s];
+  if (new2old)
+    for (int iz = 0; iz < nz; ++iz)
+      for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix) new2old[g.old2new(ix, iy, iz)] = (iz * ny + iy) * nx + ix;
+  return HPCG_B200_OK;
+}
+
+double hpcg_b200_memory_use(const hpcg_b200_problem* p) { return valid(p) ? (double)p->bytes : 0.0; }
+
+int hpcg_b200_get_rhs(hpcg_b200_problem* p, double* b) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!b) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  return store_vector(p, 0, p->b, b);
+}
+
+int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!diagonal) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  Level& L = p->lev[0];
+  Context* c = p->ctx;
+  const double* src = diagonal;
+  if (!is_device_ptr(diagonal)) {
+    HB_TRY(ensure_stage(c, L.n));
+    HB_CK(cudaMemcpyAsync(c->stage[1], diagonal, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
+    src = c->stage[1];
+  }
+  k_set_diag<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(src, L.old2new, L.val + kDiagSlot * L.pitch, L.n);
+  HB_CK(cudaGetLastError());
+  if (L.val32) {  // the FP32 copy is rebuilt on next use
+    dev_free(L.val32);
+    L.val32 = nullptr;
+  }
+  HB_CK(cudaStreamSynchronize(c->stream));
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!values27 || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  Level& L = p->lev[level];
+  Context* c = p->ctx;
+  double* tmp = nullptr;
+  const double* src = values27;
+  if (!is_device_ptr(values27)) {
+    HB_CK(cudaMalloc(&tmp, sizeof(double) * (size_t)kSlots * L.n));
+    cudaError_t e = cudaMemcpy(tmp, values27, sizeof(double) * (size_t)kSlots * L.n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(tmp);
+      set_error("set_values upload", e);
+      return status_of(e);
+    }
+    src = tmp;
+  }
+  k_set_values<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(src, L.new2old, L.val, L.pitch, L.n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) {
+    set_error("set_values", e);
+    return status_of(e);
+  }
+  if (L.val32) {
+    dev_free(L.val32);
+    L.val32 = nullptr;
+  }
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_set_symgs_mode(hpcg_b200_problem* p, int mode) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (mode != HPCG_B200_SYMGS_COLOUR && mode != HPCG_B200_SYMGS_NATURAL) return HPCG_B200_ERR_ARG;
+  p->symgs_mode = mode;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64_t* pitch, int* colour_start) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  const Level& L = p->lev[level];
+  if (nrow) *nrow = L.n;
+  if (pitch) *pitch = L.pitch;
+  if (colour_start)
+    for (int s = 0; s <= kColours; ++s) colour_start[s] = L.g.start[s];
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_export_level(const hpcg_b200_problem* p, int level, int* new2old, int* cols, double* vals, int* f2c) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  const Level& L = p->lev[level];
+  HB_CK(cudaStreamSynchronize(p->ctx->stream));
+  if (new2old) HB_CK(cudaMemcpy(new2old, L.new2old, sizeof(int) * L.n, cudaMemcpyDeviceToHost));
+  if (cols) HB_CK(cudaMemcpy(cols, L.col, sizeof(int) * kSlots * L.pitch, cudaMemcpyDeviceToHost));
+  if (vals) HB_CK(cudaMemcpy(vals, L.val, sizeof(double) * kSlots * L.pitch, cudaMemcpyDeviceToHost));
+  if (f2c && L.f2c) HB_CK(cudaMemcpy(f2c, L.f2c, sizeof(int) * p->lev[level + 1].n, cudaMemcpyDeviceToHost));
+  return HPCG_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,522 @@
+// Entry points of the PCG path: SpMV, SYMGS, the V-cycle, CG and the vector
+// routines, with the host-side drivers that sequence the kernels.
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace hb {
+
+namespace {
+
+constexpr uint32_t kAllSlots = (1u << kSlots) - 1;
+constexpr int kPerSm = 8;  // resident 256-thread blocks per SM targeted by grid-stride kernels
+
+inline int red_blocks(const Context* c, int64_t n) {
+  int b = grid_for(c, n, kThreads, kPerSm);
+  return b > kRedBlocksMax / 2 ? kRedBlocksMax / 2 : b;
+}
+
+// Slots read by a first-sweep colour phase: neighbours of colours swept
+// earlier in this sweep. All others (and the diagonal) multiply x = 0.
+uint32_t first_mask(const ColourGrid& g, int s) {
+  const int c = g.sweep[s];
+  uint32_t m = 0;
+  for (int k = 0; k < kSlots; ++k) {
+    if (k == kDiagSlot) continue;
+    if (g.pos[c ^ slot_flip(k)] < s) m |= 1u << k;
+  }
+  return m;
+}
+
+template <typename T, typename TR>
+int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int s, bool first, bool top) {
+  const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
+  if (r1 <= r0) return HPCG_B200_OK;
+  const int grid = grid_for(c, r1 - r0, kThreads, kPerSm);
+  const int kind = top ? (first ? kProfGsFirst : kProfGsFull) : -1;
+  cudaEvent_t ev0 = nullptr;
+  HB_TRY(prof_begin(c, kind, &ev0));
+  if (first)
+    k_gs_phase<T, TR, true><<<grid, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1,
+                                                               first_mask(L.g, s));
+  else
+    k_gs_phase<T, TR, false><<<grid, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+  HB_CK(cudaGetLastError());
+  return prof_end(c, kind, ev0, r1 - r0);
+}
+
+// One symmetric Gauss-Seidel step in colour order: forward over the sweep
+// positions, then backward. The last non-empty colour of the forward sweep is
+// not repeated at the start of the backward sweep: its rows read only other
+// colours, none of which changed in between, so a repeat would rewrite the
+// same bits. first: x enters as zero (ComputeMG_ref.cpp:42).
+template <typename T, typename TR>
+int gs_colour(Context* c, const Level& L, const T* val, const TR* rhs, T* x, bool first, bool top) {
+  int last = -1;
+  for (int s = 0; s < kColours; ++s) {
+    if (L.g.start[s + 1] > L.g.start[s]) last = s;
+    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, first, top)));
+  }
+  for (int s = last - 1; s >= 0; --s) HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, false, top)));
+  return HPCG_B200_OK;
+}
+
+// Wavefronts ix + 2 iy + 4 iz: every lower neighbour (in the reference's natural
+// order) of a row lies on an earlier wavefront, every upper one on a later one.
+int ensure_waves(Level& L) {
+  if (L.wave_rows) return HPCG_B200_OK;
+  const ColourGrid& g = L.g;
+  const int nw = (g.nx - 1) + 2 * (g.ny - 1) + 4 * (g.nz - 1) + 1;
+  std::vector<int> count(nw + 1, 0), rows(L.n);
+  std::vector<int> wave(L.n);
+  for (int q = 0; q < L.n; ++q) {
+    int ix, iy, iz;
+    g.coords(q, ix, iy, iz);
+    wave[q] = ix + 2 * iy + 4 * iz;
+    ++count[wave[q] + 1];
+  }
+  for (int w = 0; w < nw; ++w) count[w + 1] += count[w];
+  std::vector<int> fill(count.begin(), count.end() - 1);
+  for (int q = 0; q < L.n; ++q) rows[fill[wave[q]]++] = q;
+  int* d = nullptr;
+  HB_CK(cudaMalloc(&d, sizeof(int) * L.n));
+  cudaError_t e = cudaMemcpy(d, rows.data(), sizeof(int) * L.n, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    set_error("wave upload", e);
+    return status_of(e);
+  }
+  L.wave_rows = d;
+  L.nwaves = nw;
+  L.wave_start = new int[nw + 1];
+  for (int w = 0; w <= nw; ++w) L.wave_start[w] = count[w];
+  return HPCG_B200_OK;
+}
+
+int gs_natural(Context* c, Level& L, const double* rhs, double* x) {
+  HB_TRY(ensure_waves(L));
+  for (int dir = 0; dir < 2; ++dir) {
+    for (int t = 0; t < L.nwaves; ++t) {
+      const int w = dir == 0 ? t : L.nwaves - 1 - t;
+      const int b = L.wave_start[w], cnt = L.wave_start[w + 1] - b;
+      if (cnt == 0) continue;
+      k_gs_rows<double><<<grid_for(c, cnt, kThreads, kPerSm), kThreads, 0, c->stream>>>(
+          L.val, L.col, L.pitch, rhs, x, L.wave_rows + b, cnt);
+    }
+  }
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int symgs_level(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero) {
+  Level& L = p->lev[l];
+  Context* c = p->ctx;
+  if (p->symgs_mode == HPCG_B200_SYMGS_NATURAL) {
+    if (x_is_zero) HB_CK(cudaMemsetAsync(x, 0, sizeof(double) * L.n, c->stream));
+    return gs_natural(c, L, rhs, x);
+  }
+  return gs_colour<double, double>(c, L, L.val, rhs, x, x_is_zero, l == 0);
+}
+
+// ComputeMG_ref.cpp:39-63 on colour-order device vectors of level l.
+int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x) {
+  Level& L = p->lev[l];
+  Context* c = p->ctx;
+  HB_TRY(symgs_level(p, l, r, x, true));
+  if (l + 1 < p->nlev) {
+    Level& C = p->lev[l + 1];
+    cudaEvent_t ev0 = nullptr;
+    HB_TRY(prof_begin(c, l == 0 ? kProfRestrict : -1, &ev0));
+    k_restrict<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x,
+                                                                                         L.f2c, C.r, C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(prof_end(c, l == 0 ? kProfRestrict : -1, ev0, C.n));
+    HB_TRY(mg_level(p, l + 1, C.r, C.x));
+    k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x, x, C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(symgs_level(p, l, r, x, false));
+  }
+  return HPCG_B200_OK;
+}
+
+int finalize(Context* c, int nparts, int op, double* out = nullptr) {
+  k_finalize<<<1, kThreads, 0, c->stream>>>(c->partials, nparts, op, c->scal, out);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int read_scalars(Context* c) {
+  HB_CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  return HPCG_B200_OK;
+}
+
+struct Setter {  // selects the problem's device for the duration of a call
+  int prev = -1;
+  explicit Setter(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~Setter() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// CG.cpp:59-143 on the resident vectors p->b, p->x (colour order).
+int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niters, double* normr_out,
+           double* normr0_out, double* times) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const int n = L.n;
+  const int nb = red_blocks(c, n);
+  const int gv = grid_for(c, n, kThreads, kPerSm);
+  const double t_begin = now_s();
+  std::vector<cudaEvent_t> ev;
+  auto mark = [&](void) -> int {
+    if (!times) return HPCG_B200_OK;
+    cudaEvent_t e;
+    HB_CK(cudaEventCreate(&e));
+    ev.push_back(e);
+    HB_CK(cudaEventRecord(e, c->stream));
+    return HPCG_B200_OK;
+  };
+  // p = x; Ap = A p; r = b - Ap; normr = sqrt(r'r)   (CG.cpp:86-90)
+  k_spmv<double, false><<<gv, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->x, P->Ap, n, nullptr);
+  k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, P->b, -1.0, P->Ap, P->r, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinNormr));
+  HB_TRY(read_scalars(c));
+  double normr = std::sqrt(c->scal_host->normr2);
+  const double normr0 = normr;
+  *niters = 0;
+  for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
+    HB_TRY(mark());
+    if (prec) {
+      HB_TRY(mg_level(P, 0, P->r, P->z));                                   // CG.cpp:103
+    } else {
+      HB_CK(cudaMemcpyAsync(P->z, P->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :105
+    }
+    HB_TRY(mark());
+    k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);  // :110 / :113
+    HB_CK(cudaGetLastError());
+    if (k == 1) {
+      HB_TRY(finalize(c, nb, kFinRtzFirst));
+      HB_CK(cudaMemcpyAsync(P->p, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :109
+    } else {
+      HB_TRY(finalize(c, nb, kFinRtz));
+      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);  // :115
+      HB_CK(cudaGetLastError());
+    }
+    HB_TRY(mark());
+    cudaEvent_t ev0 = nullptr;
+    HB_TRY(prof_begin(c, kProfSpmv, &ev0));
+    k_spmv<double, true><<<nb, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->p, P->Ap, n, c->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(prof_end(c, kProfSpmv, ev0, n));
+    HB_TRY(finalize(c, nb, kFinPap));                                       // :118-120
+    HB_TRY(mark());
+    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);  // :121-123
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize(c, nb, kFinNormr));
+    HB_TRY(mark());
+    HB_TRY(read_scalars(c));
+    normr = std::sqrt(c->scal_host->normr2);
+    *niters = k;
+  }
+  *normr_out = normr;
+  *normr0_out = normr0;
+  if (c->prof) HB_TRY(prof_flush(c));
+  if (times) {
+    HB_CK(cudaStreamSynchronize(c->stream));
+    double t_mg = 0, t_dw = 0, t_spmv = 0, t_up = 0;
+    for (size_t i = 0; i + 4 < ev.size(); i += 5) {
+      float a, b2, d, e;
+      cudaEventElapsedTime(&a, ev[i], ev[i + 1]);
+      cudaEventElapsedTime(&b2, ev[i + 1], ev[i + 2]);
+      cudaEventElapsedTime(&d, ev[i + 2], ev[i + 3]);
+      cudaEventElapsedTime(&e, ev[i + 3], ev[i + 4]);
+      t_mg += a * 1e-3; t_dw += b2 * 1e-3; t_spmv += d * 1e-3; t_up += e * 1e-3;
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    times[1] += 0.5 * (t_dw + t_up);  // dot products (fused with the vector updates)
+    times[2] += 0.5 * (t_dw + t_up);  // WAXPBY
+    times[3] += t_spmv;
+    times[5] += t_mg;
+    times[0] += now_s() - t_begin;
+  }
+  return HPCG_B200_OK;
+}
+
+
+// ---- FP32 V-cycle ----------------------------------------------------------
+
+// FP32 copies of the values and FP32 work vectors of every level (first use).
+int ensure_f32(hpcg_b200_problem* P) {
+  Context* c = P->ctx;
+  for (int l = 0; l < P->nlev; ++l) {
+    Level& L = P->lev[l];
+    if (!L.val32) {
+      HB_TRY(dev_alloc((void**)&L.val32, sizeof(float) * kSlots * L.pitch, &P->bytes));
+      const int64_t cnt = (int64_t)kSlots * L.pitch;
+      k_convert<float, double><<<grid_for(c, cnt, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.val,
+                                                                                            (int)cnt);
+      HB_CK(cudaGetLastError());
+    }
+    if (!L.r32) {
+      HB_TRY(dev_alloc((void**)&L.r32, sizeof(float) * L.pitch, &P->bytes));
+      HB_TRY(dev_alloc((void**)&L.x32, sizeof(float) * L.pitch, &P->bytes));
+      HB_CK(cudaMemsetAsync(L.r32, 0, sizeof(float) * L.pitch, c->stream));
+      HB_CK(cudaMemsetAsync(L.x32, 0, sizeof(float) * L.pitch, c->stream));
+    }
+  }
+  return HPCG_B200_OK;
+}
+
+// ComputeMG_ref.cpp:39-63 with FP32 values, vectors and arithmetic.
+int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
+  Level& L = p->lev[l];
+  Context* c = p->ctx;
+  HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, true, false)));
+  if (l + 1 < p->nlev) {
+    Level& C = p->lev[l + 1];
+    k_restrict<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.col, L.pitch, r,
+                                                                                        x, L.f2c, C.r32, C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(mg32_level(p, l + 1, C.r32, C.x32));
+    k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x32, x, C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, false, false)));
+  }
+  return HPCG_B200_OK;
+}
+
+// Flexible PCG in FP64 around the FP32 V-cycle: z = widen(MG32(narrow(r))),
+// beta = r'(z - z_prev) / r_prev'z_prev (Polak-Ribiere), everything else as CG.cpp.
+int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, double* normr_out,
+                 double* normr0_out) {
+  HB_TRY(ensure_f32(P));
+  Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const int n = L.n;
+  const int nb = red_blocks(c, n);
+  const int gv = grid_for(c, n, kThreads, kPerSm);
+  k_spmv<double, false><<<gv, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->x, P->Ap, n, nullptr);
+  k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, P->b, -1.0, P->Ap, P->r, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinNormr));
+  HB_TRY(read_scalars(c));
+  double normr = std::sqrt(c->scal_host->normr2);
+  const double normr0 = normr;
+  *niters = 0;
+  for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
+    k_convert<float, double><<<gv, kThreads, 0, c->stream>>>(L.r32, P->r, n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(mg32_level(P, 0, L.r32, L.x32));
+    k_convert<double, float><<<gv, kThreads, 0, c->stream>>>(P->z, L.x32, n);
+    HB_CK(cudaGetLastError());
+    if (k == 1) {
+      k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);
+      HB_CK(cudaGetLastError());
+      HB_TRY(finalize(c, nb, kFinRtzFirst));
+      HB_CK(cudaMemcpyAsync(P->p, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      k_dot<true><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, P->zprev, c->partials);
+      HB_CK(cudaGetLastError());
+      HB_TRY(finalize(c, nb, kFinFlex));
+      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);
+      HB_CK(cudaGetLastError());
+    }
+    HB_CK(cudaMemcpyAsync(P->zprev, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    k_spmv<double, true><<<nb, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->p, P->Ap, n, c->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize(c, nb, kFinPap));
+    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize(c, nb, kFinNormr));
+    HB_TRY(read_scalars(c));
+    normr = std::sqrt(c->scal_host->normr2);
+    *niters = k;
+  }
+  *normr_out = normr;
+  *normr0_out = normr0;
+  return HPCG_B200_OK;
+}
+
+}  // namespace
+
+// natural-order src (host or device) -> colour-order device dst
+int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
+  const Level& L = p->lev[level];
+  Context* c = p->ctx;
+  const double* s = src;
+  if (!is_device_ptr(src)) {
+    HB_TRY(ensure_stage(c, L.n));
+    HB_CK(cudaMemcpyAsync(c->stage[0], src, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
+    s = c->stage[0];
+  }
+  k_gather<double><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(dst, s, L.new2old, L.n);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+// colour-order device src -> natural-order dst (host or device); synchronises
+int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
+  const Level& L = p->lev[level];
+  Context* c = p->ctx;
+  const bool dev = is_device_ptr(dst);
+  double* d = dst;
+  if (!dev) {
+    HB_TRY(ensure_stage(c, L.n));
+    d = c->stage[1];
+  }
+  k_gather<double><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n);
+  HB_CK(cudaGetLastError());
+  if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * L.n, cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  return HPCG_B200_OK;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+namespace {
+
+// A vector argument of the standalone routines as a device pointer: device
+// memory is used in place, host memory is staged into stage[slot].
+int device_view(Context* c, const double* v, int n, int slot, const double** out) {
+  if (is_device_ptr(v)) {
+    *out = v;
+    return HPCG_B200_OK;
+  }
+  HB_TRY(ensure_stage(c, (size_t)n));
+  HB_CK(cudaMemcpyAsync(c->stage[slot], v, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  *out = c->stage[slot];
+  return HPCG_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hpcg_b200_spmv(hpcg_b200_problem* p, const double* x, double* y) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!x || !y) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  const Level& L = p->lev[0];
+  Context* c = p->ctx;
+  HB_TRY(load_vector(p, 0, x, p->p));
+  k_spmv<double, false><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, p->p,
+                                                                                        p->Ap, L.n, nullptr);
+  HB_CK(cudaGetLastError());
+  return store_vector(p, 0, p->Ap, y);
+}
+
+int hpcg_b200_symgs(hpcg_b200_problem* p, const double* r, double* x) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!r || !x) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  HB_TRY(load_vector(p, 0, r, p->r));
+  HB_TRY(load_vector(p, 0, x, p->x));
+  HB_TRY(symgs_level(p, 0, p->r, p->x, false));
+  return store_vector(p, 0, p->x, x);
+}
+
+int hpcg_b200_mg(hpcg_b200_problem* p, const double* r, double* x) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!r || !x) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  HB_TRY(load_vector(p, 0, r, p->r));
+  HB_TRY(mg_level(p, 0, p->r, p->z));
+  return store_vector(p, 0, p->z, x);
+}
+
+int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
+                 int do_preconditioning, int* niters, double* normr, double* normr0, double* times) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  HB_TRY(load_vector(p, 0, b, p->b));
+  HB_TRY(load_vector(p, 0, x, p->x));
+  HB_TRY(run_cg(p, max_iter, tolerance, do_preconditioning != 0, niters, normr, normr0, times));
+  return store_vector(p, 0, p->x, x);
+}
+
+int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
+                       int* niters, double* normr, double* normr0) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  HB_TRY(load_vector(p, 0, b, p->b));
+  HB_TRY(load_vector(p, 0, x, p->x));
+  HB_TRY(run_cg_mixed(p, max_iter, tolerance, niters, normr, normr0));
+  return store_vector(p, 0, p->x, x);
+}
+
+int hpcg_b200_dot(int n, const double* x, const double* y, double* result) {
+  if (!x || !y || !result || n < 0) return HPCG_B200_ERR_ARG;
+  Context* c = current_context();
+  if (!c) return HPCG_B200_ERR_CUDA;
+  if (n == 0) {
+    *result = 0.0;
+    return HPCG_B200_OK;
+  }
+  const double *dx, *dy;
+  HB_TRY(device_view(c, x, n, 0, &dx));
+  if (y == x) dy = dx;
+  else HB_TRY(device_view(c, y, n, 1, &dy));
+  const int nb = red_blocks(c, n);
+  k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, dx, dy, nullptr, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinStore, &c->scal->tmp));
+  HB_TRY(read_scalars(c));
+  *result = c->scal_host->tmp;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_waxpby(int n, double alpha, const double* x, double beta, const double* y, double* w) {
+  if (!x || !y || !w || n < 0) return HPCG_B200_ERR_ARG;
+  Context* c = current_context();
+  if (!c) return HPCG_B200_ERR_CUDA;
+  if (n == 0) return HPCG_B200_OK;
+  const double *dx, *dy;
+  HB_TRY(device_view(c, x, n, 0, &dx));
+  if (y == x) dy = dx;
+  else HB_TRY(device_view(c, y, n, 1, &dy));
+  const bool wdev = is_device_ptr(w);
+  if (!wdev) HB_TRY(ensure_stage(c, (size_t)n));
+  double* dw = wdev ? w : c->stage[2];
+  k_waxpby<false><<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, alpha, dx, beta, dy, dw, nullptr);
+  HB_CK(cudaGetLastError());
+  if (!wdev) HB_CK(cudaMemcpyAsync(w, dw, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_residual(int n, const double* v1, const double* v2, double* residual) {
+  if (!v1 || !v2 || !residual || n < 0) return HPCG_B200_ERR_ARG;
+  Context* c = current_context();
+  if (!c) return HPCG_B200_ERR_CUDA;
+  if (n == 0) {
+    *residual = 0.0;
+    return HPCG_B200_OK;
+  }
+  const double *a, *b;
+  HB_TRY(device_view(c, v1, n, 0, &a));
+  HB_TRY(device_view(c, v2, n, 1, &b));
+  const int nb = red_blocks(c, n);
+  k_maxdiff<<<nb, kThreads, 0, c->stream>>>(n, a, b, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinMax, &c->scal->tmp));
+  HB_TRY(read_scalars(c));
+  *residual = c->scal_host->tmp;
+  return HPCG_B200_OK;
+}
+
+}  // extern "C"

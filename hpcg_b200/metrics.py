@@ -1,0 +1,101 @@
+"""HPCG work models used to turn timings into GFLOP/s and GB/s.
+
+* ``hpcg_flops`` -- the reference's FLOP model, src/ReportResults.cpp:75-99.
+* ``hpcg_model_bytes`` -- the reference's read+write model, src/ReportResults.cpp:101-136.
+* ``compulsory_bytes`` -- the bytes one CG iteration must move between HBM and
+  the SMs when each kernel streams its matrix rows once (the roofline numerator
+  of the whole iteration).
+* ``gs_phase_bytes`` -- the algorithmic bytes of one Gauss-Seidel colour phase
+  (the roofline numerator of the dominant kernel).
+
+All sizes follow the generated problem: level l of an (nx, ny, nz) grid has
+(nx>>l)(ny>>l)(nz>>l) rows and (3nx_l-2)(3ny_l-2)(3nz_l-2) nonzeros.
+"""
+from __future__ import annotations
+
+SLOTS = 27
+
+
+def level_sizes(nx, ny, nz, nlevels=4):
+    """[(rows, nnz)] per level."""
+    out = []
+    for l in range(nlevels):
+        a, b, c = nx >> l, ny >> l, nz >> l
+        out.append((a * b * c, (3 * a - 2) * (3 * b - 2) * (3 * c - 2)))
+    return out
+
+
+def hpcg_flops(nx, ny, nz, iters, sets=1, nlevels=4):
+    """ReportResults.cpp:75-98: fnops for `sets` CG sets of `iters` iterations
+    (one preamble per set), 1 pre- and 1 post-smoothing step per level."""
+    lv = level_sizes(nx, ny, nz, nlevels)
+    nrow, nnz = lv[0]
+    fniters = sets * iters
+    f = (3.0 * fniters + sets) * 2.0 * nrow        # ddot
+    f += (3.0 * fniters + sets) * 2.0 * nrow       # waxpby
+    f += (fniters + sets) * 2.0 * nnz              # spmv
+    for l in range(nlevels - 1):
+        f += fniters * (4.0 + 2.0 + 4.0) * lv[l][1]  # pre-smoother, fine residual, post-smoother
+    f += fniters * 4.0 * lv[-1][1]                 # coarsest SYMGS
+    return f
+
+
+def hpcg_model_bytes(nx, ny, nz, iters, sets=1, nlevels=4):
+    """ReportResults.cpp:101-136: reads + writes of the reference's byte model."""
+    lv = level_sizes(nx, ny, nz, nlevels)
+    nrow, nnz = lv[0]
+    d, i = 8.0, 4.0
+    fniters = sets * iters
+    rd = (3.0 * fniters + sets) * 2.0 * nrow * d
+    wr = (3.0 * fniters + sets) * d
+    rd += (3.0 * fniters + sets) * 2.0 * nrow * d
+    wr += (3.0 * fniters + sets) * nrow * d
+    rd += (fniters + sets) * (nnz * (d + i) + nrow * d)
+    wr += (fniters + sets) * nrow * d
+    for l in range(nlevels - 1):
+        n_l, z_l = lv[l]
+        rd += fniters * (2.0 * z_l * (d + i) + n_l * d)  # pre-smoother
+        wr += fniters * n_l * d
+        rd += fniters * (z_l * (d + i) + n_l * d)        # fine residual
+        wr += fniters * z_l * d
+        rd += fniters * (2.0 * z_l * (d + i) + n_l * d)  # post-smoother
+        wr += fniters * z_l * d
+    n_l, z_l = lv[-1]
+    rd += fniters * (2.0 * z_l * (d + i) + n_l * d)
+    wr += fniters * n_l * d
+    return rd + wr
+
+
+def compulsory_bytes(nx, ny, nz, nlevels=4, vb=8):
+    """HBM bytes of one CG iteration when every matrix row is streamed once per use:
+
+        sum_{l < L-1} [4.125 M_l + 13.625 N_l vb] + 2 M_{L-1} + 6 N_{L-1} vb + 12 nnz_0 + 136 N_0
+
+    with M_l = nnz_l (vb + 4) (values + int32 columns). Per MG level: four
+    Gauss-Seidel sweeps over the matrix plus the residual at the 1/8 injected
+    rows (4.125 M_l) and the vector traffic of the sweeps, restriction and
+    prolongation (13.625 N_l vb); the coarsest level does one symmetric sweep;
+    the top level adds the CG SpMV (12 nnz_0) and 17 FP64 vector passes of the CG
+    updates and dots (136 N_0). vb = 4 gives the FP32 V-cycle."""
+    lv = level_sizes(nx, ny, nz, nlevels)
+    b = 0.0
+    for l in range(nlevels - 1):
+        n_l, z_l = lv[l]
+        b += 4.125 * z_l * (vb + 4) + 13.625 * n_l * vb
+    n_l, z_l = lv[-1]
+    b += 2.0 * z_l * (vb + 4) + 6.0 * n_l * vb
+    n0, z0 = lv[0]
+    b += 12.0 * z0 + 136.0 * n0
+    return b
+
+
+def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8):
+    """Algorithmic bytes of Gauss-Seidel colour phases that together updated
+    `rows_in_phase` rows of a level with `rows_in_level` rows, per phase:
+    27 ELL slots (value + int32 column) and the right-hand side read, x written,
+    for every row of the colour; and x of the seven other colours read once
+    (each row of a colour neighbours all of them). For rows_in_phase = R summed
+    over launches of one colour each, the other-colour reads are 7 R vb (the
+    colours hold an eighth of the rows each)."""
+    per_row = SLOTS * (vb + 4) + 2 * vb
+    return rows_in_phase * per_row + 7.0 * rows_in_phase * vb

@@ -1,0 +1,179 @@
+/*
+ * hpcg_b200 -- C ABI of the B200 (sm_100a) implementation of the HPCG 3.1
+ * preconditioned-CG path.
+ *
+ * Every entry point replaces one optimisable routine of the reference and is
+ * called from the drop-in translation unit hpcg_b200/dropin/hpcg_dropin.cpp,
+ * which keeps the reference's C++ signatures. Conventions:
+ *
+ *  - Every function returns an int status: 0 (HPCG_B200_OK) on success, a
+ *    positive HPCG_B200_ERR_* code otherwise, like the reference's routines
+ *    (callers such as src/main.cpp:190 only log non-zero codes). Nothing aborts.
+ *  - Vectors are passed as plain double pointers in the reference's natural row
+ *    order (row = (iz*ny + iy)*nx + ix). A pointer may be host memory (pageable or
+ *    pinned) or device memory of the problem's GPU; the library detects which.
+ *    Host results are complete when the call returns (calls synchronise, since the
+ *    reference times them with a host clock, src/mytimer.cpp).
+ *  - Internally the matrix is device-resident in an 8-colour order; vectors are
+ *    permuted on the way in and out.
+ */
+#ifndef HPCG_B200_H
+#define HPCG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPCG_B200_OK 0
+#define HPCG_B200_ERR_CUDA 1        /* a CUDA runtime call failed */
+#define HPCG_B200_ERR_ARG 2         /* null pointer, bad size or mismatched lengths */
+#define HPCG_B200_ERR_UNSUPPORTED 3 /* matrix is not a 27-point stencil over its grid, or grid not coarsenable */
+#define HPCG_B200_ERR_NOMEM 4       /* device memory exhausted (or the configured budget exceeded) */
+#define HPCG_B200_ERR_HANDLE 5      /* null or corrupted problem handle */
+#define HPCG_B200_ERR_TIMEOUT 6     /* a bounded device-side wait gave up */
+
+/* Gauss-Seidel orderings */
+#define HPCG_B200_SYMGS_COLOUR 0    /* 8-colour sweep (the performance path) */
+#define HPCG_B200_SYMGS_NATURAL 1   /* level-scheduled natural order: ComputeSYMGS_ref's operator exactly */
+
+typedef struct hpcg_b200_problem hpcg_b200_problem; /* opaque; the drop-in keeps it in A.optimizationData */
+
+/*
+ * One level of the multigrid hierarchy, as the reference's structures hold it
+ * (src/SparseMatrix.hpp:39-76, src/MGData.hpp:28-40, src/Geometry.hpp:50-74).
+ */
+typedef struct hpcg_b200_level_desc {
+  int nx, ny, nz;                         /* Geometry::nx/ny/nz of this level */
+  int nrow;                               /* SparseMatrix::localNumberOfRows */
+  int ncol;                               /* SparseMatrix::localNumberOfColumns (== nrow, one process) */
+  const char* nonzeros_in_row;            /* SparseMatrix::nonzerosInRow */
+  const int* const* mtx_ind_l;            /* SparseMatrix::mtxIndL */
+  const double* const* matrix_values;     /* SparseMatrix::matrixValues */
+  const int* f2c;                         /* MGData::f2cOperator (NULL on the coarsest level) */
+} hpcg_b200_level_desc;
+
+/* ---- setup ------------------------------------------------------------- */
+
+/* Replaces OptimizeProblem (src/OptimizeProblem.cpp:37). Builds the device
+ * hierarchy from the reference's host structures: `levels[0]` is the fine
+ * matrix A, levels[l+1] is levels[l]'s A.Ac. Checks that every row holds only
+ * 27-point-stencil neighbours of its grid point. */
+int hpcg_b200_optimize(const hpcg_b200_level_desc* levels, int nlevels, int device, hpcg_b200_problem** out);
+
+/* Builds the same hierarchy directly on the device, as GenerateProblem_ref
+ * (src/GenerateProblem_ref.cpp:131-183) and GenerateCoarseProblem
+ * (src/GenerateCoarseProblem.cpp:71-104) would for one process, without host
+ * arrays: the route for grids whose host structures would not fit (512^3 has
+ * 3.6e9 nonzeros, beyond the reference's int local_int_t). The reference's
+ * right-hand side (b_i = 27 - nnz_i, :178) is kept on the device; read it with
+ * hpcg_b200_get_rhs. */
+int hpcg_b200_generate(int nx, int ny, int nz, int nlevels, int device, hpcg_b200_problem** out);
+
+/* Copies the problem's right-hand side (natural order) to b (host or device). */
+int hpcg_b200_get_rhs(hpcg_b200_problem* p, double* b);
+
+/* Releases everything a problem holds (the reference's DeleteMatrix never frees
+ * optimizationData, src/SparseMatrix.hpp:151-183, so the drop-in calls this). */
+int hpcg_b200_free(hpcg_b200_problem* p);
+
+/* Replaces OptimizeProblemMemoryUse (src/OptimizeProblem.cpp:103): bytes of device
+ * memory the problem retains. Returns 0.0 for a null handle. */
+double hpcg_b200_memory_use(const hpcg_b200_problem* p);
+
+/* Re-reads the fine-level diagonal after the host changed it through
+ * ReplaceMatrixDiagonal (src/SparseMatrix.hpp:139; TestCG.cpp:79 and :114 do).
+ * `diagonal` holds one value per row in natural order. */
+int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal);
+
+/* Overwrites every value of one level, keeping its sparsity. values27 holds 27
+ * values per row, rows in natural order, value k of a row belonging to the
+ * stencil direction k = (sz+1)*9 + (sy+1)*3 + (sx+1) (the reference's entry
+ * order, GenerateProblem_ref.cpp:152-172, with directions that leave the grid
+ * present and ignored). */
+int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27);
+
+/* Selects the SYMGS ordering used by hpcg_b200_symgs / _mg / _cg. */
+int hpcg_b200_set_symgs_mode(hpcg_b200_problem* p, int mode);
+
+/* ---- kernels (all vectors natural order, host or device memory) --------- */
+
+/* y = A x on level 0. Replaces ComputeSPMV (src/ComputeSPMV.cpp:40; ComputeSPMV_ref.cpp:47-72). */
+int hpcg_b200_spmv(hpcg_b200_problem* p, const double* x, double* y);
+
+/* One symmetric Gauss-Seidel step on x with right-hand side r. Replaces
+ * ComputeSYMGS (src/ComputeSYMGS.cpp:50; ComputeSYMGS_ref.cpp:54-103). */
+int hpcg_b200_symgs(hpcg_b200_problem* p, const double* r, double* x);
+
+/* x = V-cycle(r). Replaces ComputeMG (src/ComputeMG.cpp:33; ComputeMG_ref.cpp:39-63). */
+int hpcg_b200_mg(hpcg_b200_problem* p, const double* r, double* x);
+
+/* result = x'y over n entries. Replaces ComputeDotProduct
+ * (src/ComputeDotProduct.cpp:41; ComputeDotProduct_ref.cpp:46-80). Deterministic. */
+int hpcg_b200_dot(int n, const double* x, const double* y, double* result);
+
+/* w = alpha x + beta y. Replaces ComputeWAXPBY (src/ComputeWAXPBY.cpp:42; ComputeWAXPBY_ref.cpp:42-70). */
+int hpcg_b200_waxpby(int n, double alpha, const double* x, double beta, const double* y, double* w);
+
+/* residual = max_i |v1_i - v2_i|. Replaces ComputeResidual (src/ComputeResidual.cpp:49-89). */
+int hpcg_b200_residual(int n, const double* v1, const double* v2, double* residual);
+
+/* Preconditioned CG. Replaces CG (src/CG.cpp:59-143): same arguments and
+ * stopping rule (k <= max_iter && normr/normr0 > tolerance). times (may be
+ * NULL) accumulates like the reference's times[0..5]. */
+int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
+                 int do_preconditioning, int* niters, double* normr, double* normr0, double* times);
+
+/* ---- changed form 1: FP32 V-cycle inside FP64 flexible PCG --------------- */
+
+/* As hpcg_b200_cg, but the V-cycle (values, vectors, smoother, transfers) runs
+ * in FP32 and beta is the flexible Polak-Ribiere form; the SpMV, dots, alpha,
+ * beta and x/r updates stay FP64. No reference counterpart (changed form). */
+int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
+                       int* niters, double* normr, double* normr0);
+
+/* ---- inspection (tests) -------------------------------------------------- */
+
+/* Rows, padded pitch and colour-block boundaries (9 ints) of one level. */
+int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64_t* pitch, int* colour_start);
+
+/* Copies one level's device layout to host: new2old[nrow] (colour row -> natural
+ * row), cols[27*pitch] and vals[27*pitch] (slot-major, colour order), f2c[nrow of
+ * next level] (colour order, NULL allowed). */
+int hpcg_b200_export_level(const hpcg_b200_problem* p, int level, int* new2old, int* cols, double* vals,
+                           int* f2c);
+
+/* The row order the library uses for an (nx, ny, nz) grid, computed on the host
+ * (no GPU needed): new2old[q] = natural row of colour-order row q, and
+ * colour_start[s]..colour_start[s+1] the rows of the s-th colour swept (9 ints).
+ * The colours are the parity classes of (ix, iy, iz), an 8-colouring of the
+ * 27-point stencil (the greedy colouring of src/OptimizeProblem.cpp:50-96 finds
+ * the same classes); the class of the injected points (all coordinates even,
+ * src/GenerateCoarseProblem.cpp:71-82) is swept last. */
+int hpcg_b200_colour_permutation(int nx, int ny, int nz, int* new2old, int* colour_start);
+
+/* ---- measurement ---------------------------------------------------------- */
+
+/* The CUDA stream (a cudaStream_t) the library launches on for `device`. All
+ * work of an entry point is ordered on it; callers may record events on it. */
+void* hpcg_b200_stream(int device);
+
+/* Launch profiler: with enable != 0, CUDA events are recorded around each launch
+ * of the timed kernel classes; enabling resets the totals. Kinds:
+ * 0 Gauss-Seidel colour phase on level 0 (all slots), 1 first forward sweep on
+ * level 0, 2 CG SpMV on level 0, 3 residual+restriction from level 0. */
+#define HPCG_B200_PROF_GS_FULL 0
+#define HPCG_B200_PROF_GS_FIRST 1
+#define HPCG_B200_PROF_SPMV 2
+#define HPCG_B200_PROF_RESTRICT 3
+int hpcg_b200_profile(int device, int enable);
+int hpcg_b200_profile_read(int device, int kind, double* total_ms, int64_t* launches, int64_t* rows);
+
+/* The CUDA error string of the last failing call on this thread ("" if none). */
+const char* hpcg_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPCG_B200_H */

@@ -1,0 +1,462 @@
+"""Parity of the CUDA path with the oracle, through the C ABI (needs a B200).
+
+Tolerances. The row kernels (SpMV, Gauss-Seidel, restriction, prolongation,
+WAXPBY) use the reference's operation order without contraction, so their
+results are compared bit for bit (np.array_equal, which counts -0.0 == 0.0).
+Dot products reduce in a fixed tree instead of a serial loop: relative 1e-13.
+CG residual histories: relative 1e-10 while the scaled residual is above
+1e-12 (below that it is rounding noise), as the north star states.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def levels_of(P):
+    return [dict(nx=L.nx, ny=L.ny, nz=L.nz, nnz=L.nnz, cols=L.cols, vals=L.vals, f2c=L.f2c) for L in P.levels]
+
+
+def perms_of(binding, P):
+    return [binding.colour_permutation(L.nx, L.ny, L.nz)[0] for L in P.levels]
+
+
+@pytest.fixture(scope="module")
+def case16(oracle, binding):
+    P = oracle.generate(16)
+    D = binding.Problem.optimize(levels_of(P))
+    perms = perms_of(binding, P)
+    yield P, D, perms, oracle.permute(P.levels, perms)
+    D.free()
+
+
+@pytest.fixture(scope="module")
+def case32(oracle, binding):
+    P = oracle.generate(32)
+    D = binding.Problem.optimize(levels_of(P))
+    perms = perms_of(binding, P)
+    yield P, D, perms, oracle.permute(P.levels, perms)
+    D.free()
+
+
+def hist_close(a, b, rel=1e-10):
+    a, b = np.asarray(a), np.asarray(b)
+    big = np.abs(b) > 1e-12
+    assert np.all(np.abs(a[big] - b[big]) <= rel * np.abs(b[big])), (a, b)
+    assert np.all(np.abs(a[~big]) <= 1e-11)
+
+
+# ---------------------------------------------------------------------------
+# layout
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (16, 24, 32), (24, 24, 24)])
+def test_layout_matches_reference_structures(oracle, binding, dims):
+    P = oracle.generate(*dims)
+    D = binding.Problem.optimize(levels_of(P))
+    try:
+        for l, L in enumerate(P.levels):
+            E = D.export_level(l)
+            n2o, starts = binding.colour_permutation(L.nx, L.ny, L.nz)
+            assert np.array_equal(E["new2old"], n2o) and np.array_equal(E["starts"], starts)
+            o2n = np.empty_like(n2o)
+            o2n[n2o] = np.arange(L.n, dtype=np.int32)
+            cols, vals = L.dense_rows()
+            exp_c = np.full((27, L.n), L.n, np.int32)
+            exp_v = np.zeros((27, L.n))
+            for i in range(L.n):
+                q = o2n[i]
+                iz, rem = divmod(i, L.nx * L.ny)
+                iy, ix = divmod(rem, L.nx)
+                for j in range(L.nnz[i]):
+                    c = cols[i, j]
+                    cz, r2 = divmod(c, L.nx * L.ny)
+                    cy, cx = divmod(r2, L.nx)
+                    k = (cz - iz + 1) * 9 + (cy - iy + 1) * 3 + (cx - ix + 1)
+                    exp_c[k, q] = o2n[c]
+                    exp_v[k, q] = vals[i, j]
+            assert np.array_equal(E["cols"][:, : L.n], exp_c)
+            assert np.array_equal(E["vals"][:, : L.n], exp_v)
+            if L.f2c is not None:
+                nc = P.levels[l + 1]
+                c_n2o = binding.colour_permutation(nc.nx, nc.ny, nc.nz)[0]
+                assert np.array_equal(E["f2c"], o2n[L.f2c[c_n2o]])
+    finally:
+        D.free()
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (16, 24, 32), (24, 24, 24), (32, 32, 32)])
+def test_device_generator_equals_optimize(oracle, binding, dims):
+    """hpcg_b200_generate builds on the device what OptimizeProblem builds from
+    the reference's host structures (GenerateProblem_ref + GenerateCoarseProblem)."""
+    P = oracle.generate(*dims)
+    A = binding.Problem.optimize(levels_of(P))
+    G = binding.Problem.generate(*dims)
+    try:
+        for l, L in enumerate(P.levels):
+            a, g = A.export_level(l), G.export_level(l)
+            n = a["n"]
+            for key in ("new2old", "starts"):
+                assert np.array_equal(a[key], g[key])
+            assert np.array_equal(a["cols"][:, :n], g["cols"][:, :n])
+            assert np.array_equal(a["vals"][:, :n], g["vals"][:, :n])
+            if a["f2c"] is not None:
+                assert np.array_equal(a["f2c"], g["f2c"])
+        assert np.array_equal(G.get_rhs(), P.b)
+        assert G.memory_use() > 0
+    finally:
+        A.free()
+        G.free()
+
+
+# ---------------------------------------------------------------------------
+# row kernels: bitwise
+# ---------------------------------------------------------------------------
+
+def test_spmv_bitwise(oracle, case32):
+    P, D, _, _ = case32
+    rng = np.random.default_rng(11)
+    for x in (rng.random(P.levels[0].n), rng.standard_normal(P.levels[0].n), P.xexact):
+        y = np.zeros_like(x)
+        assert D.ComputeSPMV(x, y) == 0
+        assert np.array_equal(y, oracle.spmv(P.levels[0], x))
+    # A * xexact = b exactly (b_i = 27 - nnz_i, GenerateProblem_ref.cpp:178)
+    y = np.zeros(P.levels[0].n)
+    D.ComputeSPMV(P.xexact, y)
+    assert np.array_equal(y, P.b)
+
+
+def test_spmv_matches_reference_golden(oracle, case16):
+    P, D, _, _ = case16
+    g = np.load(os.path.join(GOLD, "golden_16.npz"))
+    y = np.zeros(16 ** 3)
+    D.ComputeSPMV(g["x_seed"], y)
+    assert np.array_equal(y, g["spmv"])
+
+
+def test_symgs_colour_bitwise(oracle, binding, case32):
+    P, D, perms, PL = case32
+    rng = np.random.default_rng(12)
+    r, x0 = rng.standard_normal(P.levels[0].n), rng.standard_normal(P.levels[0].n)
+    x = x0.copy()
+    D.set_symgs_mode(binding.SYMGS_COLOUR)
+    D.ComputeSYMGS(r, x)
+    p0 = perms[0]
+    exp = np.empty_like(x)
+    exp[p0] = oracle.symgs(PL[0], r[p0], x0[p0])
+    assert np.array_equal(x, exp)
+
+
+def test_symgs_natural_is_reference_bitwise(oracle, binding, case16):
+    """The level-scheduled mode reproduces ComputeSYMGS_ref's natural-order sweep."""
+    P, D, _, _ = case16
+    g = np.load(os.path.join(GOLD, "golden_16.npz"))
+    D.set_symgs_mode(binding.SYMGS_NATURAL)
+    try:
+        x = g["x_seed"].copy()
+        D.ComputeSYMGS(g["b"], x)
+        assert np.array_equal(x, g["symgs"])
+        rng = np.random.default_rng(13)
+        r, x0 = rng.standard_normal(16 ** 3), rng.standard_normal(16 ** 3)
+        x = x0.copy()
+        D.ComputeSYMGS(r, x)
+        assert np.array_equal(x, oracle.symgs(P.levels[0], r, x0))
+    finally:
+        D.set_symgs_mode(binding.SYMGS_COLOUR)
+
+
+def test_mg_colour_bitwise(oracle, binding, case32):
+    P, D, perms, PL = case32
+    r = np.random.default_rng(14).standard_normal(P.levels[0].n)
+    z = np.zeros_like(r)
+    D.ComputeMG(r, z)
+    p0 = perms[0]
+    exp = np.empty_like(z)
+    exp[p0] = oracle.mg(PL, r[p0])
+    assert np.array_equal(z, exp)
+
+
+def test_mg_natural_is_reference_bitwise(oracle, binding, case16):
+    P, D, _, _ = case16
+    g = np.load(os.path.join(GOLD, "golden_16.npz"))
+    D.set_symgs_mode(binding.SYMGS_NATURAL)
+    try:
+        z = np.zeros(16 ** 3)
+        D.ComputeMG(g["x_seed"], z)
+        assert np.array_equal(z, g["mg"])
+    finally:
+        D.set_symgs_mode(binding.SYMGS_COLOUR)
+
+
+def test_mg_repeat_is_identical(case32):
+    """Stale work vectors never leak into a V-cycle: two calls give the same bits."""
+    P, D, _, _ = case32
+    rng = np.random.default_rng(15)
+    r1, r2 = rng.standard_normal(P.levels[0].n), rng.standard_normal(P.levels[0].n)
+    a = np.zeros_like(r1)
+    D.ComputeMG(r1, a)
+    b_ = np.zeros_like(r1)
+    D.ComputeMG(r2, b_)
+    c = np.zeros_like(r1)
+    D.ComputeMG(r1, c)
+    assert np.array_equal(a, c)
+
+
+# ---------------------------------------------------------------------------
+# vector routines
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("n", [1, 7, 1000, 32768, 1 << 20])
+def test_dot_waxpby_residual(oracle, binding, n):
+    rng = np.random.default_rng(n)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    d = binding.ComputeDotProduct(n, x, y)
+    ref = oracle.dot(x, y)
+    assert abs(d - ref) <= 1e-13 * max(abs(ref), np.abs(x * y).sum() * 1e-3)
+    assert binding.ComputeDotProduct(n, x, y) == d  # deterministic
+    assert binding.ComputeDotProduct(n, x, x) == pytest.approx(oracle.dot(x, x), rel=1e-13)
+    for alpha, beta in ((1.0, 2.5), (0.75, 1.0), (-1.5, 0.25), (1.0, 0.0)):
+        w = np.zeros(n)
+        binding.ComputeWAXPBY(n, alpha, x, beta, y, w)
+        assert np.array_equal(w, oracle.waxpby(alpha, x, beta, y))
+    assert binding.ComputeResidual(n, x, y) == oracle.residual(x, y)
+
+
+def test_zero_length_and_aliasing(binding):
+    x = np.arange(5.0)
+    assert binding.ComputeDotProduct(0, x, x) == 0.0
+    w = x.copy()
+    binding.ComputeWAXPBY(5, 2.0, w, 1.0, w, w)  # in place, x == y == w
+    assert np.array_equal(w, 3.0 * x)
+
+
+def test_device_pointers_match_host(oracle, binding, case32):
+    import torch
+    P, D, _, _ = case32
+    n = P.levels[0].n
+    x = np.random.default_rng(16).standard_normal(n)
+    yh = np.zeros(n)
+    D.ComputeSPMV(x, yh)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    D.ComputeSPMV(xd, yd)
+    torch.cuda.synchronize()
+    assert np.array_equal(yd.cpu().numpy(), yh)
+    zh = np.zeros(n)
+    D.ComputeMG(x, zh)
+    zd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    D.ComputeMG(xd, zd)
+    assert np.array_equal(zd.cpu().numpy(), zh)
+    assert binding.ComputeDotProduct(n, xd, yd) == binding.ComputeDotProduct(n, x, yh)
+
+
+# ---------------------------------------------------------------------------
+# CG
+# ---------------------------------------------------------------------------
+
+def test_cg_colour_history_vs_reference_on_permuted_system(oracle, binding, case16):
+    """History against CG_ref run by the reference itself on the colour-permuted
+    hierarchy (golden_16.npz cg_hist_perm)."""
+    P, D, perms, PL = case16
+    g = np.load(os.path.join(GOLD, "golden_16.npz"))
+    ours = []
+    for k in range(1, 21):
+        x = np.zeros(16 ** 3)
+        ni, nr, nr0 = D.CG(P.b, x, k, 0.0, True)
+        assert ni == k
+        ours.append(nr / nr0)
+    hist_close(ours, g["cg_hist_perm"])
+
+
+def test_cg_colour_vs_oracle_32(oracle, case32):
+    P, D, perms, PL = case32
+    b = P.b[perms[0]]
+    for k in (1, 5, 10, 25, 50):
+        x = np.zeros(32 ** 3)
+        ni, nr, nr0 = D.CG(P.b, x, k, 0.0, True)
+        xo, nio, nro, nr0o, _ = oracle.cg(PL, b, np.zeros(32 ** 3), k, 0.0)
+        assert ni == nio == k
+        assert abs(nr0 - nr0o) <= 1e-13 * nr0o
+        hist_close([nr / nr0], [nro / nr0o])
+        xn = np.empty_like(xo)
+        xn[perms[0]] = xo
+        assert np.max(np.abs(x - xn)) <= 1e-10 * max(np.max(np.abs(xn)), 1.0)
+
+
+def test_cg_natural_is_reference(oracle, binding, case16):
+    """Natural-order SYMGS: the whole CG is CG_ref except for the dot reductions."""
+    P, D, _, _ = case16
+    g = np.load(os.path.join(GOLD, "golden_16.npz"))
+    D.set_symgs_mode(binding.SYMGS_NATURAL)
+    try:
+        ours = []
+        for k in (1, 2, 5, 10, 20):
+            x = np.zeros(16 ** 3)
+            ni, nr, nr0 = D.CG(P.b, x, k, 0.0, True)
+            ours.append(nr / nr0)
+            assert nr0 == pytest.approx(float(g["normr0"]), rel=1e-14)
+            if k == 10:
+                assert np.max(np.abs(x - g["cg_x10"])) <= 1e-12
+        hist_close(ours, g["cg_hist"][[0, 1, 4, 9, 19]])
+    finally:
+        D.set_symgs_mode(binding.SYMGS_COLOUR)
+
+
+def test_cg_tolerance_stop_and_unpreconditioned(oracle, case32):
+    P, D, perms, PL = case32
+    b = P.b[perms[0]]
+    for prec in (True, False):
+        x = np.zeros(32 ** 3)
+        ni, nr, nr0 = D.CG(P.b, x, 500, 1e-8, prec)
+        _, nio, nro, nr0o, _ = oracle.cg(PL, b, np.zeros(32 ** 3), 500, 1e-8, prec)
+        assert ni == nio
+        assert nr / nr0 <= 1e-8
+
+
+def test_cg_reproducible_testnorms(case32):
+    """TestNorms (src/TestNorms.cpp:31-46) needs the scaled residual of repeated
+    sets to vary < 1e-6; the fixed reduction order makes it identical."""
+    P, D, _, _ = case32
+    vals = []
+    for _ in range(3):
+        x = np.zeros(32 ** 3)
+        ni, nr, nr0 = D.CG(P.b, x, 50, 0.0, True)
+        vals.append(nr / nr0)
+    assert vals[0] == vals[1] == vals[2]
+
+
+def test_testcg_exaggerated_diagonal(oracle, binding):
+    """TestCG.cpp:52-123 on the device: the diagonal is rewritten through
+    ReplaceMatrixDiagonal on the host, resent with hpcg_b200_set_diagonal; CG
+    converges in <= 12 unpreconditioned and <= 2 preconditioned iterations."""
+    P = oracle.generate(32)
+    D = binding.Problem.optimize(levels_of(P))
+    try:
+        n = P.levels[0].n
+        diag = np.full(n, 26.0)
+        scale = np.full(n, 1.0e6)
+        scale[:9] = (np.arange(9) + 2) * 1.0e6
+        D.set_diagonal(diag * scale)
+        b = P.b * scale
+        counts = []
+        for prec in (False, True):
+            for _ in range(2):
+                x = np.zeros(n)
+                ni, nr, nr0 = D.CG(b, x, 50, 1e-12, prec)
+                counts.append(ni)
+        assert max(counts[:2]) <= 12 and max(counts[2:]) <= 2, counts
+        D.set_diagonal(diag)
+        y = np.zeros(n)
+        D.ComputeSPMV(P.xexact, y)
+        assert np.array_equal(y, P.b)
+    finally:
+        D.free()
+
+
+def test_symmetry_departure(binding, case32):
+    """TestSymmetry.cpp:60-138 with the library's SpMV, MG and dot."""
+    P, D, _, _ = case32
+    n = P.levels[0].n
+    rng = np.random.default_rng(17)
+    x, y = rng.random(n) + 1.0, rng.random(n) + 1.0
+    eps = np.finfo(float).eps
+    xn, yn = binding.ComputeDotProduct(n, x, x), binding.ComputeDotProduct(n, y, y)
+    z = np.zeros(n)
+    D.ComputeSPMV(y, z)
+    xtAy = binding.ComputeDotProduct(n, x, z)
+    D.ComputeSPMV(x, z)
+    ytAx = binding.ComputeDotProduct(n, y, z)
+    assert abs(xtAy - ytAx) / ((xn * 52 * yn + yn * 52 * xn) * eps) <= 1.0
+    D.ComputeMG(y, z)
+    xtMy = binding.ComputeDotProduct(n, x, z)
+    D.ComputeMG(x, z)
+    ytMx = binding.ComputeDotProduct(n, y, z)
+    assert abs(xtMy - ytMx) / ((xn * 52 * yn + yn * 52 * xn) * eps) <= 1.0
+
+
+def test_mixed_precision_vs_oracle(oracle, binding, case32):
+    P, D, perms, PL = case32
+    x = np.zeros(32 ** 3)
+    ni, nr, nr0 = D.CG_mixed(P.b, x, 200, 1e-9)
+    xo, nio, nro, nr0o, _ = oracle.cg_mixed(PL, P.b[perms[0]], np.zeros(32 ** 3), 200, 1e-9)
+    assert abs(ni - nio) <= 1
+    assert nr / nr0 <= 1e-9
+    x64 = np.zeros(32 ** 3)
+    D.CG(P.b, x64, 200, 1e-9, True)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) <= 1e-7
+
+
+# ---------------------------------------------------------------------------
+# larger grids: size-independent properties
+# ---------------------------------------------------------------------------
+
+def test_large_grid_properties(binding):
+    import torch
+    n = 192
+    D = binding.Problem.generate(n)
+    try:
+        N = n ** 3
+        b = torch.zeros(N, dtype=torch.float64, device="cuda")
+        D.get_rhs(b)
+        ones = torch.ones(N, dtype=torch.float64, device="cuda")
+        y = torch.zeros_like(ones)
+        D.ComputeSPMV(ones, y)
+        assert torch.equal(y, b)  # A * xexact = b exactly
+        g = torch.Generator(device="cuda").manual_seed(5)
+        u = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
+        v = torch.rand(N, dtype=torch.float64, device="cuda", generator=g)
+        Au, Av = torch.zeros_like(u), torch.zeros_like(v)
+        D.ComputeSPMV(u, Au)
+        D.ComputeSPMV(v, Av)
+        a, c = binding.ComputeDotProduct(N, v, Au), binding.ComputeDotProduct(N, u, Av)
+        assert abs(a - c) <= 1e-12 * abs(a)
+        x = torch.zeros(N, dtype=torch.float64, device="cuda")
+        res = []
+        for k in (1, 5, 10):
+            x.zero_()
+            ni, nr, nr0 = D.CG(b, x, k, 0.0, True)
+            res.append(nr / nr0)
+        assert res[0] > res[1] > res[2] and res[2] < 1e-3
+    finally:
+        D.free()
+
+
+# ---------------------------------------------------------------------------
+# errors come back as status codes
+# ---------------------------------------------------------------------------
+
+def test_unsupported_matrix_is_rejected(oracle, binding):
+    P = oracle.generate(16)
+    lv = levels_of(P)
+    cols = lv[0]["cols"].copy()
+    cols[5 * 27 + 2] = 4000  # not a stencil neighbour of row 5
+    lv[0] = dict(lv[0], cols=cols)
+    with pytest.raises(binding.HpcgError) as e:
+        binding.Problem.optimize(lv)
+    assert e.value.status == binding.ERR_UNSUPPORTED
+    lv = levels_of(P)
+    f2c = lv[0]["f2c"].copy()
+    f2c[3] = -1
+    lv[0] = dict(lv[0], f2c=f2c)
+    with pytest.raises(binding.HpcgError) as e:
+        binding.Problem.optimize(lv)
+    assert e.value.status == binding.ERR_ARG
+    with pytest.raises(binding.HpcgError) as e:
+        binding.Problem.generate(20, 20, 20, 4)  # 20 -> 10 -> 5 -> not halvable
+    assert e.value.status == binding.ERR_UNSUPPORTED
+
+
+def test_device_budget_gives_nomem():
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from hpcg_b200 import binding as B\n"
+            "try:\n    B.Problem.generate(64)\nexcept B.HpcgError as e:\n    print('status', e.status)\n"
+            "p = None\n") % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, HPCG_B200_DEVICE_BUDGET="1000000")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "status 4" in out.stdout
