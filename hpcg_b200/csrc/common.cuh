@@ -95,6 +95,10 @@ struct Level {
   double* x = nullptr;       // coarse solution (levels > 0), [pitch]
   float* r32 = nullptr;      // FP32 V-cycle vectors, [pitch]
   float* x32 = nullptr;
+  // kernel configuration of this level's row kernels, chosen by the autotuner
+  int gs_sched = 1;          // kernel configuration (0..3) of the Gauss-Seidel phases
+  int mv_sched = 1;          // kernel configuration of SpMV / restriction
+  bool tuned = false;
   // level-scheduled natural order (built on first use)
   int* wave_rows = nullptr;  // colour-order rows sorted by ix + 2 iy + 4 iz
   int nwaves = 0;

@@ -72,7 +72,9 @@ Context* context_for(int device) {
   c->device = device;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  // a blocking stream: ordered with work on the legacy default stream (where
+  // callers such as torch write the device vectors they pass in)
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
   if (e == cudaSuccess) e = cudaMalloc(&c->partials, sizeof(double) * kRedBlocksMax);
   if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(Scalars));
   if (e == cudaSuccess) e = cudaMemset(c->scal, 0, sizeof(Scalars));

@@ -52,21 +52,60 @@ __device__ __forceinline__ double block_max(double v) {
 // (neighbours not yet swept, and the diagonal) multiply a zero and are skipped,
 // which leaves every sum bitwise unchanged.
 // ---------------------------------------------------------------------------
-template <typename T, typename TR, bool FIRST>
-__global__ void __launch_bounds__(kThreads) k_gs_phase(const T* __restrict__ val, const int* __restrict__ col,
-                                                       int64_t pitch, const TR* __restrict__ rhs, T* x, int r0,
-                                                       int r1, uint32_t mask) {
+// Two load schedules of the same row arithmetic (results are bitwise equal):
+//  kPlain  -- loads issued as the compiler schedules the slot loop;
+//  kStaged -- all masked value/column loads issued first (27 independent loads
+//             in flight per thread), then the 27 gathers of x, then the sum; the
+//             matrix is read with evict-first hints (__ldcs) so that the stream of
+//             values and columns, read once per phase, does not push the vector
+//             out of L2.
+enum LoadSchedule : int { kPlain = 0, kStaged = 1 };
+
+// Kernel configurations the autotuner chooses from: a load schedule and the
+// minimum resident 256-thread blocks per SM (which caps registers per thread:
+// 4 -> 64, 2 -> 128, 1 -> 255).
+constexpr int kConfigs = 4;
+__host__ __device__ constexpr int cfg_sched(int cfg) { return cfg >= 2 ? kStaged : kPlain; }
+__host__ __device__ constexpr int cfg_minb(int cfg) { return cfg == 0 ? 4 : cfg == 1 ? 2 : cfg == 2 ? 1 : 2; }
+
+template <typename T, typename TR, bool FIRST, int CFG, int SCHED = cfg_sched(CFG)>
+__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* __restrict__ val, const int* __restrict__ col,
+                                                          int64_t pitch, const TR* __restrict__ rhs, T* x, int r0,
+                                                          int r1, uint32_t mask) {
   const int stride = gridDim.x * blockDim.x;
   for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride) {
     T sum = (T)rhs[q];
     T xd = (T)0;
+    if (SCHED == kStaged) {
+      T a[kSlots];
+      int cl[kSlots];
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
-      if (mask & (1u << k)) {
-        const T a = val[k * pitch + q];
-        const T xv = __ldg(x + col[k * pitch + q]);
-        sum -= a * xv;
-        if (k == kDiagSlot) xd = xv;
+      for (int k = 0; k < kSlots; ++k) {
+        if (mask & (1u << k)) {
+          a[k] = __ldcs(val + k * pitch + q);
+          cl[k] = __ldcs(col + k * pitch + q);
+        }
+      }
+      T xv[kSlots];
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k)
+        if (mask & (1u << k)) xv[k] = __ldg(x + cl[k]);
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        if (mask & (1u << k)) {
+          sum -= a[k] * xv[k];
+          if (k == kDiagSlot) xd = xv[k];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        if (mask & (1u << k)) {
+          const T a = val[k * pitch + q];
+          const T xv = __ldg(x + col[k * pitch + q]);
+          sum -= a * xv;
+          if (k == kDiagSlot) xd = xv;
+        }
       }
     }
     const T d = val[kDiagSlot * pitch + q];
@@ -101,20 +140,36 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
 
 // y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y
 // (the p'Ap of CG.cpp:119, fused).
-template <typename T, bool DOT>
-__global__ void __launch_bounds__(kThreads) k_spmv(const T* __restrict__ val, const int* __restrict__ col,
-                                                   int64_t pitch, const T* __restrict__ x, T* __restrict__ y,
-                                                   int n, double* __restrict__ partials) {
+template <typename T, bool DOT, int CFG, int SCHED = cfg_sched(CFG)>
+__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(const T* __restrict__ val, const int* __restrict__ col,
+                                                      int64_t pitch, const T* __restrict__ x, T* __restrict__ y,
+                                                      int n, double* __restrict__ partials) {
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
     T sum = (T)0;
     T xq = (T)0;
+    if (SCHED == kStaged) {
+      T a[kSlots];
+      int cl[kSlots];
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
-      const T xv = __ldg(x + col[k * pitch + q]);
-      sum += val[k * pitch + q] * xv;
-      if (k == kDiagSlot) xq = xv;
+      for (int k = 0; k < kSlots; ++k) {
+        a[k] = __ldcs(val + k * pitch + q);
+        cl[k] = __ldcs(col + k * pitch + q);
+      }
+      T xv[kSlots];
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) xv[k] = __ldg(x + cl[k]);
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) sum += a[k] * xv[k];
+      xq = xv[kDiagSlot];
+    } else {
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const T xv = __ldg(x + col[k * pitch + q]);
+        sum += val[k * pitch + q] * xv;
+        if (k == kDiagSlot) xq = xv;
+      }
     }
     y[q] = sum;
     if (DOT) acc += (double)xq * (double)sum;
@@ -128,17 +183,32 @@ __global__ void __launch_bounds__(kThreads) k_spmv(const T* __restrict__ val, co
 // Restriction fused with the residual it needs (ComputeMG_ref.cpp:49-51):
 // rc[q] = rf[f] - (A xf)[f] for f = f2c[q]; the residual is formed only at the
 // injected rows (ComputeRestriction_ref.cpp:51 reads no others).
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_restrict(const T* __restrict__ val, const int* __restrict__ col,
-                                                       int64_t pitch, const T* __restrict__ rf,
-                                                       const T* __restrict__ xf, const int* __restrict__ f2c,
-                                                       T* __restrict__ rc, int nc) {
+template <typename T, int CFG, int SCHED = cfg_sched(CFG)>
+__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* __restrict__ val, const int* __restrict__ col,
+                                                          int64_t pitch, const T* __restrict__ rf,
+                                                          const T* __restrict__ xf, const int* __restrict__ f2c,
+                                                          T* __restrict__ rc, int nc) {
   const int stride = gridDim.x * blockDim.x;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) {
     const int f = f2c[q];
     T sum = (T)0;
+    if (SCHED == kStaged) {
+      T a[kSlots];
+      int cl[kSlots];
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) sum += val[k * pitch + f] * __ldg(xf + col[k * pitch + f]);
+      for (int k = 0; k < kSlots; ++k) {
+        a[k] = __ldcs(val + k * pitch + f);
+        cl[k] = __ldcs(col + k * pitch + f);
+      }
+      T xv[kSlots];
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) xv[k] = __ldg(xf + cl[k]);
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) sum += a[k] * xv[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) sum += val[k * pitch + f] * __ldg(xf + col[k * pitch + f]);
+    }
     rc[q] = rf[f] - sum;
   }
 }
@@ -165,8 +235,8 @@ __global__ void __launch_bounds__(kThreads) k_gather(T* __restrict__ dst, const 
 // beta == 1 branches give the same bits, multiplication by 1.0 being exact).
 // NORM: partials of w'w.
 template <bool NORM>
-__global__ void __launch_bounds__(kThreads) k_waxpby(int n, double alpha, const double* __restrict__ x, double beta,
-                                                     const double* __restrict__ y, double* w,
+__global__ void __launch_bounds__(kThreads) k_waxpby(int n, double alpha, const double* x, double beta,
+                                                     const double* y, double* w,
                                                      double* __restrict__ partials) {
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
@@ -281,9 +351,9 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const 
 
 // precision conversion for the FP32 V-cycle
 template <typename TO, typename TI>
-__global__ void __launch_bounds__(kThreads) k_convert(TO* __restrict__ dst, const TI* __restrict__ src, int n) {
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (TO)src[i];
+__global__ void __launch_bounds__(kThreads) k_convert(TO* __restrict__ dst, const TI* __restrict__ src, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (TO)src[i];
 }
 
 }  // namespace hb

@@ -1,6 +1,7 @@
 // Entry points of the PCG path: SpMV, SYMGS, the V-cycle, CG and the vector
 // routines, with the host-side drivers that sequence the kernels.
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -30,19 +31,86 @@ uint32_t first_mask(const ColourGrid& g, int s) {
   return m;
 }
 
+// Resident blocks per SM of a kernel (at least 1).
+template <typename K>
+int resident(K kernel) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 1;
+  }
+  return b;
+}
+
+// Grid of a grid-stride row kernel: every SM filled once with resident blocks.
+template <typename K>
+int grid_of(Context* c, K kernel, int64_t rows) {
+  return grid_for(c, rows, kThreads, resident(kernel));
+}
+
+template <typename T, typename TR, bool FIRST, int CFG>
+void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask) {
+  auto k = k_gs_phase<T, TR, FIRST, CFG>;
+  k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask);
+}
+
+template <typename T, typename TR, bool FIRST>
+void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rhs, T* x, int r0, int r1,
+                 uint32_t mask) {
+  switch (cfg) {
+    case 0: gs_launch<T, TR, FIRST, 0>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 1: gs_launch<T, TR, FIRST, 1>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 2: gs_launch<T, TR, FIRST, 2>(c, L, val, rhs, x, r0, r1, mask); break;
+    default: gs_launch<T, TR, FIRST, 3>(c, L, val, rhs, x, r0, r1, mask); break;
+  }
+}
+
+template <typename T, bool DOT, int CFG>
+int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
+  auto k = k_spmv<T, DOT, CFG>;
+  const int g = grid_of(c, k, L.n);
+  k<<<g, kThreads, 0, c->stream>>>(val, L.col, L.pitch, x, y, L.n, partials);
+  return g;
+}
+
+// Launches y = A x on level L; returns the grid (the number of partials written when DOT).
+template <typename T, bool DOT>
+int spmv_dispatch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
+  switch (L.mv_sched) {
+    case 0: return spmv_launch<T, DOT, 0>(c, L, val, x, y, partials);
+    case 1: return spmv_launch<T, DOT, 1>(c, L, val, x, y, partials);
+    case 2: return spmv_launch<T, DOT, 2>(c, L, val, x, y, partials);
+    default: return spmv_launch<T, DOT, 3>(c, L, val, x, y, partials);
+  }
+}
+
+template <typename T, int CFG>
+void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
+  auto k = k_restrict<T, CFG>;
+  k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rf, xf, L.f2c, rc, nc);
+}
+
+template <typename T>
+void restrict_dispatch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
+  switch (L.mv_sched) {
+    case 0: restrict_launch<T, 0>(c, L, val, rf, xf, rc, nc); break;
+    case 1: restrict_launch<T, 1>(c, L, val, rf, xf, rc, nc); break;
+    case 2: restrict_launch<T, 2>(c, L, val, rf, xf, rc, nc); break;
+    default: restrict_launch<T, 3>(c, L, val, rf, xf, rc, nc); break;
+  }
+}
+
 template <typename T, typename TR>
 int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int s, bool first, bool top) {
   const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
   if (r1 <= r0) return HPCG_B200_OK;
-  const int grid = grid_for(c, r1 - r0, kThreads, kPerSm);
   const int kind = top ? (first ? kProfGsFirst : kProfGsFull) : -1;
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
   if (first)
-    k_gs_phase<T, TR, true><<<grid, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1,
-                                                               first_mask(L.g, s));
+    gs_dispatch<T, TR, true>(c, L, L.gs_sched, val, rhs, x, r0, r1, first_mask(L.g, s));
   else
-    k_gs_phase<T, TR, false><<<grid, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+    gs_dispatch<T, TR, false>(c, L, L.gs_sched, val, rhs, x, r0, r1, kAllSlots);
   HB_CK(cudaGetLastError());
   return prof_end(c, kind, ev0, r1 - r0);
 }
@@ -129,14 +197,69 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x) {
     Level& C = p->lev[l + 1];
     cudaEvent_t ev0 = nullptr;
     HB_TRY(prof_begin(c, l == 0 ? kProfRestrict : -1, &ev0));
-    k_restrict<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x,
-                                                                                         L.f2c, C.r, C.n);
+    restrict_dispatch<double>(c, L, L.val, r, x, C.r, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(prof_end(c, l == 0 ? kProfRestrict : -1, ev0, C.n));
     HB_TRY(mg_level(p, l + 1, C.r, C.x));
     k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x, x, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(symgs_level(p, l, r, x, false));
+  }
+  return HPCG_B200_OK;
+}
+
+// Autotuner: per level, times each kernel configuration (load schedule x
+// registers per thread) of the Gauss-Seidel phase and of the SpMV on scratch
+// vectors (Ap as x, zprev as right-hand side on level 0; the coarse r/x pair
+// otherwise) and keeps the fastest. Every configuration computes the same bits,
+// so the choice only affects speed. HPCG_B200_CONFIG=0..3 forces one.
+int autotune(hpcg_b200_problem* P) {
+  Context* c = P->ctx;
+  const char* force = std::getenv("HPCG_B200_CONFIG");
+  for (int l = 0; l < P->nlev; ++l) {
+    Level& L = P->lev[l];
+    if (L.tuned) continue;
+    L.tuned = true;
+    if (force && *force) {
+      const int f = std::atoi(force);
+      L.gs_sched = L.mv_sched = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
+      continue;
+    }
+    double* xs = l == 0 ? P->Ap : L.x;
+    double* rs = l == 0 ? P->zprev : L.r;
+    double* ys = l == 0 ? P->z : L.r;  // SpMV output (coarse levels: r, rewritten before use)
+    const int r0 = L.g.start[1], r1 = L.g.start[2];
+    if (r1 <= r0) continue;
+    cudaEvent_t e0, e1;
+    HB_CK(cudaEventCreate(&e0));
+    HB_CK(cudaEventCreate(&e1));
+    float best_gs = 1e30f, best_mv = 1e30f;
+    for (int sched = 0; sched < kConfigs; ++sched) {
+      float t_gs = 1e30f, t_mv = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        HB_CK(cudaEventRecord(e0, c->stream));
+        gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
+        HB_CK(cudaEventRecord(e1, c->stream));
+        HB_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+        t_gs = ms < t_gs ? ms : t_gs;
+        const int keep = L.mv_sched;
+        L.mv_sched = sched;
+        HB_CK(cudaEventRecord(e0, c->stream));
+        spmv_dispatch<double, false>(c, L, L.val, xs, ys, nullptr);
+        HB_CK(cudaEventRecord(e1, c->stream));
+        HB_CK(cudaEventSynchronize(e1));
+        L.mv_sched = keep;
+        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+        t_mv = ms < t_mv ? ms : t_mv;
+      }
+      if (t_gs < best_gs) { best_gs = t_gs; L.gs_sched = sched; }
+      if (t_mv < best_mv) { best_mv = t_mv; L.mv_sched = sched; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    HB_CK(cudaGetLastError());
   }
   return HPCG_B200_OK;
 }
@@ -186,8 +309,9 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
     HB_CK(cudaEventRecord(e, c->stream));
     return HPCG_B200_OK;
   };
+  HB_TRY(autotune(P));
   // p = x; Ap = A p; r = b - Ap; normr = sqrt(r'r)   (CG.cpp:86-90)
-  k_spmv<double, false><<<gv, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->x, P->Ap, n, nullptr);
+  spmv_dispatch<double, false>(c, L, L.val, P->x, P->Ap, nullptr);
   k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, P->b, -1.0, P->Ap, P->r, c->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize(c, nb, kFinNormr));
@@ -216,10 +340,10 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
     HB_TRY(mark());
     cudaEvent_t ev0 = nullptr;
     HB_TRY(prof_begin(c, kProfSpmv, &ev0));
-    k_spmv<double, true><<<nb, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->p, P->Ap, n, c->partials);
+    const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(prof_end(c, kProfSpmv, ev0, n));
-    HB_TRY(finalize(c, nb, kFinPap));                                       // :118-120
+    HB_TRY(finalize(c, gs, kFinPap));                                       // :118-120
     HB_TRY(mark());
     k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);  // :121-123
     HB_CK(cudaGetLastError());
@@ -264,8 +388,7 @@ int ensure_f32(hpcg_b200_problem* P) {
     if (!L.val32) {
       HB_TRY(dev_alloc((void**)&L.val32, sizeof(float) * kSlots * L.pitch, &P->bytes));
       const int64_t cnt = (int64_t)kSlots * L.pitch;
-      k_convert<float, double><<<grid_for(c, cnt, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.val,
-                                                                                            (int)cnt);
+      k_convert<float, double><<<grid_for(c, cnt, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.val, cnt);
       HB_CK(cudaGetLastError());
     }
     if (!L.r32) {
@@ -285,8 +408,7 @@ int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
   HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, true, false)));
   if (l + 1 < p->nlev) {
     Level& C = p->lev[l + 1];
-    k_restrict<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.col, L.pitch, r,
-                                                                                        x, L.f2c, C.r32, C.n);
+    restrict_dispatch<float>(c, L, L.val32, r, x, C.r32, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(mg32_level(p, l + 1, C.r32, C.x32));
     k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x32, x, C.n);
@@ -306,7 +428,8 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
   const int n = L.n;
   const int nb = red_blocks(c, n);
   const int gv = grid_for(c, n, kThreads, kPerSm);
-  k_spmv<double, false><<<gv, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->x, P->Ap, n, nullptr);
+  HB_TRY(autotune(P));
+  spmv_dispatch<double, false>(c, L, L.val, P->x, P->Ap, nullptr);
   k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, P->b, -1.0, P->Ap, P->r, c->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize(c, nb, kFinNormr));
@@ -333,9 +456,9 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
       HB_CK(cudaGetLastError());
     }
     HB_CK(cudaMemcpyAsync(P->zprev, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-    k_spmv<double, true><<<nb, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, P->p, P->Ap, n, c->partials);
+    const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
     HB_CK(cudaGetLastError());
-    HB_TRY(finalize(c, nb, kFinPap));
+    HB_TRY(finalize(c, gs, kFinPap));
     k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, nb, kFinNormr));
@@ -412,8 +535,8 @@ int hpcg_b200_spmv(hpcg_b200_problem* p, const double* x, double* y) {
   const Level& L = p->lev[0];
   Context* c = p->ctx;
   HB_TRY(load_vector(p, 0, x, p->p));
-  k_spmv<double, false><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, p->p,
-                                                                                        p->Ap, L.n, nullptr);
+  HB_TRY(autotune(p));
+  spmv_dispatch<double, false>(c, L, L.val, p->p, p->Ap, nullptr);
   HB_CK(cudaGetLastError());
   return store_vector(p, 0, p->Ap, y);
 }
@@ -424,6 +547,7 @@ int hpcg_b200_symgs(hpcg_b200_problem* p, const double* r, double* x) {
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, r, p->r));
   HB_TRY(load_vector(p, 0, x, p->x));
+  HB_TRY(autotune(p));
   HB_TRY(symgs_level(p, 0, p->r, p->x, false));
   return store_vector(p, 0, p->x, x);
 }
@@ -433,6 +557,7 @@ int hpcg_b200_mg(hpcg_b200_problem* p, const double* r, double* x) {
   if (!r || !x) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, r, p->r));
+  HB_TRY(autotune(p));
   HB_TRY(mg_level(p, 0, p->r, p->z));
   return store_vector(p, 0, p->z, x);
 }

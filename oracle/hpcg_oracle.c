@@ -96,6 +96,11 @@ void ora_symgs(const ora_level* A, const double* r, double* x) {
   ora_gs_backward(A, r, x);
 }
 
+void ora_symgs_skip(const ora_level* A, const double* r, double* x, int skip) {
+  ora_gs_forward(A, r, x);
+  for (int i = A->n - 1 - skip; i >= 0; --i) x[i] = gs_row(A, i, r, x);
+}
+
 void ora_restriction(int nc, const int* f2c, const double* rf, const double* Axf, double* rc) {
   for (int i = 0; i < nc; ++i) rc[i] = rf[f2c[i]] - Axf[f2c[i]];
 }
@@ -108,7 +113,12 @@ void ora_prolongation(int nc, const int* f2c, const double* xc, double* xf) {
  * restrict; recurse on the coarse level; prolong; one post-smoothing SYMGS.
  * The coarsest level does a single SYMGS. */
 int ora_mg(const ora_level* L, int nlev, int lev, const double* r, double* x) {
+  return ora_mg_skip(L, nlev, lev, r, x, NULL);
+}
+
+int ora_mg_skip(const ora_level* L, int nlev, int lev, const double* r, double* x, const int* skip) {
   const ora_level* A = &L[lev];
+  const int sk = skip ? skip[lev] : 0;
   memset(x, 0, sizeof(double) * (size_t)A->n);
   if (lev + 1 < nlev) {
     const int nc = L[lev + 1].n;
@@ -116,18 +126,18 @@ int ora_mg(const ora_level* L, int nlev, int lev, const double* r, double* x) {
     double* rc = (double*)malloc(sizeof(double) * (size_t)nc);
     double* xc = (double*)malloc(sizeof(double) * (size_t)nc);
     if (!Axf || !rc || !xc) { free(Axf); free(rc); free(xc); return 1; }
-    ora_symgs(A, r, x);
+    ora_symgs_skip(A, r, x, sk);
     ora_spmv(A, x, Axf);
     ora_restriction(nc, A->f2c, r, Axf, rc);
-    int err = ora_mg(L, nlev, lev + 1, rc, xc);
+    int err = ora_mg_skip(L, nlev, lev + 1, rc, xc, skip);
     if (!err) {
       ora_prolongation(nc, A->f2c, xc, x);
-      ora_symgs(A, r, x);
+      ora_symgs_skip(A, r, x, sk);
     }
     free(Axf); free(rc); free(xc);
     return err;
   }
-  ora_symgs(A, r, x);
+  ora_symgs_skip(A, r, x, sk);
   return 0;
 }
 
@@ -164,6 +174,11 @@ double ora_residual(int n, const double* v1, const double* v2) {
 /* CG_ref.cpp:58-144 */
 int ora_cg(const ora_level* L, int nlev, const double* b, double* x, int max_iter, double tolerance,
            int do_prec, int* niters, double* normr_out, double* normr0_out, double* hist) {
+  return ora_cg_skip(L, nlev, b, x, max_iter, tolerance, do_prec, niters, normr_out, normr0_out, hist, NULL);
+}
+
+int ora_cg_skip(const ora_level* L, int nlev, const double* b, double* x, int max_iter, double tolerance,
+                int do_prec, int* niters, double* normr_out, double* normr0_out, double* hist, const int* skip) {
   const ora_level* A = &L[0];
   const int n = A->n;
   double* r = (double*)malloc(sizeof(double) * (size_t)n);
@@ -182,7 +197,7 @@ int ora_cg(const ora_level* L, int nlev, const double* b, double* x, int max_ite
   int err = 0;
   for (int k = 1; k <= max_iter && normr / normr0 > tolerance; ++k) {
     if (do_prec) {
-      err = ora_mg(L, nlev, 0, r, z);                      /* :104 */
+      err = ora_mg_skip(L, nlev, 0, r, z, skip);           /* :104 */
       if (err) break;
     } else {
       ora_waxpby(n, 1.0, r, 0.0, r, z);                    /* :106 */

@@ -67,6 +67,19 @@ void ora_symgs(const ora_level* A, const double* r, double* x);
 /* forward sweep only / backward sweep only (the two halves of the above) */
 void ora_gs_forward(const ora_level* A, const double* r, double* x);
 void ora_gs_backward(const ora_level* A, const double* r, double* x);
+/* ComputeSYMGS_ref.cpp:67-100 with the backward update of the last `skip` rows
+ * left out. The library sweeps colour blocks in row order and does not repeat
+ * the last block at the turn of the sweep (its other-colour inputs are
+ * unchanged); with the reference's subtract-then-add-back diagonal term the
+ * repeat would differ from the forward value only by rounding. skip = 0 is
+ * ComputeSYMGS_ref itself. */
+void ora_symgs_skip(const ora_level* A, const double* r, double* x, int skip);
+/* ComputeMG_ref.cpp:39-63 with ora_symgs_skip(skip[l]) on level l. */
+int ora_mg_skip(const ora_level* levels, int nlev, int lev, const double* r, double* x, const int* skip);
+/* CG_ref.cpp:58-144 with that V-cycle (skip may be NULL: the reference's). */
+int ora_cg_skip(const ora_level* levels, int nlev, const double* b, double* x, int max_iter, double tolerance,
+                int do_prec, int* niters, double* normr, double* normr0, double* hist, const int* skip);
+
 /* ComputeRestriction_ref.cpp:51 */
 void ora_restriction(int nc, const int* f2c, const double* rf, const double* Axf, double* rc);
 /* ComputeProlongation_ref.cpp:49 */

@@ -67,6 +67,13 @@ def _load_oracle():
     lib.ora_cg.restype = C.c_int
     lib.ora_cg.argtypes = [C.POINTER(_Level), C.c_int, _f64p, _f64p, C.c_int, C.c_double, C.c_int,
                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double), _f64p]
+    lib.ora_symgs_skip.argtypes = [C.POINTER(_Level), _f64p, _f64p, C.c_int]
+    lib.ora_mg_skip.restype = C.c_int
+    lib.ora_mg_skip.argtypes = [C.POINTER(_Level), C.c_int, C.c_int, _f64p, _f64p, C.c_void_p]
+    lib.ora_cg_skip.restype = C.c_int
+    lib.ora_cg_skip.argtypes = [C.POINTER(_Level), C.c_int, _f64p, _f64p, C.c_int, C.c_double, C.c_int,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double), _f64p,
+                                C.c_void_p]
     lib.ora_permute_level.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p, _f64p, _i32p,
                                       _i32p, _i32p, _f64p, _i32p]
     lib.ora_permute_f2c.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p]
@@ -182,10 +189,20 @@ def gs_forward(L: Level, r, x):
     return x
 
 
-def mg(levels, r, lev=0):
+def mg(levels, r, lev=0, skip=None):
+    """ComputeMG_ref; skip[l] = trailing rows of level l whose backward GS update is
+    left out (see ora_symgs_skip), None for the reference's V-cycle."""
     x = np.zeros(levels[lev].n)
-    err = lib().ora_mg(_levels_c(levels), len(levels), lev, np.ascontiguousarray(r, np.float64), x)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.int32)
+    err = lib().ora_mg_skip(_levels_c(levels), len(levels), lev, np.ascontiguousarray(r, np.float64), x,
+                            sk.ctypes.data if sk is not None else None)
     assert err == 0
+    return x
+
+
+def symgs_skip(L: Level, r, x, skip):
+    x = np.array(x, np.float64, copy=True)
+    lib().ora_symgs_skip(C.byref(L.c()), np.ascontiguousarray(r, np.float64), x, int(skip))
     return x
 
 
@@ -219,13 +236,15 @@ def residual(v1, v2):
                               np.ascontiguousarray(v2, np.float64))
 
 
-def cg(levels, b, x0, max_iter, tolerance, do_prec=True):
-    """CG_ref. Returns (x, niters, normr, normr0, hist[0..niters])."""
+def cg(levels, b, x0, max_iter, tolerance, do_prec=True, skip=None):
+    """CG_ref (with the V-cycle of mg(skip=...)). Returns (x, niters, normr, normr0, hist[0..niters])."""
     x = np.array(x0, np.float64, copy=True)
     hist = np.zeros(max_iter + 1)
     ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
-    err = lib().ora_cg(_levels_c(levels), len(levels), np.ascontiguousarray(b, np.float64), x, max_iter,
-                       tolerance, int(do_prec), C.byref(ni), C.byref(nr), C.byref(nr0), hist)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.int32)
+    err = lib().ora_cg_skip(_levels_c(levels), len(levels), np.ascontiguousarray(b, np.float64), x, max_iter,
+                            tolerance, int(do_prec), C.byref(ni), C.byref(nr), C.byref(nr0), hist,
+                            sk.ctypes.data if sk is not None else None)
     assert err == 0
     return x, ni.value, nr.value, nr0.value, hist[: ni.value + 1].copy()
 
