@@ -36,7 +36,7 @@ EXPORTS = (
     "hpcg_b200_spmv", "hpcg_b200_symgs", "hpcg_b200_mg", "hpcg_b200_dot", "hpcg_b200_waxpby",
     "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
-    "hpcg_b200_profile_read", "hpcg_b200_last_error",
+    "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_last_error",
 )
 
 
@@ -90,6 +90,7 @@ def lib():
         l.hpcg_b200_stream.restype = vp
         l.hpcg_b200_profile.argtypes = [i, i]
         l.hpcg_b200_profile_read.argtypes = [i, i, C.POINTER(d), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        l.hpcg_b200_dot_noalloc.argtypes = [i, vp, vp, vp, vp]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)

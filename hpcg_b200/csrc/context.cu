@@ -29,6 +29,8 @@ void set_error(const char* what, cudaError_t e) {
   std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
 }
 
+void set_error_text(const char* msg) { std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg); }
+
 int status_of(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? HPCG_B200_ERR_NOMEM : HPCG_B200_ERR_CUDA;
 }

@@ -133,6 +133,23 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
 int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0);
 
+/* ---- dot product without device allocation -------------------------------- */
+
+/* result[0] = x'y over n entries, for callers that cannot allocate device
+ * memory (their allocator owns the GPU's memory, or allocation is not allowed
+ * where they call from). No counterpart in the reference: it is an extra entry
+ * point beside hpcg_b200_dot, which allocates its per-device work buffers on
+ * first use. x, y and result must be device memory of the current GPU; the two
+ * kernels are queued on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) and the call returns without waiting. Its only scratch is a fixed
+ * 512 KiB array inside the library (present on every GPU that loads it), so
+ * n is limited to HPCG_B200_DOT_NOALLOC_MAX_N; larger n returns
+ * HPCG_B200_ERR_ARG. The first call on each device looks the array's address up
+ * (make it before any stream capture). Calls that overlap on the GPU share the
+ * array and race: serialise them. */
+#define HPCG_B200_DOT_NOALLOC_MAX_N 268435456
+int hpcg_b200_dot_noalloc(int n, const double* x, const double* y, double* result, void* stream);
+
 /* ---- inspection (tests) -------------------------------------------------- */
 
 /* Rows, padded pitch and colour-block boundaries (9 ints) of one level. */
