@@ -271,6 +271,8 @@ def b200_arm(args, rank, world, local_rank):
     ms = e0.elapsed_time(e1)
     gs_ms, gs_launch, gs_rows = B.profile_read(B.PROF_GS_FULL, dev)
     sp_ms, sp_launch, sp_rows = B.profile_read(B.PROF_SPMV, dev)
+    gf_ms, gf_launch, gf_rows = B.profile_read(B.PROF_GS_FIRST, dev)
+    rs_ms, rs_launch, rs_rows = B.profile_read(B.PROF_RESTRICT, dev)
     B.profile(False, dev)
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
@@ -337,6 +339,12 @@ def b200_arm(args, rank, world, local_rank):
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
             "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
                      "gbs": round((sp_rows * (27 * 12 + 8 + 8)) / (sp_ms * 1e-3) / 1e9, 1) if sp_ms else None},
+            "kernel_ms_per_iter": {
+                "gs_full_l0": round(gs_ms / (args.iters * args.steps), 3),
+                "gs_first_l0": round(gf_ms / (args.iters * args.steps), 3),
+                "spmv_l0": round(sp_ms / (args.iters * args.steps), 3),
+                "restrict_l0": round(rs_ms / (args.iters * args.steps), 3),
+                "iteration": round(ms / (args.iters * args.steps), 3)},
             "gpu_launches": gpu_launches_per_set(args.iters) * args.steps,
             "clocks": clk,
         }

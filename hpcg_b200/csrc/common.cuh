@@ -91,6 +91,8 @@ struct Level {
   int* new2old = nullptr;    // [n] colour row -> natural row
   int* old2new = nullptr;    // [n]
   int* f2c = nullptr;        // [n of next level] coarse colour row -> fine colour row
+  int* tf = nullptr;         // transfer pairs (fine row, coarse row) sorted by fine row:
+  int* tq = nullptr;         //   tf[t] = f2c[tq[t]], tf increasing
   double* r = nullptr;       // coarse right-hand side (levels > 0), [pitch]
   double* x = nullptr;       // coarse solution (levels > 0), [pitch]
   float* r32 = nullptr;      // FP32 V-cycle vectors, [pitch]
@@ -98,6 +100,7 @@ struct Level {
   // kernel configuration of this level's row kernels, chosen by the autotuner
   int gs_sched = 1;          // kernel configuration (0..3) of the Gauss-Seidel phases
   int mv_sched = 1;          // kernel configuration of SpMV / restriction
+  bool mv_nat = true;        // SpMV visits rows in natural grid order
   bool tuned = false;
   // level-scheduled natural order (built on first use)
   int* wave_rows = nullptr;  // colour-order rows sorted by ix + 2 iy + 4 iz
@@ -207,6 +210,9 @@ inline int grid_for(const Context* c, int64_t work, int threads, int per_sm) {
   if (blocks < 1) blocks = 1;
   return (int)blocks;
 }
+
+// Builds the sorted transfer pairs (tf, tq) of level l from its device f2c.
+int build_transfer(hpcg_b200_problem* p, int l);
 
 // natural <-> colour order vector movement (solver.cu)
 int load_vector(hpcg_b200_problem* p, int level, const double* src_natural, double* dst_colour);

@@ -140,13 +140,25 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
 
 // y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y
 // (the p'Ap of CG.cpp:119, fused).
-template <typename T, bool DOT, int CFG, int SCHED = cfg_sched(CFG)>
-__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(const T* __restrict__ val, const int* __restrict__ col,
-                                                      int64_t pitch, const T* __restrict__ x, T* __restrict__ y,
-                                                      int n, double* __restrict__ partials) {
+// NAT: rows are visited in the natural order of the grid (row q = old2new of the
+// thread's natural index), so consecutive threads touch neighbouring points and
+// the x values they gather stay in a window of a few planes held in L2; in
+// storage order each colour block would gather the other seven colours' x
+// across the whole grid again. Each warp still reads two contiguous runs of a
+// slot (the two parities of ix).
+template <typename T, bool DOT, int CFG, bool NAT, int SCHED = cfg_sched(CFG)>
+__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, const T* __restrict__ val,
+                                                                  const int* __restrict__ col, int64_t pitch,
+                                                                  const T* __restrict__ x, T* __restrict__ y, int n,
+                                                                  double* __restrict__ partials) {
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+    int q = t;
+    if (NAT) {
+      const int ix = t % g.nx, iy = (t / g.nx) % g.ny, iz = t / (g.nx * g.ny);
+      q = g.old2new(ix, iy, iz);
+    }
     T sum = (T)0;
     T xq = (T)0;
     if (SCHED == kStaged) {
@@ -181,16 +193,20 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(const T* __res
 }
 
 // Restriction fused with the residual it needs (ComputeMG_ref.cpp:49-51):
-// rc[q] = rf[f] - (A xf)[f] for f = f2c[q]; the residual is formed only at the
-// injected rows (ComputeRestriction_ref.cpp:51 reads no others).
+// rc[q] = rf[f] - (A xf)[f] for each transfer pair (f, q) of f2c; the residual
+// is formed only at the injected rows (ComputeRestriction_ref.cpp:51 reads no
+// others). The pairs are sorted by fine row, so the matrix rows are streamed in
+// storage order and only the coarse writes scatter.
 template <typename T, int CFG, int SCHED = cfg_sched(CFG)>
 __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* __restrict__ val, const int* __restrict__ col,
-                                                          int64_t pitch, const T* __restrict__ rf,
-                                                          const T* __restrict__ xf, const int* __restrict__ f2c,
-                                                          T* __restrict__ rc, int nc) {
+                                                                      int64_t pitch, const T* __restrict__ rf,
+                                                                      const T* __restrict__ xf,
+                                                                      const int* __restrict__ tf,
+                                                                      const int* __restrict__ tq, T* __restrict__ rc,
+                                                                      int nc) {
   const int stride = gridDim.x * blockDim.x;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) {
-    const int f = f2c[q];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += stride) {
+    const int f = tf[t];
     T sum = (T)0;
     if (SCHED == kStaged) {
       T a[kSlots];
@@ -209,16 +225,16 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
 #pragma unroll
       for (int k = 0; k < kSlots; ++k) sum += val[k * pitch + f] * __ldg(xf + col[k * pitch + f]);
     }
-    rc[q] = rf[f] - sum;
+    rc[tq[t]] = rf[f] - sum;
   }
 }
 
-// ComputeProlongation_ref.cpp:49
+// ComputeProlongation_ref.cpp:49 over the same sorted pairs
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_prolong(const int* __restrict__ f2c, const T* __restrict__ xc,
-                                                      T* __restrict__ xf, int nc) {
+__global__ void __launch_bounds__(kThreads) k_prolong(const int* __restrict__ tf, const int* __restrict__ tq,
+                                                      const T* __restrict__ xc, T* __restrict__ xf, int nc) {
   const int stride = gridDim.x * blockDim.x;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += stride) xf[f2c[q]] += xc[q];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += stride) xf[tf[t]] += xc[tq[t]];
 }
 
 // ---- vectors ----------------------------------------------------------------

@@ -131,13 +131,38 @@ int check_dims(int nx, int ny, int nz, int nlevels) {
 
 }  // namespace
 
+// The pairs (f2c[q], q) ordered by fine row: counting by fine row, since f2c is
+// injective into [0, n).
+int build_transfer(hpcg_b200_problem* p, int l) {
+  Level& L = p->lev[l];
+  if (!L.f2c || l + 1 >= p->nlev) return HPCG_B200_OK;
+  const int nc = p->lev[l + 1].n;
+  std::vector<int> f(nc);
+  HB_CK(cudaMemcpy(f.data(), L.f2c, sizeof(int) * nc, cudaMemcpyDeviceToHost));
+  std::vector<int> inv(L.n, -1);
+  for (int q = 0; q < nc; ++q) {
+    if (f[q] < 0 || f[q] >= L.n || inv[f[q]] >= 0) return HPCG_B200_ERR_ARG;
+    inv[f[q]] = q;
+  }
+  std::vector<int> tf(nc), tq(nc);
+  int t = 0;
+  for (int i = 0; i < L.n; ++i)
+    if (inv[i] >= 0) { tf[t] = i; tq[t] = inv[i]; ++t; }
+  HB_TRY(alloc_n(p, &L.tf, nc));
+  HB_TRY(alloc_n(p, &L.tq, nc));
+  HB_CK(cudaMemcpy(L.tf, tf.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+  HB_CK(cudaMemcpy(L.tq, tq.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+  return HPCG_B200_OK;
+}
+
 int free_problem(hpcg_b200_problem* p) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   cudaSetDevice(p->device);
   if (p->ctx) cudaStreamSynchronize(p->ctx->stream);
   for (int l = 0; l < kMaxLevels; ++l) {
     Level& L = p->lev[l];
-    void* ptrs[] = {L.val, L.col, L.val32, L.new2old, L.old2new, L.f2c, L.r, L.x, L.r32, L.x32, L.wave_rows};
+    void* ptrs[] = {L.val, L.col, L.val32, L.new2old, L.old2new, L.f2c, L.tf, L.tq, L.r, L.x, L.r32, L.x32,
+                    L.wave_rows};
     for (void* q : ptrs) dev_free(q);
     delete[] L.wave_start;
   }
@@ -245,6 +270,7 @@ int hpcg_b200_optimize(const hpcg_b200_level_desc* desc, int nlevels, int device
     }
   }
   if (status == HPCG_B200_OK) status = alloc_vectors(p);
+  for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
   if (status == HPCG_B200_OK) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { set_error("optimize sync", e); status = status_of(e); }
@@ -298,6 +324,7 @@ int hpcg_b200_generate(int nx, int ny, int nz, int nlevels, int device, hpcg_b20
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { set_error("generate", e); status = status_of(e); }
   }
+  for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
   if (status != HPCG_B200_OK) {
     free_problem(p);
     return status;

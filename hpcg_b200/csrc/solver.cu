@@ -67,9 +67,15 @@ void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rh
 
 template <typename T, bool DOT, int CFG>
 int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
-  auto k = k_spmv<T, DOT, CFG>;
+  if (L.mv_nat) {
+    auto k = k_spmv<T, DOT, CFG, true>;
+    const int g = grid_of(c, k, L.n);
+    k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
+    return g;
+  }
+  auto k = k_spmv<T, DOT, CFG, false>;
   const int g = grid_of(c, k, L.n);
-  k<<<g, kThreads, 0, c->stream>>>(val, L.col, L.pitch, x, y, L.n, partials);
+  k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
   return g;
 }
 
@@ -87,7 +93,7 @@ int spmv_dispatch(Context* c, const Level& L, const T* val, const T* x, T* y, do
 template <typename T, int CFG>
 void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   auto k = k_restrict<T, CFG>;
-  k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rf, xf, L.f2c, rc, nc);
+  k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rf, xf, L.tf, L.tq, rc, nc);
 }
 
 template <typename T>
@@ -201,7 +207,7 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x) {
     HB_CK(cudaGetLastError());
     HB_TRY(prof_end(c, l == 0 ? kProfRestrict : -1, ev0, C.n));
     HB_TRY(mg_level(p, l + 1, C.r, C.x));
-    k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x, x, C.n);
+    k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x, x, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(symgs_level(p, l, r, x, false));
   }
@@ -235,7 +241,7 @@ int autotune(hpcg_b200_problem* P) {
     HB_CK(cudaEventCreate(&e1));
     float best_gs = 1e30f, best_mv = 1e30f;
     for (int sched = 0; sched < kConfigs; ++sched) {
-      float t_gs = 1e30f, t_mv = 1e30f;
+      float t_gs = 1e30f, t_mv[2] = {1e30f, 1e30f};
       for (int rep = 0; rep < 3; ++rep) {
         HB_CK(cudaEventRecord(e0, c->stream));
         gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
@@ -245,17 +251,23 @@ int autotune(hpcg_b200_problem* P) {
         HB_CK(cudaEventElapsedTime(&ms, e0, e1));
         t_gs = ms < t_gs ? ms : t_gs;
         const int keep = L.mv_sched;
-        L.mv_sched = sched;
-        HB_CK(cudaEventRecord(e0, c->stream));
-        spmv_dispatch<double, false>(c, L, L.val, xs, ys, nullptr);
-        HB_CK(cudaEventRecord(e1, c->stream));
-        HB_CK(cudaEventSynchronize(e1));
+        const bool keep_nat = L.mv_nat;
+        for (int nat = 0; nat < 2; ++nat) {
+          L.mv_sched = sched;
+          L.mv_nat = nat != 0;
+          HB_CK(cudaEventRecord(e0, c->stream));
+          spmv_dispatch<double, false>(c, L, L.val, xs, ys, nullptr);
+          HB_CK(cudaEventRecord(e1, c->stream));
+          HB_CK(cudaEventSynchronize(e1));
+          HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < t_mv[nat]) t_mv[nat] = ms;
+        }
         L.mv_sched = keep;
-        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-        t_mv = ms < t_mv ? ms : t_mv;
+        L.mv_nat = keep_nat;
       }
       if (t_gs < best_gs) { best_gs = t_gs; L.gs_sched = sched; }
-      if (t_mv < best_mv) { best_mv = t_mv; L.mv_sched = sched; }
+      for (int nat = 0; nat < 2; ++nat)
+        if (t_mv[nat] < best_mv) { best_mv = t_mv[nat]; L.mv_sched = sched; L.mv_nat = nat != 0; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -411,7 +423,7 @@ int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
     restrict_dispatch<float>(c, L, L.val32, r, x, C.r32, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(mg32_level(p, l + 1, C.r32, C.x32));
-    k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.f2c, C.x32, x, C.n);
+    k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x32, x, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, false, false)));
   }
