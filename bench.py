@@ -44,6 +44,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-n", type=int, default=128, help="grid side of the CPU reference sample")
     ap.add_argument("--ref-seconds", type=float, default=20.0, help="CPU seconds budget of a reference sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 V-cycle vs FP64 time-to-1e-9 comparison")
+    ap.add_argument("--mixed-rhs", default="hpcg", choices=["hpcg", "uniform", "both"],
+                    help="right-hand side(s) of the mixed-precision comparison: b = 27 - nnz, U[-1,1], or both")
+    ap.add_argument("--mixed-tol", type=float, default=1e-9)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the 128^3 implicit-adjoint timing")
     return ap.parse_args()
 
 
@@ -204,6 +209,77 @@ def committed_traffic():
 # B200 arm
 # ---------------------------------------------------------------------------
 
+RHS_SEED = 0x48504347
+
+
+def uniform_rhs(nrow, device):
+    """b ~ U[-1, 1], FP64, from a fixed seed (numpy PCG64), built on the host."""
+    import numpy as np
+    import torch
+    b = np.random.Generator(np.random.PCG64(RHS_SEED)).uniform(-1.0, 1.0, nrow)
+    return torch.from_numpy(b).to(device)
+
+
+def timed(lib_stream, fn):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(lib_stream)
+    out = fn()
+    e1.record(lib_stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) * 1e-3
+
+
+def adjoint_timing(dev, n=128, tol=1e-10):
+    """Perturbed symmetric stencil at n^3: forward solve to `tol`, loss
+    0.5 ||x - x_target||^2, then the implicit adjoint (dL/db and dL/da)."""
+    import torch
+    from hpcg_b200 import binding as B
+    from hpcg_b200 import perturbed as PT
+    nrow = n ** 3
+    P = B.Problem.generate(n, n, n, 4, dev)
+    try:
+        vals = torch.from_numpy(PT.perturbed_values(n, n, n)).to(f"cuda:{dev}")
+        P.set_values(0, vals)
+        b = torch.from_numpy(PT.rhs_uniform(nrow)).to(f"cuda:{dev}")
+        xt = torch.from_numpy(PT.target_normal(nrow)).to(f"cuda:{dev}")
+        lib_stream = torch.cuda.ExternalStream(B.stream(dev), device=dev)
+        x = torch.zeros_like(b)
+        (it_f, nr, nr0), t_f = timed(lib_stream, lambda: P.CG(b, x, 2000, tol, True))
+        g = x - xt
+        gb = torch.empty_like(b)
+        gv = torch.empty_like(vals)
+        it_a, t_a = timed(lib_stream, lambda: P.adjoint(x, g, 2000, tol, gb, gv))
+        return {"grid": [n, n, n], "tolerance": tol, "forward": {"iters": it_f, "seconds": round(t_f, 4)},
+                "adjoint": {"iters": it_a, "seconds": round(t_a, 4)},
+                "loss": float(0.5 * torch.sum((x - xt) ** 2)), "grad_b_norm": float(torch.linalg.vector_norm(gb)),
+                "grad_values_norm": float(torch.linalg.vector_norm(gv))}
+    finally:
+        P.free()
+
+
+def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000):
+    """Time to a relative residual `tol` from x = 0: FP64 PCG (hpcg_b200_cg) against
+    FP64 flexible PCG around the FP32 V-cycle (hpcg_b200_cg_mixed)."""
+    import torch
+    from hpcg_b200 import binding as B
+    n = b.numel()
+    x64 = torch.zeros_like(b)
+    (it64, nr64, nr064), t64 = timed(lib_stream, lambda: P.CG(b, x64, max_iter, tol, True))
+    x32 = torch.zeros_like(b)
+    (it32, nr32, nr032), t32 = timed(lib_stream, lambda: P.CG_mixed(b, x32, max_iter, tol))
+    err = float(torch.linalg.vector_norm(x32 - x64) / torch.linalg.vector_norm(x64))
+    ax = torch.zeros_like(b)
+    P.ComputeSPMV(x32, ax)
+    torch.cuda.synchronize()
+    res = B.ComputeDotProduct(n, b - ax, b - ax) ** 0.5 / B.ComputeDotProduct(n, b, b) ** 0.5
+    return {"fp64": {"iters": it64, "seconds": round(t64, 3), "scaled_residual": nr64 / nr064},
+            "fp32_vcycle": {"iters": it32, "seconds": round(t32, 3), "scaled_residual": nr32 / nr032,
+                            "true_residual": res},
+            "time_ratio": round(t32 / t64, 4), "x_rel_diff_vs_fp64": err}
+
 def gpu_launches_per_set(iters, nlevels=4):
     """Kernels the library launches for one CG call (its own kernels only)."""
     mg = 15 * 2 + 2  # per non-coarsest level: pre and post symmetric sweeps (15 colour phases each),
@@ -309,6 +385,18 @@ def b200_arm(args, rank, world, local_rank):
                "h2d_bytes_per_step": 2 * nrow * 8, "d2h_bytes_per_step": nrow * 8 + 64,
                "ms_per_step": round(ems / args.steps, 3)}
 
+    mixed = None
+    if not args.no_mixed:
+        mixed = {"tolerance": args.mixed_tol}
+        if args.mixed_rhs in ("hpcg", "both"):
+            mixed["rhs_hpcg"] = mixed_vs_fp64(P, b, lib_stream, args.mixed_tol)
+        if args.mixed_rhs in ("uniform", "both"):
+            mixed["rhs_uniform"] = mixed_vs_fp64(P, uniform_rhs(nrow, f"cuda:{dev}"), lib_stream, args.mixed_tol)
+
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_timing(dev)
+
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -350,6 +438,10 @@ def b200_arm(args, rank, world, local_rank):
         }
         if e2e:
             line["e2e"] = e2e
+        if mixed:
+            line["mixed_precision"] = mixed
+        if adjoint:
+            line["adjoint"] = adjoint
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(args)

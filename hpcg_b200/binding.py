@@ -36,7 +36,7 @@ EXPORTS = (
     "hpcg_b200_spmv", "hpcg_b200_symgs", "hpcg_b200_mg", "hpcg_b200_dot", "hpcg_b200_waxpby",
     "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
-    "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_last_error",
+    "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_last_error",
 )
 
 
@@ -91,6 +91,7 @@ def lib():
         l.hpcg_b200_profile.argtypes = [i, i]
         l.hpcg_b200_profile_read.argtypes = [i, i, C.POINTER(d), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         l.hpcg_b200_dot_noalloc.argtypes = [i, vp, vp, vp, vp]
+        l.hpcg_b200_adjoint.argtypes = [vp, vp, vp, i, d, vp, vp, C.POINTER(i)]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -116,8 +117,8 @@ def _ptr(v, n=None):
     if isinstance(v, np.ndarray):
         if v.dtype != np.float64 or not v.flags.c_contiguous:
             raise TypeError("vectors must be contiguous float64")
-        if n is not None and v.shape[0] < n:
-            raise ValueError(f"vector of length {v.shape[0]} shorter than {n}")
+        if n is not None and v.size < n:
+            raise ValueError(f"vector of length {v.size} shorter than {n}")
         return v.ctypes.data
     if hasattr(v, "data_ptr"):
         import torch
@@ -242,6 +243,15 @@ class Problem:
         _check(lib().hpcg_b200_cg_mixed(self._h, _ptr(b, self.nrow), _ptr(x, self.nrow), max_iter, tolerance,
                                         C.byref(ni), C.byref(nr), C.byref(nr0)), "CG_mixed")
         return ni.value, nr.value, nr0.value
+
+    def adjoint(self, x, g, max_iter, tolerance, grad_b, grad_values27):
+        """Implicit adjoint of the solve: grad_b = lambda (A lambda = g), grad_values27
+        = -lambda_i x_j per slot. Returns the adjoint solve's iteration count."""
+        ni = C.c_int(0)
+        _check(lib().hpcg_b200_adjoint(self._h, _ptr(x, self.nrow), _ptr(g, self.nrow), max_iter, tolerance,
+                                       _ptr(grad_b, self.nrow), _ptr(grad_values27, 27 * self.nrow), C.byref(ni)),
+               "hpcg_b200_adjoint")
+        return ni.value
 
     # ---- inspection ------------------------------------------------------------
     def level_info(self, level):

@@ -98,7 +98,8 @@ struct Level {
   float* r32 = nullptr;      // FP32 V-cycle vectors, [pitch]
   float* x32 = nullptr;
   // kernel configuration of this level's row kernels, chosen by the autotuner
-  int gs_sched = 1;          // kernel configuration (0..3) of the Gauss-Seidel phases
+  int gs_sched = 1;          // kernel configuration of the Gauss-Seidel phases (FP64)
+  int gs_sched32 = 1;        // kernel configuration of the Gauss-Seidel phases (FP32 V-cycle)
   int mv_sched = 1;          // kernel configuration of SpMV / restriction
   bool mv_nat = true;        // SpMV visits rows in natural grid order
   bool tuned = false;

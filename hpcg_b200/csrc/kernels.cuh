@@ -52,65 +52,165 @@ __device__ __forceinline__ double block_max(double v) {
 // (neighbours not yet swept, and the diagonal) multiply a zero and are skipped,
 // which leaves every sum bitwise unchanged.
 // ---------------------------------------------------------------------------
-// Two load schedules of the same row arithmetic (results are bitwise equal):
-//  kPlain  -- loads issued as the compiler schedules the slot loop;
-//  kStaged -- all masked value/column loads issued first (27 independent loads
-//             in flight per thread), then the 27 gathers of x, then the sum; the
-//             matrix is read with evict-first hints (__ldcs) so that the stream of
-//             values and columns, read once per phase, does not push the vector
-//             out of L2.
+// Kernel configurations the autotuner chooses from. Every configuration
+// computes the same bits; they differ in how the loads are issued:
+//  - schedule: kPlain issues loads as the compiler schedules the slot loop;
+//    kStaged issues all masked value/column loads first (27 independent loads in
+//    flight per thread), then the 27 gathers of x, then the sum, and reads the
+//    matrix with evict-first hints (__ldcs) so that the stream of values and
+//    columns, read once per phase, does not push the vector out of L2;
+//  - rows per thread (R): with R > 1 a thread updates R adjacent rows of a
+//    colour with vector loads (double2, float2/float4, int2/int4), so each load
+//    instruction moves R times the bytes and more bytes are in flight per thread
+//    (the FP32 matrix stream otherwise moves only 4 bytes a load); R > 1 needs
+//    the row range to start on a multiple of R (checked on the host);
+//  - the minimum resident 256-thread blocks per SM, which caps registers per
+//    thread (4 -> 64, 2 -> 128, 1 -> 255).
 enum LoadSchedule : int { kPlain = 0, kStaged = 1 };
 
-// Kernel configurations the autotuner chooses from: a load schedule and the
-// minimum resident 256-thread blocks per SM (which caps registers per thread:
-// 4 -> 64, 2 -> 128, 1 -> 255).
-constexpr int kConfigs = 4;
-__host__ __device__ constexpr int cfg_sched(int cfg) { return cfg >= 2 ? kStaged : kPlain; }
-__host__ __device__ constexpr int cfg_minb(int cfg) { return cfg == 0 ? 4 : cfg == 1 ? 2 : cfg == 2 ? 1 : 2; }
+constexpr int kConfigs = 7;
+__host__ __device__ constexpr int cfg_sched(int cfg) { return cfg == 2 || cfg == 3 ? kStaged : kPlain; }
+__host__ __device__ constexpr int cfg_minb(int cfg) {
+  return cfg == 0 || cfg == 4 ? 4 : cfg == 2 ? 1 : 2;
+}
+__host__ __device__ constexpr int cfg_rows(int cfg) { return cfg == 4 || cfg == 5 ? 2 : cfg == 6 ? 4 : 1; }
 
-template <typename T, typename TR, bool FIRST, int CFG, int SCHED = cfg_sched(CFG)>
-__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* __restrict__ val, const int* __restrict__ col,
-                                                          int64_t pitch, const TR* __restrict__ rhs, T* x, int r0,
-                                                          int r1, uint32_t mask) {
-  const int stride = gridDim.x * blockDim.x;
-  for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride) {
-    T sum = (T)rhs[q];
-    T xd = (T)0;
-    if (SCHED == kStaged) {
-      T a[kSlots];
-      int cl[kSlots];
+// R consecutive elements through one or two vector loads (p aligned to R elements).
+template <typename T, int R>
+__device__ __forceinline__ void load_vec(const T* __restrict__ p, T (&out)[R]) {
+  static_assert(sizeof(T) * R == 4 || sizeof(T) * R == 8 || sizeof(T) * R == 16 || sizeof(T) * R == 32, "");
+  if constexpr (sizeof(T) * R == 4) {
+    out[0] = *p;
+  } else if constexpr (sizeof(T) * R == 8) {
+    const uint2 u = *reinterpret_cast<const uint2*>(p);
+    memcpy(out, &u, 8);
+  } else if constexpr (sizeof(T) * R == 16) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    memcpy(out, &u, 16);
+  } else {
+    const uint4 u0 = reinterpret_cast<const uint4*>(p)[0];
+    const uint4 u1 = reinterpret_cast<const uint4*>(p)[1];
+    memcpy(out, &u0, 16);
+    memcpy(reinterpret_cast<char*>(out) + 16, &u1, 16);
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void store_vec(T* __restrict__ p, const T (&in)[R]) {
+  if constexpr (sizeof(T) * R == 4) {
+    *p = in[0];
+  } else if constexpr (sizeof(T) * R == 8) {
+    uint2 u;
+    memcpy(&u, in, 8);
+    *reinterpret_cast<uint2*>(p) = u;
+  } else if constexpr (sizeof(T) * R == 16) {
+    uint4 u;
+    memcpy(&u, in, 16);
+    *reinterpret_cast<uint4*>(p) = u;
+  } else {
+    uint4 u0, u1;
+    memcpy(&u0, in, 16);
+    memcpy(&u1, reinterpret_cast<const char*>(in) + 16, 16);
+    reinterpret_cast<uint4*>(p)[0] = u0;
+    reinterpret_cast<uint4*>(p)[1] = u1;
+  }
+}
+
+// One Gauss-Seidel row update, ComputeSYMGS_ref.cpp:72-80: sum = r_i - sum_j a_ij x_j
+// (diagonal included, slot order), sum += x_i a_ii, x_i = sum / a_ii. FIRST: x
+// enters as zero; the masked-out slots (and the diagonal) multiply a zero.
+template <typename T, typename TR, bool FIRST, int SCHED>
+__device__ __forceinline__ void gs_row(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                                       const TR* __restrict__ rhs, T* x, int q, uint32_t mask) {
+  T sum = (T)rhs[q];
+  T xd = (T)0;
+  if (SCHED == kStaged) {
+    T a[kSlots];
+    int cl[kSlots];
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        if (mask & (1u << k)) {
-          a[k] = __ldcs(val + k * pitch + q);
-          cl[k] = __ldcs(col + k * pitch + q);
-        }
+    for (int k = 0; k < kSlots; ++k) {
+      if (mask & (1u << k)) {
+        a[k] = __ldcs(val + k * pitch + q);
+        cl[k] = __ldcs(col + k * pitch + q);
       }
-      T xv[kSlots];
+    }
+    T xv[kSlots];
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k)
-        if (mask & (1u << k)) xv[k] = __ldg(x + cl[k]);
+    for (int k = 0; k < kSlots; ++k)
+      if (mask & (1u << k)) xv[k] = __ldg(x + cl[k]);
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        if (mask & (1u << k)) {
-          sum -= a[k] * xv[k];
-          if (k == kDiagSlot) xd = xv[k];
-        }
+    for (int k = 0; k < kSlots; ++k) {
+      if (mask & (1u << k)) {
+        sum -= a[k] * xv[k];
+        if (k == kDiagSlot) xd = xv[k];
       }
-    } else {
+    }
+  } else {
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        if (mask & (1u << k)) {
-          const T a = val[k * pitch + q];
-          const T xv = __ldg(x + col[k * pitch + q]);
-          sum -= a * xv;
-          if (k == kDiagSlot) xd = xv;
+    for (int k = 0; k < kSlots; ++k) {
+      if (mask & (1u << k)) {
+        const T a = val[k * pitch + q];
+        const T xv = __ldg(x + col[k * pitch + q]);
+        sum -= a * xv;
+        if (k == kDiagSlot) xd = xv;
+      }
+    }
+  }
+  const T d = val[kDiagSlot * pitch + q];
+  if (!FIRST) sum += xd * d;
+  x[q] = sum / d;
+}
+
+// Gauss-Seidel colour phase: rows [r0, r1) of one colour, updated in parallel
+// (no two rows of a colour are neighbours).
+template <typename T, typename TR, bool FIRST, int CFG, int SCHED = cfg_sched(CFG), int R = cfg_rows(CFG)>
+__global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* __restrict__ val,
+                                                                      const int* __restrict__ col, int64_t pitch,
+                                                                      const TR* __restrict__ rhs, T* x, int r0,
+                                                                      int r1, uint32_t mask) {
+  if (R == 1) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride)
+      gs_row<T, TR, FIRST, SCHED>(val, col, pitch, rhs, x, q, mask);
+    return;
+  }
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+  for (int64_t q0 = r0 + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; q0 < r1; q0 += stride) {
+    if (q0 + R > r1) {
+      for (int q = (int)q0; q < r1; ++q) gs_row<T, TR, FIRST, kPlain>(val, col, pitch, rhs, x, q, mask);
+      continue;
+    }
+    TR rv[R];
+    load_vec<TR, R>(rhs + q0, rv);
+    T sum[R], xd[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      sum[r] = (T)rv[r];
+      xd[r] = (T)0;
+    }
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      if (mask & (1u << k)) {
+        T a[R];
+        int c[R];
+        load_vec<T, R>(val + k * pitch + q0, a);
+        load_vec<int, R>(col + k * pitch + q0, c);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const T xv = __ldg(x + c[r]);
+          sum[r] -= a[r] * xv;
+          if (k == kDiagSlot) xd[r] = xv;
         }
       }
     }
-    const T d = val[kDiagSlot * pitch + q];
-    if (!FIRST) sum += xd * d;
-    x[q] = sum / d;
+    T d[R], out[R];
+    load_vec<T, R>(val + kDiagSlot * pitch + q0, d);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (!FIRST) sum[r] += xd[r] * d[r];
+      out[r] = sum[r] / d[r];
+    }
+    store_vec<T, R>(x + q0, out);
   }
 }
 
@@ -146,45 +246,87 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
 // storage order each colour block would gather the other seven colours' x
 // across the whole grid again. Each warp still reads two contiguous runs of a
 // slot (the two parities of ix).
-template <typename T, bool DOT, int CFG, bool NAT, int SCHED = cfg_sched(CFG)>
+template <typename T, bool DOT, int CFG, bool NAT, int SCHED = cfg_sched(CFG), int R = NAT ? 1 : cfg_rows(CFG)>
 __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, const T* __restrict__ val,
                                                                   const int* __restrict__ col, int64_t pitch,
                                                                   const T* __restrict__ x, T* __restrict__ y, int n,
                                                                   double* __restrict__ partials) {
-  const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-    int q = t;
-    if (NAT) {
-      const int ix = t % g.nx, iy = (t / g.nx) % g.ny, iz = t / (g.nx * g.ny);
-      q = g.old2new(ix, iy, iz);
+  if (R == 1) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+      int q = t;
+      if (NAT) {
+        const int ix = t % g.nx, iy = (t / g.nx) % g.ny, iz = t / (g.nx * g.ny);
+        q = g.old2new(ix, iy, iz);
+      }
+      T sum = (T)0;
+      T xq = (T)0;
+      if (SCHED == kStaged) {
+        T a[kSlots];
+        int cl[kSlots];
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          a[k] = __ldcs(val + k * pitch + q);
+          cl[k] = __ldcs(col + k * pitch + q);
+        }
+        T xv[kSlots];
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) xv[k] = __ldg(x + cl[k]);
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) sum += a[k] * xv[k];
+        xq = xv[kDiagSlot];
+      } else {
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          const T xv = __ldg(x + col[k * pitch + q]);
+          sum += val[k * pitch + q] * xv;
+          if (k == kDiagSlot) xq = xv;
+        }
+      }
+      y[q] = sum;
+      if (DOT) acc += (double)xq * (double)sum;
     }
-    T sum = (T)0;
-    T xq = (T)0;
-    if (SCHED == kStaged) {
-      T a[kSlots];
-      int cl[kSlots];
+  } else {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
+    for (int64_t q0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; q0 < n; q0 += stride) {
+      const int cnt = q0 + R <= n ? R : (int)(n - q0);
+      if (cnt < R) {
+        for (int q = (int)q0; q < n; ++q) {
+          T sum = (T)0, xq = (T)0;
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            const T xv = __ldg(x + col[k * pitch + q]);
+            sum += val[k * pitch + q] * xv;
+            if (k == kDiagSlot) xq = xv;
+          }
+          y[q] = sum;
+          if (DOT) acc += (double)xq * (double)sum;
+        }
+        continue;
+      }
+      T sum[R], xq[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) sum[r] = xq[r] = (T)0;
 #pragma unroll
       for (int k = 0; k < kSlots; ++k) {
-        a[k] = __ldcs(val + k * pitch + q);
-        cl[k] = __ldcs(col + k * pitch + q);
+        T a[R];
+        int c[R];
+        load_vec<T, R>(val + k * pitch + q0, a);
+        load_vec<int, R>(col + k * pitch + q0, c);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const T xv = __ldg(x + c[r]);
+          sum[r] += a[r] * xv;
+          if (k == kDiagSlot) xq[r] = xv;
+        }
       }
-      T xv[kSlots];
+      store_vec<T, R>(y + q0, sum);
+      if (DOT) {
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) xv[k] = __ldg(x + cl[k]);
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k) sum += a[k] * xv[k];
-      xq = xv[kDiagSlot];
-    } else {
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        const T xv = __ldg(x + col[k * pitch + q]);
-        sum += val[k * pitch + q] * xv;
-        if (k == kDiagSlot) xq = xv;
+        for (int r = 0; r < R; ++r) acc += (double)xq[r] * (double)sum[r];
       }
     }
-    y[q] = sum;
-    if (DOT) acc += (double)xq * (double)sum;
   }
   if (DOT) {
     const double s = block_sum(acc);
@@ -363,6 +505,29 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const 
   }
   const double sum = block_sum(acc);
   if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+}
+
+// Implicit adjoint, value part: with lambda solving A' lambda = dL/dx (A is
+// symmetric), dL/da_ij = -lambda_i x_j for every stored slot. One thread per
+// natural row i writes its 27 slots out[i*27 + k] (0 for a direction that leaves
+// the grid), the layout hpcg_b200_set_values takes; lambda and x are in colour
+// order.
+__global__ void __launch_bounds__(kThreads) k_adjoint_values(ColourGrid g, const int* __restrict__ col,
+                                                             int64_t pitch, int n, const double* __restrict__ lam,
+                                                             const double* __restrict__ x,
+                                                             double* __restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int ix = i % g.nx, iy = (i / g.nx) % g.ny, iz = i / (g.nx * g.ny);
+    const int q = g.old2new(ix, iy, iz);
+    const double l = lam[q];
+    double* o = out + (int64_t)i * kSlots;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const int c = col[k * pitch + q];
+      o[k] = c == n ? 0.0 : -(l * x[c]);
+    }
+  }
 }
 
 // precision conversion for the FP32 V-cycle

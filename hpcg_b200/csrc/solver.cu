@@ -51,17 +51,25 @@ int grid_of(Context* c, K kernel, int64_t rows) {
 template <typename T, typename TR, bool FIRST, int CFG>
 void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask) {
   auto k = k_gs_phase<T, TR, FIRST, CFG>;
-  k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask);
+  const int64_t units = ((int64_t)(r1 - r0) + cfg_rows(CFG) - 1) / cfg_rows(CFG);
+  k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask);
 }
+
+// A configuration with R rows per thread needs the row range to start on a
+// multiple of R (vector loads); otherwise the scalar configuration 1 runs.
+inline int usable_cfg(int cfg, int r0) { return r0 % cfg_rows(cfg) == 0 ? cfg : 1; }
 
 template <typename T, typename TR, bool FIRST>
 void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rhs, T* x, int r0, int r1,
                  uint32_t mask) {
-  switch (cfg) {
+  switch (usable_cfg(cfg, r0)) {
     case 0: gs_launch<T, TR, FIRST, 0>(c, L, val, rhs, x, r0, r1, mask); break;
     case 1: gs_launch<T, TR, FIRST, 1>(c, L, val, rhs, x, r0, r1, mask); break;
     case 2: gs_launch<T, TR, FIRST, 2>(c, L, val, rhs, x, r0, r1, mask); break;
-    default: gs_launch<T, TR, FIRST, 3>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 3: gs_launch<T, TR, FIRST, 3>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 4: gs_launch<T, TR, FIRST, 4>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 5: gs_launch<T, TR, FIRST, 5>(c, L, val, rhs, x, r0, r1, mask); break;
+    default: gs_launch<T, TR, FIRST, 6>(c, L, val, rhs, x, r0, r1, mask); break;
   }
 }
 
@@ -74,7 +82,7 @@ int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, doub
     return g;
   }
   auto k = k_spmv<T, DOT, CFG, false>;
-  const int g = grid_of(c, k, L.n);
+  const int g = grid_of(c, k, ((int64_t)L.n + cfg_rows(CFG) - 1) / cfg_rows(CFG));
   k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
   return g;
 }
@@ -86,7 +94,10 @@ int spmv_dispatch(Context* c, const Level& L, const T* val, const T* x, T* y, do
     case 0: return spmv_launch<T, DOT, 0>(c, L, val, x, y, partials);
     case 1: return spmv_launch<T, DOT, 1>(c, L, val, x, y, partials);
     case 2: return spmv_launch<T, DOT, 2>(c, L, val, x, y, partials);
-    default: return spmv_launch<T, DOT, 3>(c, L, val, x, y, partials);
+    case 3: return spmv_launch<T, DOT, 3>(c, L, val, x, y, partials);
+    case 4: return spmv_launch<T, DOT, 4>(c, L, val, x, y, partials);
+    case 5: return spmv_launch<T, DOT, 5>(c, L, val, x, y, partials);
+    default: return spmv_launch<T, DOT, 6>(c, L, val, x, y, partials);
   }
 }
 
@@ -98,11 +109,11 @@ void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, cons
 
 template <typename T>
 void restrict_dispatch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
-  switch (L.mv_sched) {
-    case 0: restrict_launch<T, 0>(c, L, val, rf, xf, rc, nc); break;
-    case 1: restrict_launch<T, 1>(c, L, val, rf, xf, rc, nc); break;
+  switch (L.mv_sched) {  // scalar configurations only: the transfer pairs need not be contiguous
+    case 0: case 4: restrict_launch<T, 0>(c, L, val, rf, xf, rc, nc); break;
     case 2: restrict_launch<T, 2>(c, L, val, rf, xf, rc, nc); break;
-    default: restrict_launch<T, 3>(c, L, val, rf, xf, rc, nc); break;
+    case 3: restrict_launch<T, 3>(c, L, val, rf, xf, rc, nc); break;
+    default: restrict_launch<T, 1>(c, L, val, rf, xf, rc, nc); break;
   }
 }
 
@@ -113,10 +124,11 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
   const int kind = top ? (first ? kProfGsFirst : kProfGsFull) : -1;
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
+  const int cfg = sizeof(T) == 4 ? L.gs_sched32 : L.gs_sched;
   if (first)
-    gs_dispatch<T, TR, true>(c, L, L.gs_sched, val, rhs, x, r0, r1, first_mask(L.g, s));
+    gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, first_mask(L.g, s));
   else
-    gs_dispatch<T, TR, false>(c, L, L.gs_sched, val, rhs, x, r0, r1, kAllSlots);
+    gs_dispatch<T, TR, false>(c, L, cfg, val, rhs, x, r0, r1, kAllSlots);
   HB_CK(cudaGetLastError());
   return prof_end(c, kind, ev0, r1 - r0);
 }
@@ -408,6 +420,36 @@ int ensure_f32(hpcg_b200_problem* P) {
       HB_TRY(dev_alloc((void**)&L.x32, sizeof(float) * L.pitch, &P->bytes));
       HB_CK(cudaMemsetAsync(L.r32, 0, sizeof(float) * L.pitch, c->stream));
       HB_CK(cudaMemsetAsync(L.x32, 0, sizeof(float) * L.pitch, c->stream));
+      // FP32 phases load half the bytes per instruction: tune them on their own
+      // (on the level's FP32 work vectors, which every V-cycle rewrites)
+      const char* force = std::getenv("HPCG_B200_CONFIG");
+      if (force && *force) {
+        const int f = std::atoi(force);
+        L.gs_sched32 = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
+        continue;
+      }
+      const int r0 = L.g.start[1], r1 = L.g.start[2];
+      if (r1 <= r0) continue;
+      cudaEvent_t e0, e1;
+      HB_CK(cudaEventCreate(&e0));
+      HB_CK(cudaEventCreate(&e1));
+      float best = 1e30f;
+      for (int cfg = 0; cfg < kConfigs; ++cfg) {
+        float t = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+          HB_CK(cudaEventRecord(e0, c->stream));
+          gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
+          HB_CK(cudaEventRecord(e1, c->stream));
+          HB_CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+          t = ms < t ? ms : t;
+        }
+        if (t < best) { best = t; L.gs_sched32 = cfg; }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      HB_CK(cudaGetLastError());
     }
   }
   return HPCG_B200_OK;
@@ -594,6 +636,37 @@ int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max
   HB_TRY(load_vector(p, 0, x, p->x));
   HB_TRY(run_cg_mixed(p, max_iter, tolerance, niters, normr, normr0));
   return store_vector(p, 0, p->x, x);
+}
+
+int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, int max_iter, double tolerance,
+                      double* grad_b, double* grad_values27, int* niters) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!x || !g || !grad_b || !grad_values27 || !niters || max_iter < 0) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  const Level& L = p->lev[0];
+  Context* c = p->ctx;
+  // lambda: A lambda = g with the same preconditioned CG, from lambda = 0
+  HB_TRY(load_vector(p, 0, g, p->b));
+  HB_CK(cudaMemsetAsync(p->x, 0, sizeof(double) * L.pitch, c->stream));
+  double nr = 0, nr0 = 0;
+  HB_TRY(run_cg(p, max_iter, tolerance, true, niters, &nr, &nr0, nullptr));
+  HB_TRY(store_vector(p, 0, p->x, grad_b));  // dL/db = lambda
+  HB_TRY(load_vector(p, 0, x, p->Ap));       // the forward solution, colour order
+  double* out = grad_values27;
+  const bool dev_out = is_device_ptr(grad_values27);
+  const size_t bytes = sizeof(double) * kSlots * (size_t)L.n;
+  if (!dev_out) HB_CK(cudaMalloc(&out, bytes));
+  k_adjoint_values<<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.g, L.col, L.pitch, L.n, p->x,
+                                                                                    p->Ap, out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && !dev_out) e = cudaMemcpyAsync(grad_values27, out, bytes, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (!dev_out) cudaFree(out);
+  if (e != cudaSuccess) {
+    set_error("hpcg_b200_adjoint", e);
+    return status_of(e);
+  }
+  return HPCG_B200_OK;
 }
 
 int hpcg_b200_dot(int n, const double* x, const double* y, double* result) {

@@ -133,6 +133,18 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
 int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0);
 
+/* ---- changed form 3: implicit adjoint of the solve ------------------------ */
+
+/* Gradients of a loss L(x) through the solve A x = b, given the converged
+ * forward solution x and g = dL/dx (both natural order). Solves A lambda = g
+ * with the same preconditioned CG and hierarchy (A is symmetric, so A' = A),
+ * from lambda = 0 to `tolerance`, then writes dL/db = lambda into grad_b and
+ * dL/da = -lambda_i x_j into grad_values27, in the layout of
+ * hpcg_b200_set_values (natural rows, 27 direction slots, 0 outside the grid).
+ * Keeps no iterate history. No reference counterpart (changed form). */
+int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, int max_iter, double tolerance,
+                      double* grad_b, double* grad_values27, int* niters);
+
 /* ---- dot product without device allocation -------------------------------- */
 
 /* result[0] = x'y over n entries, for callers that cannot allocate device

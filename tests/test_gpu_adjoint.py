@@ -1,0 +1,93 @@
+"""The implicit adjoint on the GPU (hpcg_b200_adjoint, through the C ABI and the
+torch.autograd shim), on the perturbed symmetric stencil at 16^3:
+
+* against the FP64 host adjoint built on the oracle's CG_ref restatement
+  (relative 1e-8 of the largest component);
+* against central finite differences with step 1e-6 on 64 seeded coordinates
+  (48 value slots, 16 right-hand-side entries): relative 1e-6 per coordinate
+  (components below 1e-3 of the largest are held to 1e-6 of that floor)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+pytest.importorskip("scipy")
+import scipy.sparse.linalg as spla  # noqa: E402
+
+from hpcg_b200 import perturbed as PT  # noqa: E402
+from test_adjoint_host import (central_difference_rhs, central_difference_slot, host_adjoint,  # noqa: E402
+                               perturbed_levels, sparse_from_slots)
+
+N = 16
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def adj_case(binding):
+    n = N ** 3
+    v = PT.perturbed_values(N, N, N)
+    b = PT.rhs_uniform(n)
+    xt = PT.target_normal(n)
+    P = binding.Problem.generate(N)
+    P.set_values(0, v)
+    x = np.zeros(n)
+    P.CG(b, x, 2000, TOL, True)
+    g = x - xt
+    gb = np.zeros(n)
+    gv = np.zeros((n, 27))
+    P.adjoint(x, g, 2000, TOL, gb, gv)
+    yield dict(P=P, v=v, b=b, xt=xt, x=x, gb=gb, gv=gv)
+    P.free()
+
+
+def test_forward_solve_matches_direct(adj_case):
+    c = adj_case
+    A = sparse_from_slots(c["v"], N, N, N).tocsc()
+    xd = spla.spsolve(A, c["b"])
+    assert np.max(np.abs(c["x"] - xd)) <= 1e-9 * np.max(np.abs(xd))
+
+
+def test_adjoint_matches_host_adjoint(oracle, adj_case):
+    c = adj_case
+    levels = perturbed_levels(oracle, N, N, N, c["v"])
+    lam, gv = host_adjoint(oracle, levels, c["v"], c["x"], c["x"] - c["xt"])
+    assert np.max(np.abs(c["gb"] - lam)) <= 1e-8 * np.max(np.abs(lam))
+    assert np.max(np.abs(c["gv"] - gv)) <= 1e-8 * np.max(np.abs(gv))
+    assert np.all(c["gv"][c["v"] == 0.0] == 0.0)
+
+
+def test_adjoint_matches_finite_differences(adj_case):
+    c = adj_case
+    n = N ** 3
+    v, b, xt, x = c["v"], c["b"], c["xt"], c["x"]
+    A = sparse_from_slots(v, N, N, N).tocsc()
+    rng = np.random.default_rng(0x48504347)
+    floor_v = 1e-3 * np.abs(c["gv"]).max()
+    slots = 0
+    while slots < 48:
+        i, k = int(rng.integers(n)), int(rng.integers(27))
+        if v[i, k] == 0.0:
+            continue
+        fd = central_difference_slot(v, b, xt, i, k, 1e-6, N, N, N)
+        adj = c["gv"][i, k]
+        assert abs(fd - adj) <= 1e-6 * max(abs(adj), floor_v), (i, k, fd, adj)
+        slots += 1
+    floor_b = 1e-3 * np.abs(c["gb"]).max()
+    for i in rng.integers(n, size=16):
+        fd = central_difference_rhs(A, b, xt, x, int(i), 1e-6)
+        adj = c["gb"][i]
+        assert abs(fd - adj) <= 1e-6 * max(abs(adj), floor_b), (i, fd, adj)
+
+
+def test_autograd_shim(binding, adj_case):
+    import torch
+    from hpcg_b200.autograd import HpcgSolve
+    c = adj_case
+    dev = "cuda"
+    v = torch.tensor(c["v"], device=dev, requires_grad=True)
+    b = torch.tensor(c["b"], device=dev, requires_grad=True)
+    xt = torch.tensor(c["xt"], device=dev)
+    x = HpcgSolve.apply(v, b, c["P"], TOL, 2000)
+    loss = 0.5 * torch.sum((x - xt) ** 2)
+    loss.backward()
+    assert np.max(np.abs(v.grad.cpu().numpy() - c["gv"])) <= 1e-10 * np.abs(c["gv"]).max()
+    assert np.max(np.abs(b.grad.cpu().numpy() - c["gb"])) <= 1e-10 * np.abs(c["gb"]).max()
