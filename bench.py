@@ -49,6 +49,7 @@ def parse():
                     help="right-hand side(s) of the mixed-precision comparison: b = 27 - nnz, U[-1,1], or both")
     ap.add_argument("--mixed-tol", type=float, default=1e-9)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 128^3 implicit-adjoint timing")
+    ap.add_argument("--no-multi", action="store_true", help="skip the 256^3, 8 right-hand-side comparison")
     return ap.parse_args()
 
 
@@ -260,6 +261,41 @@ def adjoint_timing(dev, n=128, tol=1e-10):
         P.free()
 
 
+def multi_rhs(dev, n=256, k=8, tol=1e-9, max_iter=2000):
+    """k systems b_j ~ U[-1, 1] (seeded) on the n^3 problem: the lockstep solver
+    (hpcg_b200_cg_multi) against k one-at-a-time solves (hpcg_b200_cg)."""
+    import numpy as np
+    import torch
+    from hpcg_b200 import binding as B
+    nrow = n ** 3
+    P = B.Problem.generate(n, n, n, 4, dev)
+    try:
+        lib_stream = torch.cuda.ExternalStream(B.stream(dev), device=dev)
+        rng = np.random.Generator(np.random.PCG64(RHS_SEED))
+        b = torch.from_numpy(rng.uniform(-1.0, 1.0, (k, nrow))).to(f"cuda:{dev}")
+        x = torch.zeros_like(b)
+        P.CG_multi(b[:, :], x, 1, tol)  # first use allocates the multi-system vectors
+        x.zero_()
+        (ni, nr, nr0), t_multi = timed(lib_stream, lambda: P.CG_multi(b, x, max_iter, tol))
+        xs = torch.zeros(nrow, dtype=torch.float64, device=f"cuda:{dev}")
+        iters_single, t_single = [], 0.0
+        for j in range(k):
+            xs.zero_()
+            bj = b[j].contiguous()
+            (it, _, _), t = timed(lib_stream, lambda: P.CG(bj, xs, max_iter, tol, True))
+            iters_single.append(it)
+            t_single += t
+        return {"grid": [n, n, n], "rhs": k, "tolerance": tol,
+                "lockstep": {"iters": [int(v) for v in ni], "seconds": round(t_multi, 3),
+                             "solves_per_s": round(k / t_multi, 3),
+                             "max_scaled_residual": float(np.max(nr / nr0))},
+                "one_at_a_time": {"iters": iters_single, "seconds": round(t_single, 3),
+                                  "solves_per_s": round(k / t_single, 3)},
+                "speedup": round(t_single / t_multi, 3)}
+    finally:
+        P.free()
+
+
 def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000):
     """Time to a relative residual `tol` from x = 0: FP64 PCG (hpcg_b200_cg) against
     FP64 flexible PCG around the FP32 V-cycle (hpcg_b200_cg_mixed)."""
@@ -396,6 +432,9 @@ def b200_arm(args, rank, world, local_rank):
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_timing(dev)
+    multi = None
+    if not args.no_multi:
+        multi = multi_rhs(dev)
 
     line = None
     if rank == 0:
@@ -442,6 +481,8 @@ def b200_arm(args, rank, world, local_rank):
             line["mixed_precision"] = mixed
         if adjoint:
             line["adjoint"] = adjoint
+        if multi:
+            line["multi_rhs"] = multi
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(args)

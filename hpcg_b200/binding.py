@@ -36,7 +36,8 @@ EXPORTS = (
     "hpcg_b200_spmv", "hpcg_b200_symgs", "hpcg_b200_mg", "hpcg_b200_dot", "hpcg_b200_waxpby",
     "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
-    "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_last_error",
+    "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
+    "hpcg_b200_last_error",
 )
 
 
@@ -92,6 +93,8 @@ def lib():
         l.hpcg_b200_profile_read.argtypes = [i, i, C.POINTER(d), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         l.hpcg_b200_dot_noalloc.argtypes = [i, vp, vp, vp, vp]
         l.hpcg_b200_adjoint.argtypes = [vp, vp, vp, i, d, vp, vp, C.POINTER(i)]
+        l.hpcg_b200_cg_multi.argtypes = [vp, i, vp, vp, i, d, vp, vp, vp]
+        l.hpcg_b200_mg_multi.argtypes = [vp, i, vp, vp]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -243,6 +246,24 @@ class Problem:
         _check(lib().hpcg_b200_cg_mixed(self._h, _ptr(b, self.nrow), _ptr(x, self.nrow), max_iter, tolerance,
                                         C.byref(ni), C.byref(nr), C.byref(nr0)), "CG_mixed")
         return ni.value, nr.value, nr0.value
+
+    def CG_multi(self, b, x, max_iter, tolerance):
+        """nrhs = len(b) / nrow systems (b, x: [nrhs, nrow] contiguous float64).
+        Returns (niters, normr, normr0) as numpy arrays, x updated in place."""
+        nrhs = (b.size if isinstance(b, np.ndarray) else b.numel()) // self.nrow
+        ni = np.zeros(nrhs, np.int32)
+        nr = np.zeros(nrhs)
+        nr0 = np.zeros(nrhs)
+        _check(lib().hpcg_b200_cg_multi(self._h, nrhs, _ptr(b, nrhs * self.nrow), _ptr(x, nrhs * self.nrow),
+                                        max_iter, tolerance, ni.ctypes.data, nr.ctypes.data, nr0.ctypes.data),
+               "hpcg_b200_cg_multi")
+        return ni, nr, nr0
+
+    def ComputeMG_multi(self, r, x):
+        nrhs = (r.size if isinstance(r, np.ndarray) else r.numel()) // self.nrow
+        _check(lib().hpcg_b200_mg_multi(self._h, nrhs, _ptr(r, nrhs * self.nrow), _ptr(x, nrhs * self.nrow)),
+               "hpcg_b200_mg_multi")
+        return 0
 
     def adjoint(self, x, g, max_iter, tolerance, grad_b, grad_values27):
         """Implicit adjoint of the solve: grad_b = lambda (A lambda = g), grad_values27

@@ -81,6 +81,18 @@ struct ColourGrid {
   }
 };
 
+// Slots read by a first-sweep colour phase: neighbours of colours swept
+// earlier in this sweep. All others (and the diagonal) multiply x = 0.
+inline uint32_t first_mask(const ColourGrid& g, int s) {
+  const int c = g.sweep[s];
+  uint32_t m = 0;
+  for (int k = 0; k < kSlots; ++k) {
+    if (k == kDiagSlot) continue;
+    if (g.pos[c ^ slot_flip(k)] < s) m |= 1u << k;
+  }
+  return m;
+}
+
 struct Level {
   ColourGrid g;
   int n = 0;                 // rows
@@ -110,6 +122,7 @@ struct Level {
 };
 
 struct Context;
+struct MultiState;
 
 }  // namespace hb
 
@@ -122,6 +135,7 @@ struct hpcg_b200_problem {
   int symgs_mode;
   // level-0 vectors, colour order, [pitch] each
   double *b, *x, *r, *z, *p, *Ap, *zprev;
+  hb::MultiState* multi;  // work vectors of the multi-system path (created on first use)
   size_t bytes;  // device bytes held
 };
 
@@ -212,8 +226,30 @@ inline int grid_for(const Context* c, int64_t work, int threads, int per_sm) {
   return (int)blocks;
 }
 
+// Releases the multi-system work vectors of p (multi.cu).
+void free_multi(hpcg_b200_problem* p);
+
 // Builds the sorted transfer pairs (tf, tq) of level l from its device f2c.
 int build_transfer(hpcg_b200_problem* p, int l);
+
+constexpr uint32_t kAllSlots = (1u << kSlots) - 1;
+
+// Resident blocks per SM of a kernel (at least 1).
+template <typename K>
+int resident(K kernel) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 1;
+  }
+  return b;
+}
+
+// Grid of a grid-stride row kernel: every SM filled once with resident blocks.
+template <typename K>
+int grid_of(Context* c, K kernel, int64_t rows) {
+  return grid_for(c, rows, 256, resident(kernel));
+}
 
 // natural <-> colour order vector movement (solver.cu)
 int load_vector(hpcg_b200_problem* p, int level, const double* src_natural, double* dst_colour);

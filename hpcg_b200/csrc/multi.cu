@@ -1,0 +1,295 @@
+// Multi-right-hand-side solves: hpcg_b200_cg_multi and hpcg_b200_mg_multi.
+// K systems with the same matrix advance in lockstep through the kernels of
+// kernels_multi.cuh; each matrix row is read once per sweep for all K.
+#include <cmath>
+#include <vector>
+
+#include "kernels_multi.cuh"
+
+namespace hb {
+
+void release_accounted(size_t bytes);
+
+// Work vectors of the multi-system path, interleaved [row][K], per level.
+struct MultiState {
+  int K = 0;
+  double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
+  double* lr[kMaxLevels] = {nullptr};  // coarse right-hand sides (levels > 0)
+  double* lx[kMaxLevels] = {nullptr};  // coarse solutions (levels > 0)
+  double* stage = nullptr;             // natural, system-major staging (nrhs * n)
+  size_t stage_cap = 0;
+  double* partials = nullptr;          // [K][kParts]
+  MScalars* s = nullptr;
+  MScalars* s_host = nullptr;
+  size_t bytes = 0;
+};
+
+namespace {
+
+constexpr int kParts = 1024;  // reduction blocks of the vector kernels (fixed: deterministic)
+
+void free_state(MultiState* m) {
+  if (!m) return;
+  void* v[] = {m->b, m->x, m->r, m->z, m->p, m->Ap, m->stage, m->partials, m->s};
+  for (void* q : v) cudaFree(q);
+  for (int l = 0; l < kMaxLevels; ++l) {
+    cudaFree(m->lr[l]);
+    cudaFree(m->lx[l]);
+  }
+  if (m->s_host) cudaFreeHost(m->s_host);
+  release_accounted(m->bytes);
+  delete m;
+}
+
+int alloc_z(MultiState* m, double** p, size_t count, cudaStream_t st) {
+  HB_TRY(dev_alloc((void**)p, sizeof(double) * count, &m->bytes));
+  HB_CK(cudaMemsetAsync(*p, 0, sizeof(double) * count, st));
+  return HPCG_B200_OK;
+}
+
+// The state for K systems (re-created when K changes). Vectors are zeroed, so
+// the zero row n of every level (padded stencil slots) reads 0 for all K.
+int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
+  MultiState*& m = P->multi;
+  if (m && m->K == K) {
+    *out = m;
+    return HPCG_B200_OK;
+  }
+  free_state(m);
+  m = new MultiState;
+  m->K = K;
+  cudaStream_t st = P->ctx->stream;
+  const Level& L0 = P->lev[0];
+  double** v0[] = {&m->b, &m->x, &m->r, &m->z, &m->p, &m->Ap};
+  for (double** v : v0) HB_TRY(alloc_z(m, v, (size_t)L0.pitch * K, st));
+  for (int l = 1; l < P->nlev; ++l) {
+    HB_TRY(alloc_z(m, &m->lr[l], (size_t)P->lev[l].pitch * K, st));
+    HB_TRY(alloc_z(m, &m->lx[l], (size_t)P->lev[l].pitch * K, st));
+  }
+  HB_TRY(alloc_z(m, &m->partials, (size_t)kMaxRhs * kParts, st));
+  HB_TRY(dev_alloc((void**)&m->s, sizeof(MScalars), &m->bytes));
+  HB_CK(cudaMemsetAsync(m->s, 0, sizeof(MScalars), st));
+  HB_CK(cudaMallocHost(&m->s_host, sizeof(MScalars)));
+  *out = m;
+  return HPCG_B200_OK;
+}
+
+template <int K>
+int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first) {
+  int last = -1;
+  for (int s = 0; s < kColours; ++s) {
+    const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
+    if (r1 <= r0) continue;
+    last = s;
+    if (first) {
+      auto k = k_gs_phase_m<K, true>;
+      k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1,
+                                                              first_mask(L.g, s));
+    } else {
+      auto k = k_gs_phase_m<K, false>;
+      k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+    }
+  }
+  // backward sweep, without repeating the last colour (as the single-system path)
+  for (int s = last - 1; s >= 0; --s) {
+    const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
+    if (r1 <= r0) continue;
+    auto k = k_gs_phase_m<K, false>;
+    k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+  }
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+// ComputeMG_ref.cpp:39-63 for K systems on level l (colour order, interleaved).
+template <int K>
+int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x) {
+  const Level& L = P->lev[l];
+  Context* c = P->ctx;
+  HB_TRY(gs_colour_m<K>(c, L, r, x, true));
+  if (l + 1 < P->nlev) {
+    const Level& C = P->lev[l + 1];
+    auto kr = k_restrict_m<K>;
+    kr<<<grid_of(c, kr, C.n), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x, L.tf, L.tq, m->lr[l + 1], C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(mg_m<K>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1]));
+    auto kp = k_prolong_m<K>;
+    kp<<<grid_of(c, kp, C.n), kThreads, 0, c->stream>>>(L.tf, L.tq, m->lx[l + 1], x, C.n);
+    HB_CK(cudaGetLastError());
+    HB_TRY(gs_colour_m<K>(c, L, r, x, false));
+  }
+  return HPCG_B200_OK;
+}
+
+// system-major natural src (host or device) -> interleaved colour-order dst
+template <int K>
+int load_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, double* dst) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const double* s = src;
+  if (!is_device_ptr(src)) {
+    const size_t need = (size_t)nrhs * L.n;
+    if (m->stage_cap < need) {
+      cudaFree(m->stage);
+      m->stage = nullptr;
+      m->stage_cap = 0;
+      HB_CK(cudaMalloc(&m->stage, sizeof(double) * need));
+      m->stage_cap = need;
+    }
+    HB_CK(cudaMemcpyAsync(m->stage, src, sizeof(double) * need, cudaMemcpyHostToDevice, c->stream));
+    s = m->stage;
+  }
+  auto k = k_gather_in_m<K>;
+  k<<<grid_of(c, k, L.n), kThreads, 0, c->stream>>>(dst, s, L.new2old, L.n, nrhs);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+template <int K>
+int store_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, double* dst) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const bool dev = is_device_ptr(dst);
+  double* d = dst;
+  const size_t need = (size_t)nrhs * L.n;
+  if (!dev) {
+    if (m->stage_cap < need) {
+      cudaFree(m->stage);
+      m->stage = nullptr;
+      m->stage_cap = 0;
+      HB_CK(cudaMalloc(&m->stage, sizeof(double) * need));
+      m->stage_cap = need;
+    }
+    d = m->stage;
+  }
+  auto k = k_scatter_out_m<K>;
+  k<<<grid_of(c, k, L.n), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n, nrhs);
+  HB_CK(cudaGetLastError());
+  if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  return HPCG_B200_OK;
+}
+
+template <int K>
+int finalize_m(Context* c, MultiState* m, int op, int iter, double tol) {
+  k_finalize_m<K><<<1, kThreads, 0, c->stream>>>(m->partials, kParts, op, m->s, iter, tol);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+// CG.cpp:59-143 for K systems in lockstep; a system stops updating once its
+// scaled residual is at or below the tolerance; the loop ends when none is left
+// or after max_iter iterations.
+template <int K>
+int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any_iters) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const int n = L.n;
+  auto ks = k_spmv_m<K, false>;
+  ks<<<grid_of(c, ks, n), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->x, m->Ap, n, nullptr);
+  k_resid_m<K><<<kParts, kThreads, 0, c->stream>>>(m->b, m->Ap, m->r, n, m->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize_m<K>(c, m, kMNorm0, 0, tol));
+  HB_CK(cudaMemcpyAsync(m->s_host, m->s, sizeof(MScalars), cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  int k = 1;
+  for (; k <= max_iter; ++k) {
+    bool any = false;
+    for (int j = 0; j < K; ++j) any = any || m->s_host->active[j];
+    if (!any) break;
+    HB_TRY(mg_m<K>(P, m, 0, m->r, m->z));
+    k_dot_m<K><<<kParts, kThreads, 0, c->stream>>>(m->r, m->z, n, m->partials);
+    HB_CK(cudaGetLastError());
+    if (k == 1) {
+      HB_TRY(finalize_m<K>(c, m, kMRtzFirst, k, tol));
+      HB_CK(cudaMemcpyAsync(m->p, m->z, sizeof(double) * (size_t)n * K, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      HB_TRY(finalize_m<K>(c, m, kMRtz, k, tol));
+      k_update_p_m<K><<<kParts, kThreads, 0, c->stream>>>(m->z, m->p, n, m->s);
+      HB_CK(cudaGetLastError());
+    }
+    k_spmv_m<K, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, n, m->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize_m<K>(c, m, kMPap, k, tol));
+    k_update_xr_m<K><<<kParts, kThreads, 0, c->stream>>>(m->x, m->p, m->r, m->Ap, n, m->s, m->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize_m<K>(c, m, kMNormr, k, tol));
+    HB_CK(cudaMemcpyAsync(m->s_host, m->s, sizeof(MScalars), cudaMemcpyDeviceToHost, c->stream));
+    HB_CK(cudaStreamSynchronize(c->stream));
+  }
+  *any_iters = k - 1;
+  return HPCG_B200_OK;
+}
+
+template <int K>
+int run_cg_multi(hpcg_b200_problem* P, int nrhs, const double* b, double* x, int max_iter, double tol, int* niters,
+                 double* normr, double* normr0) {
+  MultiState* m = nullptr;
+  HB_TRY(ensure_state(P, K, &m));
+  HB_TRY(load_m<K>(P, m, nrhs, b, m->b));
+  HB_TRY(load_m<K>(P, m, nrhs, x, m->x));
+  int done = 0;
+  HB_TRY(cg_m<K>(P, m, max_iter, tol, &done));
+  HB_TRY(store_m<K>(P, m, nrhs, m->x, x));
+  for (int j = 0; j < nrhs; ++j) {
+    niters[j] = m->s_host->niters[j];
+    normr[j] = std::sqrt(m->s_host->normr2[j]);
+    normr0[j] = m->s_host->normr0[j];
+  }
+  return HPCG_B200_OK;
+}
+
+template <int K>
+int run_mg_multi(hpcg_b200_problem* P, int nrhs, const double* r, double* x) {
+  MultiState* m = nullptr;
+  HB_TRY(ensure_state(P, K, &m));
+  HB_TRY(load_m<K>(P, m, nrhs, r, m->r));
+  HB_TRY(mg_m<K>(P, m, 0, m->r, m->z));
+  return store_m<K>(P, m, nrhs, m->z, x);
+}
+
+struct Setter {
+  int prev = -1;
+  explicit Setter(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~Setter() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+void free_multi(hpcg_b200_problem* p) {
+  free_state(p->multi);
+  p->multi = nullptr;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+int hpcg_b200_cg_multi(hpcg_b200_problem* p, int nrhs, const double* b, double* x, int max_iter, double tolerance,
+                       int* niters, double* normr, double* normr0) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (nrhs < 1 || nrhs > kMaxRhs || !b || !x || !niters || !normr || !normr0 || max_iter < 0)
+    return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  if (nrhs <= 2) return run_cg_multi<2>(p, nrhs, b, x, max_iter, tolerance, niters, normr, normr0);
+  if (nrhs <= 4) return run_cg_multi<4>(p, nrhs, b, x, max_iter, tolerance, niters, normr, normr0);
+  return run_cg_multi<8>(p, nrhs, b, x, max_iter, tolerance, niters, normr, normr0);
+}
+
+int hpcg_b200_mg_multi(hpcg_b200_problem* p, int nrhs, const double* r, double* x) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (nrhs < 1 || nrhs > kMaxRhs || !r || !x) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  if (nrhs <= 2) return run_mg_multi<2>(p, nrhs, r, x);
+  if (nrhs <= 4) return run_mg_multi<4>(p, nrhs, r, x);
+  return run_mg_multi<8>(p, nrhs, r, x);
+}
+
+}  // extern "C"

@@ -168,6 +168,7 @@ int free_problem(hpcg_b200_problem* p) {
   }
   void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
   for (void* q : vs) dev_free(q);
+  free_multi(p);
   release_accounted(p->bytes);
   p->magic = 0;
   delete p;

@@ -11,41 +11,11 @@ namespace hb {
 
 namespace {
 
-constexpr uint32_t kAllSlots = (1u << kSlots) - 1;
 constexpr int kPerSm = 8;  // resident 256-thread blocks per SM targeted by grid-stride kernels
 
 inline int red_blocks(const Context* c, int64_t n) {
   int b = grid_for(c, n, kThreads, kPerSm);
   return b > kRedBlocksMax / 2 ? kRedBlocksMax / 2 : b;
-}
-
-// Slots read by a first-sweep colour phase: neighbours of colours swept
-// earlier in this sweep. All others (and the diagonal) multiply x = 0.
-uint32_t first_mask(const ColourGrid& g, int s) {
-  const int c = g.sweep[s];
-  uint32_t m = 0;
-  for (int k = 0; k < kSlots; ++k) {
-    if (k == kDiagSlot) continue;
-    if (g.pos[c ^ slot_flip(k)] < s) m |= 1u << k;
-  }
-  return m;
-}
-
-// Resident blocks per SM of a kernel (at least 1).
-template <typename K>
-int resident(K kernel) {
-  int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0) != cudaSuccess || b < 1) {
-    cudaGetLastError();
-    b = 1;
-  }
-  return b;
-}
-
-// Grid of a grid-stride row kernel: every SM filled once with resident blocks.
-template <typename K>
-int grid_of(Context* c, K kernel, int64_t rows) {
-  return grid_for(c, rows, kThreads, resident(kernel));
 }
 
 template <typename T, typename TR, bool FIRST, int CFG>

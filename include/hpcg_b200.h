@@ -133,6 +133,22 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
 int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0);
 
+/* ---- changed form 2: several right-hand sides at once ---------------------- */
+
+/* Preconditioned CG (CG.cpp:59-143 semantics) for nrhs <= 8 systems with the
+ * problem's matrix, advanced in lockstep so that every matrix row is read once
+ * per sweep for all of them. b and x hold the systems one after another:
+ * b[j*n + i], natural order, n = rows (host or device memory); x is the initial
+ * guess on entry and the solution on exit. System j stops updating once
+ * normr_j / normr0_j <= tolerance; niters, normr and normr0 receive one value per
+ * system. No reference counterpart (changed form). */
+int hpcg_b200_cg_multi(hpcg_b200_problem* p, int nrhs, const double* b, double* x, int max_iter, double tolerance,
+                       int* niters, double* normr, double* normr0);
+
+/* x_j = V-cycle(r_j) for nrhs <= 8 systems, layout as hpcg_b200_cg_multi. Each
+ * x_j is bitwise what hpcg_b200_mg gives for r_j. */
+int hpcg_b200_mg_multi(hpcg_b200_problem* p, int nrhs, const double* r, double* x);
+
 /* ---- changed form 3: implicit adjoint of the solve ------------------------ */
 
 /* Gradients of a loss L(x) through the solve A x = b, given the converged
