@@ -136,6 +136,8 @@ struct hpcg_b200_problem {
   // level-0 vectors, colour order, [pitch] each
   double *b, *x, *r, *z, *p, *Ap, *zprev;
   hb::MultiState* multi;  // work vectors of the multi-system path (created on first use)
+  cudaGraphExec_t cg_graph[2];  // instantiated CG loop, [unpreconditioned, preconditioned]
+  bool cg_graph_failed;         // capture was refused once: stay with stream launches
   size_t bytes;  // device bytes held
 };
 
@@ -165,6 +167,10 @@ constexpr int kRedBlocksMax = 4096;  // reduction partial slots
 
 struct Scalars {
   double rtz, oldrtz, alpha, beta, pAp, normr2, rzprev, tmp;
+  // loop state of the graph-launched CG (CG.cpp:100's condition on the device)
+  double normr0, tol;
+  int iter;      // iterations completed
+  int max_iter;
 };
 
 // Kernel classes timed by the optional launch profiler.

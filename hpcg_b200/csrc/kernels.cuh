@@ -379,6 +379,8 @@ enum FinOp : int {
   kFinPap = 4,       // pAp = sum; alpha = rtz / pAp                    (CG.cpp:119-120)
   kFinFlex = 5,      // oldrtz = rtz; rtz = sum; beta = (rtz - sum2) / oldrtz (flexible PR)
   kFinMax = 6,       // *out = max of partials
+  kFinNormr0 = 7,    // normr2 = sum; normr0 = sqrt(sum)           (CG.cpp:89-96)
+  kFinRtzIter = 8,   // iteration 1: rtz = sum; later: as kFinRtz  (CG.cpp:107-115)
 };
 
 // One block: fixed-order reduction of nparts partials (and of the second set
@@ -405,6 +407,16 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const double* __restrict_
     case kFinRtz: s->oldrtz = s->rtz; s->rtz = sum; s->beta = sum / s->oldrtz; break;
     case kFinPap: s->pAp = sum; s->alpha = s->rtz / sum; break;
     case kFinFlex: s->oldrtz = s->rtz; s->rtz = sum; s->rzprev = sum2; s->beta = (sum - sum2) / s->oldrtz; break;
+    case kFinNormr0: s->normr2 = sum; s->normr0 = sqrt(sum); break;
+    case kFinRtzIter:
+      if (s->iter == 0) {
+        s->rtz = sum;
+      } else {
+        s->oldrtz = s->rtz;
+        s->rtz = sum;
+        s->beta = sum / s->oldrtz;
+      }
+      break;
     default: break;
   }
 }
@@ -415,6 +427,33 @@ __global__ void __launch_bounds__(kThreads) k_update_p(int n, const double* __re
   const double beta = s->beta;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = z[i] + beta * p[i];
+}
+
+// Iteration 1: p = z (CG.cpp:109); later iterations: p = z + beta p (CG.cpp:115).
+__global__ void __launch_bounds__(kThreads) k_update_p_iter(int n, const double* __restrict__ z, double* p,
+                                                            const Scalars* __restrict__ s) {
+  const bool first = s->iter == 0;
+  const double beta = s->beta;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = first ? z[i] : z[i] + beta * p[i];
+}
+
+// The loop condition of CG.cpp:100, k <= max_iter && normr/normr0 > tolerance,
+// evaluated on the device for the graph's while node. advance = 0 before the
+// loop (no iteration done yet), 1 at the end of each iteration.
+__global__ void k_cg_condition(Scalars* s, cudaGraphConditionalHandle h, int advance) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  s->iter = advance ? s->iter + 1 : 0;
+  const bool go = s->iter + 1 <= s->max_iter && sqrt(s->normr2) / s->normr0 > s->tol;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void k_cg_setup(Scalars* s, int max_iter, double tol) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s->max_iter = max_iter;
+    s->tol = tol;
+    s->iter = 0;
+  }
 }
 
 // x = x + alpha p; r = r + (-alpha) Ap (CG.cpp:121-122); partials of r'r (CG.cpp:123).

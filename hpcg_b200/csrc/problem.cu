@@ -169,6 +169,8 @@ int free_problem(hpcg_b200_problem* p) {
   void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
   for (void* q : vs) dev_free(q);
   free_multi(p);
+  for (int i = 0; i < 2; ++i)
+    if (p->cg_graph[i]) cudaGraphExecDestroy(p->cg_graph[i]);
   release_accounted(p->bytes);
   p->magic = 0;
   delete p;
@@ -416,6 +418,14 @@ int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27
 int hpcg_b200_set_symgs_mode(hpcg_b200_problem* p, int mode) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   if (mode != HPCG_B200_SYMGS_COLOUR && mode != HPCG_B200_SYMGS_NATURAL) return HPCG_B200_ERR_ARG;
+  if (mode != p->symgs_mode) {
+    // a captured CG loop holds the previous mode's kernels
+    cudaSetDevice(p->device);
+    for (int i = 0; i < 2; ++i) {
+      if (p->cg_graph[i]) cudaGraphExecDestroy(p->cg_graph[i]);
+      p->cg_graph[i] = nullptr;
+    }
+  }
   p->symgs_mode = mode;
   return HPCG_B200_OK;
 }

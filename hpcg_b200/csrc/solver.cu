@@ -2,6 +2,7 @@
 // routines, with the host-side drivers that sequence the kernels.
 #include <chrono>
 #include <cstdlib>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
@@ -285,9 +286,151 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// ---- the CG loop as one CUDA graph ------------------------------------------
+
+bool graph_enabled() {
+  const char* e = std::getenv("HPCG_B200_GRAPH");
+  return !(e && e[0] == '0');
+}
+
+// One CG iteration (CG.cpp:101-125) with the iteration-aware kernels: the body
+// of the graph's while node.
+int cg_iteration_body(hpcg_b200_problem* P, bool prec) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const int n = L.n;
+  const int nb = red_blocks(c, n);
+  const int gv = grid_for(c, n, kThreads, kPerSm);
+  if (prec) {
+    HB_TRY(mg_level(P, 0, P->r, P->z));
+  } else {
+    HB_CK(cudaMemcpyAsync(P->z, P->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinRtzIter));
+  k_update_p_iter<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);
+  HB_CK(cudaGetLastError());
+  const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, gs, kFinPap));
+  k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);
+  HB_CK(cudaGetLastError());
+  return finalize(c, nb, kFinNormr);
+}
+
+// Ends a capture begun on `st` (whether or not the captured work succeeded).
+int end_capture(cudaStream_t st, int status) {
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (status == HPCG_B200_OK && e != cudaSuccess) {
+    set_error("cudaStreamEndCapture", e);
+    return status_of(e);
+  }
+  return status;
+}
+
+// Graph: [condition before the loop] -> while (condition) { iteration; condition }.
+int build_cg_graph(hpcg_b200_problem* P, bool prec, cudaGraphExec_t* out) {
+  Context* c = P->ctx;
+  cudaGraph_t g = nullptr;
+  HB_CK(cudaGraphCreate(&g, 0));
+  int st = HPCG_B200_OK;
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("cudaGraphConditionalHandleCreate", e);
+    return status_of(e);
+  }
+  e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    k_cg_condition<<<1, 32, 0, c->stream>>>(c->scal, h, 0);
+    e = cudaGetLastError();
+    st = end_capture(c->stream, e == cudaSuccess ? HPCG_B200_OK : status_of(e));
+  }
+  if (e != cudaSuccess || st != HPCG_B200_OK) {
+    cudaGraphDestroy(g);
+    set_error("graph capture (loop condition)", e);
+    return st != HPCG_B200_OK ? st : status_of(e);
+  }
+  size_t num = 0;
+  cudaGraphNode_t init = nullptr;
+  e = cudaGraphGetNodes(g, nullptr, &num);
+  if (e == cudaSuccess && num == 1) e = cudaGraphGetNodes(g, &init, &num);
+  // zero-filled node parameters (the struct's union has no default constructor)
+  alignas(cudaGraphNodeParams) unsigned char cp_buf[sizeof(cudaGraphNodeParams)];
+  std::memset(cp_buf, 0, sizeof(cp_buf));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_buf);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop = nullptr;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&loop, g, &init, 1, &cp);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(c->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("graph while node", e);
+    return status_of(e);
+  }
+  st = cg_iteration_body(P, prec);
+  if (st == HPCG_B200_OK) {
+    k_cg_condition<<<1, 32, 0, c->stream>>>(c->scal, h, 1);
+    if (cudaGetLastError() != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  }
+  st = end_capture(c->stream, st);
+  if (st == HPCG_B200_OK) {
+    e = cudaGraphInstantiate(out, g, 0);
+    if (e != cudaSuccess) {
+      set_error("cudaGraphInstantiate", e);
+      st = status_of(e);
+    }
+  }
+  cudaGraphDestroy(g);
+  return st;
+}
+
+// The whole loop of CG.cpp:100-126 as one graph launch after the preamble on
+// the stream; no host round trip until the loop has ended.
+int run_cg_graph(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niters, double* normr_out,
+                 double* normr0_out) {
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  const int n = L.n;
+  const int nb = red_blocks(c, n);
+  spmv_dispatch<double, false>(c, L, L.val, P->x, P->Ap, nullptr);
+  k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, P->b, -1.0, P->Ap, P->r, c->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize(c, nb, kFinNormr0));
+  k_cg_setup<<<1, 32, 0, c->stream>>>(c->scal, max_iter, tol);
+  HB_CK(cudaGetLastError());
+  cudaGraphExec_t& ex = P->cg_graph[prec ? 1 : 0];
+  if (!ex) HB_TRY(build_cg_graph(P, prec, &ex));
+  HB_CK(cudaGraphLaunch(ex, c->stream));
+  HB_TRY(read_scalars(c));
+  *niters = c->scal_host->iter;
+  *normr_out = std::sqrt(c->scal_host->normr2);
+  *normr0_out = c->scal_host->normr0;
+  return HPCG_B200_OK;
+}
+
 // CG.cpp:59-143 on the resident vectors p->b, p->x (colour order).
 int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niters, double* normr_out,
            double* normr0_out, double* times) {
+  // the graph holds the colour-order kernels; the natural-order parity mode
+  // (thousands of wavefront launches) runs on the stream
+  if (!times && !P->ctx->prof && !P->cg_graph_failed && P->symgs_mode == HPCG_B200_SYMGS_COLOUR &&
+      graph_enabled()) {
+    HB_TRY(autotune(P));
+    const int st = run_cg_graph(P, max_iter, tol, prec, niters, normr_out, normr0_out);
+    if (st == HPCG_B200_OK) return st;
+    // a refused capture leaves the vectors as the preamble left them: rerun on the stream
+    P->cg_graph_failed = true;
+    cudaGetLastError();
+  }
   const Level& L = P->lev[0];
   Context* c = P->ctx;
   const int n = L.n;

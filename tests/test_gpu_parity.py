@@ -485,3 +485,20 @@ def test_device_budget_gives_nomem():
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     assert "status 4" in out.stdout
+
+
+def test_graph_loop_equals_stream_loop(case32):
+    """The CG loop as one CUDA graph (conditional while node, the loop condition
+    of CG.cpp:100 evaluated on the device) computes the same bits as the loop
+    launched kernel by kernel (used when times are requested)."""
+    P, D, _, _ = case32
+    n = P.levels[0].n
+    for max_iter, tol, prec in ((1, 0.0, True), (17, 0.0, True), (500, 1e-7, True), (30, 1e-6, False)):
+        xg = np.zeros(n)
+        ng = D.CG(P.b, xg, max_iter, tol, prec)
+        xe = np.zeros(n)
+        times = np.zeros(10)
+        ne = D.CG(P.b, xe, max_iter, tol, prec, times=times)
+        assert ng == ne, (max_iter, tol, prec)
+        assert np.array_equal(xg, xe)
+        assert times[0] > 0.0
