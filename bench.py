@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--mixed-tol", type=float, default=1e-9)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 128^3 implicit-adjoint timing")
     ap.add_argument("--no-multi", action="store_true", help="skip the 256^3, 8 right-hand-side comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 16-problem batched comparison")
     return ap.parse_args()
 
 
@@ -296,6 +297,45 @@ def multi_rhs(dev, n=256, k=8, tol=1e-9, max_iter=2000):
         P.free()
 
 
+def batched(dev, count=16, tol=1e-9, max_iter=2000):
+    """`count` problems with grid sides drawn by seed from {32, 48, 64, 96, 128}:
+    one batched solve (hpcg_b200_batch_cg_mixed) against one-at-a-time solves
+    (hpcg_b200_cg_mixed), FP64 flexible CG around the FP32 V-cycle, each
+    problem's own right-hand side, to `tol`."""
+    import numpy as np
+    import torch
+    from hpcg_b200 import binding as B
+    rng = np.random.Generator(np.random.PCG64(RHS_SEED))
+    sides = [32, 48, 64, 96, 128]
+    dims = [tuple(int(v) for v in rng.choice(sides, 3)) for _ in range(count)]
+    bt = B.Batch(dims, dev)
+    try:
+        lib_stream = torch.cuda.ExternalStream(B.stream(dev), device=dev)
+        bs = [torch.from_numpy(p.get_rhs()).to(f"cuda:{dev}") for p in bt.problems]
+        xs = [torch.zeros_like(b) for b in bs]
+        bt.CG_mixed(bs, xs, 1, tol)  # builds the graph
+        for x in xs:
+            x.zero_()
+        (ni, nr, nr0), t_batch = timed(lib_stream, lambda: bt.CG_mixed(bs, xs, max_iter, tol))
+        iters_single, t_single = [], 0.0
+        for p, b in zip(bt.problems, bs):
+            x = torch.zeros_like(b)
+            p.CG_mixed(b, x, 1, tol)  # first use prepares the FP32 copies
+            x.zero_()
+            (it, _, _), t = timed(lib_stream, lambda: p.CG_mixed(b, x, max_iter, tol))
+            iters_single.append(it)
+            t_single += t
+        return {"problems": count, "dims": dims, "tolerance": tol, "form": "FP64 flexible CG, FP32 V-cycle",
+                "batched": {"iters": [int(v) for v in ni], "seconds": round(t_batch, 4),
+                            "solves_per_s": round(count / t_batch, 2),
+                            "max_scaled_residual": float(np.max(nr / nr0))},
+                "one_at_a_time": {"iters": iters_single, "seconds": round(t_single, 4),
+                                  "solves_per_s": round(count / t_single, 2)},
+                "speedup": round(t_single / t_batch, 3)}
+    finally:
+        bt.free()
+
+
 def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000):
     """Time to a relative residual `tol` from x = 0: FP64 PCG (hpcg_b200_cg) against
     FP64 flexible PCG around the FP32 V-cycle (hpcg_b200_cg_mixed)."""
@@ -454,6 +494,9 @@ def b200_arm(args, rank, world, local_rank):
     multi = None
     if not args.no_multi:
         multi = multi_rhs(dev)
+    batch = None
+    if not args.no_batch:
+        batch = batched(dev)
 
     line = None
     if rank == 0:
@@ -505,6 +548,8 @@ def b200_arm(args, rank, world, local_rank):
             line["adjoint"] = adjoint
         if multi:
             line["multi_rhs"] = multi
+        if batch:
+            line["batched"] = batch
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(args)

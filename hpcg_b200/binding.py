@@ -37,6 +37,7 @@ EXPORTS = (
     "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
+    "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
     "hpcg_b200_last_error",
 )
 
@@ -95,6 +96,10 @@ def lib():
         l.hpcg_b200_adjoint.argtypes = [vp, vp, vp, i, d, vp, vp, C.POINTER(i)]
         l.hpcg_b200_cg_multi.argtypes = [vp, i, vp, vp, i, d, vp, vp, vp]
         l.hpcg_b200_mg_multi.argtypes = [vp, i, vp, vp]
+        l.hpcg_b200_batch_create.argtypes = [i, vp, vp, vp, i, C.POINTER(vp)]
+        l.hpcg_b200_batch_problem.argtypes = [vp, i, C.POINTER(vp)]
+        l.hpcg_b200_batch_cg_mixed.argtypes = [vp, vp, vp, i, d, vp, vp, vp]
+        l.hpcg_b200_batch_free.argtypes = [vp]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -179,6 +184,8 @@ class Problem:
         return cls(h.value, (nx, ny, nz), nlevels)
 
     def free(self):
+        if getattr(self, "_owned_by_batch", False):
+            return
         if self._h and self._h.value:
             _check(lib().hpcg_b200_free(self._h), "hpcg_b200_free")
             self._h = C.c_void_p()
@@ -302,6 +309,54 @@ def colour_permutation(nx, ny, nz):
     _check(lib().hpcg_b200_colour_permutation(nx, ny, nz, n2o.ctypes.data, starts.ctypes.data),
            "hpcg_b200_colour_permutation")
     return n2o, starts
+
+
+class Batch:
+    """Independent problems of different sizes solved together
+    (hpcg_b200_batch_*). Member problems are views owned by the batch."""
+
+    def __init__(self, dims, device=0):
+        m = len(dims)
+        nx = np.array([d[0] for d in dims], np.int32)
+        ny = np.array([d[1] for d in dims], np.int32)
+        nz = np.array([d[2] for d in dims], np.int32)
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_batch_create(m, nx.ctypes.data, ny.ctypes.data, nz.ctypes.data, device, C.byref(h)),
+               "hpcg_b200_batch_create")
+        self._h = h
+        self.dims = [tuple(int(v) for v in d) for d in dims]
+        self.problems = []
+        for i, d in enumerate(self.dims):
+            ph = C.c_void_p()
+            _check(lib().hpcg_b200_batch_problem(self._h, i, C.byref(ph)), "hpcg_b200_batch_problem")
+            p = Problem.__new__(Problem)
+            p._h, p.dims, p.nlevels = ph, d, 4
+            p._owned_by_batch = True
+            self.problems.append(p)
+
+    def CG_mixed(self, bs, xs, max_iter, tolerance):
+        m = len(self.dims)
+        bp = (C.c_void_p * m)(*[_ptr(v) for v in bs])
+        xp = (C.c_void_p * m)(*[_ptr(v) for v in xs])
+        ni = np.zeros(m, np.int32)
+        nr = np.zeros(m)
+        nr0 = np.zeros(m)
+        _check(lib().hpcg_b200_batch_cg_mixed(self._h, bp, xp, max_iter, tolerance, ni.ctypes.data,
+                                              nr.ctypes.data, nr0.ctypes.data), "hpcg_b200_batch_cg_mixed")
+        return ni, nr, nr0
+
+    def free(self):
+        if self._h and self._h.value:
+            for p in self.problems:
+                p._h = C.c_void_p()  # owned by the batch
+            _check(lib().hpcg_b200_batch_free(self._h), "hpcg_b200_batch_free")
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT = 0, 1, 2, 3

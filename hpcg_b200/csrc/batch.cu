@@ -1,0 +1,685 @@
+// Batched solves: many independent HPCG problems of different sizes advanced
+// together by flexible CG in FP64 around the FP32 V-cycle (the mixed form of
+// hpcg_b200_cg_mixed, per problem).
+//
+// Every step of an iteration is ONE kernel launch for the whole batch: the
+// launch walks a work list of row tiles that spans all problems (a colour phase
+// of every problem's level, a restriction, a vector update...), so a batch of
+// small problems costs the launches of one. The iteration loop itself is one
+// CUDA graph launch: a conditional while node repeats the iteration while any
+// problem is still above its tolerance and the iteration limit is not reached;
+// problems that have converged skip their tiles. No kernel waits on another.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "reduce.cuh"
+#include "rows.cuh"
+
+namespace hb {
+
+int prepare_f32(hpcg_b200_problem* p);
+int free_problem(hpcg_b200_problem* p);
+void release_accounted(size_t bytes);
+
+namespace {
+
+constexpr int kTile = kThreads;  // rows per tile: one thread per row
+constexpr int kBlocksPerSm = 8;
+constexpr uint64_t kBatchMagic = 0x48504347b2000b01ull;
+
+// one problem's share of a Gauss-Seidel colour phase (FP32 V-cycle)
+struct BGs {
+  const float* val;
+  const int* col;
+  int64_t pitch;
+  const float* rhs;
+  float* x;
+  int r0, r1;
+  uint32_t mask;
+  int first;
+  int prob;
+};
+// residual + restriction, and prolongation, of one problem's level
+struct BRes {
+  const float* val;
+  const int* col;
+  int64_t pitch;
+  const float* rf;
+  const float* xf;
+  const int* tf;
+  const int* tq;
+  float* rc;
+  int nc;
+  int prob;
+};
+// the level-0 (outer, FP64) vectors of one problem
+struct BVec {
+  const double* val;
+  const int* col;
+  int64_t pitch;
+  int n;
+  double *b, *x, *r, *z, *zprev, *p, *Ap;
+  float *r32, *x32;
+};
+struct BTile {
+  int item;   // index into the step's item array (or the problem for vector tiles)
+  int start;  // first row of the tile
+};
+// per-problem CG scalars
+struct BScal {
+  double rtz, oldrtz, alpha, beta, pAp, normr2, normr0, rzprev;
+  int active, niters;
+};
+struct BCtl {
+  int iter;  // iterations completed
+  int max_iter;
+  double tol;
+};
+
+// ---- kernels -----------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items, const BTile* __restrict__ tiles,
+                                                   int ntiles, const BScal* __restrict__ sc) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BGs it = items[tl.item];
+    if (!sc[it.prob].active) continue;
+    const int q = tl.start + threadIdx.x;
+    if (q >= it.r1) continue;
+    if (it.first)
+      gs_row<float, float, true, kPlain>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+    else
+      gs_row<float, float, false, kPlain>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+  }
+}
+
+// rc = (rf - A xf) at the injected rows (ComputeMG_ref.cpp:49-51, sorted pairs)
+__global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict__ items,
+                                                         const BTile* __restrict__ tiles, int ntiles,
+                                                         const BScal* __restrict__ sc) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BRes it = items[tl.item];
+    if (!sc[it.prob].active) continue;
+    const int u = tl.start + threadIdx.x;
+    if (u >= it.nc) continue;
+    const int f = it.tf[u];
+    float sum = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) sum += it.val[k * it.pitch + f] * __ldg(it.xf + it.col[k * it.pitch + f]);
+    it.rc[it.tq[u]] = it.rf[f] - sum;
+  }
+}
+
+// xf[f] += xc[q] (ComputeProlongation_ref.cpp:49); prolongation items carry xc in
+// rf and the fine solution in rc
+__global__ void __launch_bounds__(kThreads) k_b_prolong(const BRes* __restrict__ items,
+                                                        const BTile* __restrict__ tiles, int ntiles,
+                                                        const BScal* __restrict__ sc) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BRes it = items[tl.item];
+    if (!sc[it.prob].active) continue;
+    const int u = tl.start + threadIdx.x;
+    if (u >= it.nc) continue;
+    it.rc[it.tf[u]] += it.rf[it.tq[u]];
+  }
+}
+
+// y = A x (FP64 outer SpMV, CG.cpp:118); DOT: partial of x'y per tile
+template <bool DOT>
+__global__ void __launch_bounds__(kThreads) k_b_spmv(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                     int ntiles, int use_p, const BScal* __restrict__ sc,
+                                                     double* __restrict__ partials) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BVec it = v[tl.item];
+    double acc = 0.0;
+    const bool act = sc == nullptr || sc[tl.item].active;
+    const int q = tl.start + threadIdx.x;
+    if (act && q < it.n) {
+      const double* x = use_p ? it.p : it.x;
+      double sum = 0.0, xq = 0.0;
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const double xv = __ldg(x + it.col[k * it.pitch + q]);
+        sum += it.val[k * it.pitch + q] * xv;
+        if (k == kDiagSlot) xq = xv;
+      }
+      it.Ap[q] = sum;
+      if (DOT) acc = xq * sum;
+    }
+    if (DOT) {
+      const double s = block_sum(acc);
+      if (threadIdx.x == 0) partials[t] = s;
+    }
+  }
+}
+
+// r = 1.0 b + (-1.0) Ap (CG.cpp:88) and partial of r'r
+__global__ void __launch_bounds__(kThreads) k_b_resid(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                      int ntiles, double* __restrict__ partials) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BVec it = v[tl.item];
+    const int q = tl.start + threadIdx.x;
+    double acc = 0.0;
+    if (q < it.n) {
+      const double r = 1.0 * it.b[q] + -1.0 * it.Ap[q];
+      it.r[q] = r;
+      acc = r * r;
+    }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) partials[t] = s;
+  }
+}
+
+// r32 = (float) r: the FP32 V-cycle's right-hand side
+__global__ void __launch_bounds__(kThreads) k_b_to32(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                     int ntiles, const BScal* __restrict__ sc) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    if (!sc[tl.item].active) continue;
+    const BVec it = v[tl.item];
+    const int q = tl.start + threadIdx.x;
+    if (q < it.n) it.r32[q] = (float)it.r[q];
+  }
+}
+
+// z = (double) x32; partials of r'z and r'zprev (flexible beta)
+__global__ void __launch_bounds__(kThreads) k_b_to64_dots(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                          int ntiles, const BScal* __restrict__ sc,
+                                                          double* __restrict__ partials) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BVec it = v[tl.item];
+    const int q = tl.start + threadIdx.x;
+    double a1 = 0.0, a2 = 0.0;
+    if (sc[tl.item].active && q < it.n) {
+      const double z = (double)it.x32[q];
+      it.z[q] = z;
+      const double r = it.r[q];
+      a1 = r * z;
+      a2 = r * it.zprev[q];
+    }
+    const double s1 = block_sum(a1);
+    const double s2 = block_sum(a2);
+    if (threadIdx.x == 0) {
+      partials[t] = s1;
+      partials[ntiles + t] = s2;
+    }
+  }
+}
+
+// iteration 1: p = z; later: p = z + beta p; then zprev = z
+__global__ void __launch_bounds__(kThreads) k_b_update_p(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                         int ntiles, const BScal* __restrict__ sc,
+                                                         const BCtl* __restrict__ ctl) {
+  const bool first = ctl->iter == 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    if (!sc[tl.item].active) continue;
+    const BVec it = v[tl.item];
+    const double beta = sc[tl.item].beta;
+    const int q = tl.start + threadIdx.x;
+    if (q < it.n) {
+      const double z = it.z[q];
+      it.p[q] = first ? z : z + beta * it.p[q];
+      it.zprev[q] = z;
+    }
+  }
+}
+
+// x += alpha p, r += (-alpha) Ap (CG.cpp:121-122); partial of r'r
+__global__ void __launch_bounds__(kThreads) k_b_update_xr(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                          int ntiles, const BScal* __restrict__ sc,
+                                                          double* __restrict__ partials) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BTile tl = tiles[t];
+    const BVec it = v[tl.item];
+    const int q = tl.start + threadIdx.x;
+    double acc = 0.0;
+    if (q < it.n) {
+      double r = it.r[q];
+      if (sc[tl.item].active) {
+        const double alpha = sc[tl.item].alpha;
+        it.x[q] = it.x[q] + alpha * it.p[q];
+        r = r + -alpha * it.Ap[q];
+        it.r[q] = r;
+      }
+      acc = r * r;
+    }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) partials[t] = s;
+  }
+}
+
+enum BFin : int { kBNorm0 = 0, kBRtz = 1, kBPap = 2, kBNormr = 3 };
+
+// One block per problem: fixed-order sum over the problem's tiles, then its scalar step.
+__global__ void __launch_bounds__(kThreads) k_b_finalize(BScal* sc, const double* __restrict__ partials,
+                                                         int ntiles, const int* __restrict__ range, int op,
+                                                         const BCtl* __restrict__ ctl) {
+  const int p = blockIdx.x;
+  const int t0 = range[p], t1 = range[p + 1];
+  double a1 = 0.0, a2 = 0.0;
+  for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    a1 += partials[t];
+    if (op == kBRtz) a2 += partials[ntiles + t];
+  }
+  const double s1 = block_sum(a1);
+  const double s2 = op == kBRtz ? block_sum(a2) : 0.0;
+  if (threadIdx.x != 0) return;
+  BScal& s = sc[p];
+  switch (op) {
+    case kBNorm0:
+      s.normr2 = s1;
+      s.normr0 = sqrt(s1);
+      s.active = s.normr0 / s.normr0 > ctl->tol ? 1 : 0;
+      s.niters = 0;
+      break;
+    case kBRtz:
+      if (!s.active) break;
+      if (ctl->iter == 0) {
+        s.rtz = s1;
+      } else {
+        s.oldrtz = s.rtz;
+        s.rtz = s1;
+        s.rzprev = s2;
+        s.beta = (s1 - s2) / s.oldrtz;  // Polak-Ribiere
+      }
+      break;
+    case kBPap:
+      if (!s.active) break;
+      s.pAp = s1;
+      s.alpha = s.rtz / s1;
+      break;
+    case kBNormr:
+      s.normr2 = s1;
+      if (s.active) {
+        s.niters = ctl->iter + 1;
+        s.active = sqrt(s1) / s.normr0 > ctl->tol ? 1 : 0;
+      }
+      break;
+    default: break;
+  }
+}
+
+__global__ void k_b_setup(BCtl* ctl, int max_iter, double tol) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->iter = 0;
+    ctl->max_iter = max_iter;
+    ctl->tol = tol;
+  }
+}
+
+// while (iter < max_iter && any problem active)
+__global__ void k_b_condition(BCtl* ctl, const BScal* __restrict__ sc, int m, cudaGraphConditionalHandle h,
+                              int advance) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (advance) ctl->iter += 1;
+  bool any = false;
+  for (int p = 0; p < m; ++p) any = any || sc[p].active;
+  cudaGraphSetConditional(h, any && ctl->iter < ctl->max_iter ? 1u : 0u);
+}
+
+// ---- host ---------------------------------------------------------------------
+
+struct Step {
+  int kind;      // 0 = GS phase, 1 = restriction, 2 = prolongation
+  int item_off;  // first item of the step (tiles index the whole item array)
+  int tile_off;  // first tile of the step
+  int ntiles;
+};
+
+}  // namespace
+}  // namespace hb
+
+struct hpcg_b200_batch {
+  uint64_t magic;
+  int device;
+  hb::Context* ctx;
+  int m;
+  std::vector<hpcg_b200_problem*> probs;
+  // work lists (device) and the V-cycle's step sequence
+  hb::BGs* gs_items;
+  hb::BRes* res_items;
+  hb::BTile* tiles;
+  std::vector<hb::Step> steps;
+  hb::BVec* vec;
+  hb::BTile* vtiles;  // row tiles of every problem's level 0
+  int nvt;
+  int* vrange;        // [m+1] tile range of each problem
+  double* partials;   // [2 * nvt]
+  hb::BScal* sc;
+  hb::BScal* sc_host;
+  hb::BCtl* ctl;
+  size_t bytes;
+  cudaGraphExec_t graph;
+};
+
+namespace hb {
+namespace {
+
+bool valid_batch(const hpcg_b200_batch* b) { return b && b->magic == kBatchMagic; }
+
+int alloc_copy(hpcg_b200_batch* B, void** dst, const void* src, size_t bytes) {
+  HB_TRY(dev_alloc(dst, bytes, &B->bytes));
+  HB_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  return HPCG_B200_OK;
+}
+
+void tiles_of(std::vector<BTile>& tiles, int item, int r0, int r1) {
+  for (int s = r0; s < r1; s += kTile) tiles.push_back({item, s});
+}
+
+// The V-cycle of every problem as one step sequence (ComputeMG_ref.cpp:39-63
+// with the colour sweeps of the single-problem path): level l pre-smooth
+// (forward from x = 0, backward without the last colour), restriction,
+// recursion, prolongation, post-smooth; the coarsest level one symmetric sweep.
+void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<BRes>& res,
+                  std::vector<BTile>& tiles) {
+  auto phase = [&](int s, bool first) {
+    Step st{0, (int)gs.size(), (int)tiles.size(), 0};
+    for (int p = 0; p < B->m; ++p) {
+      const Level& L = B->probs[p]->lev[l];
+      const int item = (int)gs.size();
+      BGs it;
+      it.val = L.val32;
+      it.col = L.col;
+      it.pitch = L.pitch;
+      it.rhs = L.r32;
+      it.x = L.x32;
+      it.r0 = L.g.start[s];
+      it.r1 = L.g.start[s + 1];
+      it.mask = first ? first_mask(L.g, s) : kAllSlots;
+      it.first = first ? 1 : 0;
+      it.prob = p;
+      gs.push_back(it);
+      tiles_of(tiles, item, it.r0, it.r1);
+    }
+    st.ntiles = (int)tiles.size() - st.tile_off;
+    B->steps.push_back(st);
+  };
+  auto sweep = [&](bool first) {
+    for (int s = 0; s < kColours; ++s) phase(s, first);
+    for (int s = kColours - 2; s >= 0; --s) phase(s, false);
+  };
+  auto transfer = [&](int kind) {
+    Step st{kind, (int)res.size(), (int)tiles.size(), 0};
+    for (int p = 0; p < B->m; ++p) {
+      const Level& L = B->probs[p]->lev[l];
+      const Level& C = B->probs[p]->lev[l + 1];
+      const int item = (int)res.size();
+      BRes it;
+      it.val = L.val32;
+      it.col = L.col;
+      it.pitch = L.pitch;
+      it.tf = L.tf;
+      it.tq = L.tq;
+      it.nc = C.n;
+      it.prob = p;
+      if (kind == 1) {  // rc = rf - A xf
+        it.rf = L.r32;
+        it.xf = L.x32;
+        it.rc = C.r32;
+      } else {  // xf += xc: xc travels in rf, the fine solution in rc
+        it.rf = C.x32;
+        it.xf = nullptr;
+        it.rc = L.x32;
+      }
+      res.push_back(it);
+      tiles_of(tiles, item, 0, it.nc);
+    }
+    st.ntiles = (int)tiles.size() - st.tile_off;
+    B->steps.push_back(st);
+  };
+  sweep(true);
+  if (l + 1 < 4) {
+    transfer(1);
+    build_vcycle(B, l + 1, gs, res, tiles);
+    transfer(2);
+    sweep(false);
+  }
+}
+
+int grid_tiles(Context* c, int ntiles) {
+  int g = c->sms * kBlocksPerSm;
+  return ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g;
+}
+
+int launch_step(hpcg_b200_batch* B, const Step& s) {
+  Context* c = B->ctx;
+  const int g = grid_tiles(c, s.ntiles);
+  // tiles hold indices into the whole item array, so the items go in unshifted
+  if (s.kind == 0)
+    k_b_gs<<<g, kThreads, 0, c->stream>>>(B->gs_items, B->tiles + s.tile_off, s.ntiles, B->sc);
+  else if (s.kind == 1)
+    k_b_restrict<<<g, kThreads, 0, c->stream>>>(B->res_items, B->tiles + s.tile_off, s.ntiles, B->sc);
+  else
+    k_b_prolong<<<g, kThreads, 0, c->stream>>>(B->res_items, B->tiles + s.tile_off, s.ntiles, B->sc);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int finalize_b(hpcg_b200_batch* B, int op) {
+  k_b_finalize<<<B->m, kThreads, 0, B->ctx->stream>>>(B->sc, B->partials, B->nvt, B->vrange, op, B->ctl);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+// one flexible-CG iteration of every active problem
+int iteration(hpcg_b200_batch* B) {
+  Context* c = B->ctx;
+  const int gv = grid_tiles(c, B->nvt);
+  k_b_to32<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->sc);
+  HB_CK(cudaGetLastError());
+  for (const Step& s : B->steps) HB_TRY(launch_step(B, s));
+  k_b_to64_dots<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->sc, B->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize_b(B, kBRtz));
+  k_b_update_p<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->sc, B->ctl);
+  k_b_spmv<true><<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, 1, B->sc, B->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize_b(B, kBPap));
+  k_b_update_xr<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->sc, B->partials);
+  HB_CK(cudaGetLastError());
+  return finalize_b(B, kBNormr);
+}
+
+int end_capture_b(cudaStream_t st, int status) {
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (status == HPCG_B200_OK && e != cudaSuccess) {
+    set_error("cudaStreamEndCapture", e);
+    return status_of(e);
+  }
+  return status;
+}
+
+int build_graph(hpcg_b200_batch* B) {
+  Context* c = B->ctx;
+  cudaGraph_t g = nullptr;
+  HB_CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  int st = HPCG_B200_OK;
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0,
+                                                            cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 0);
+    e = cudaGetLastError();
+    st = end_capture_b(c->stream, e == cudaSuccess ? HPCG_B200_OK : status_of(e));
+  }
+  size_t num = 0;
+  cudaGraphNode_t init = nullptr;
+  if (e == cudaSuccess && st == HPCG_B200_OK) e = cudaGraphGetNodes(g, nullptr, &num);
+  if (e == cudaSuccess && st == HPCG_B200_OK && num == 1) e = cudaGraphGetNodes(g, &init, &num);
+  alignas(cudaGraphNodeParams) unsigned char buf[sizeof(cudaGraphNodeParams)];
+  std::memset(buf, 0, sizeof(buf));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(buf);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop = nullptr;
+  if (e == cudaSuccess && st == HPCG_B200_OK) e = cudaGraphAddNode(&loop, g, &init, 1, &cp);
+  if (e == cudaSuccess && st == HPCG_B200_OK)
+    e = cudaStreamBeginCaptureToGraph(c->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess || st != HPCG_B200_OK) {
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) set_error("batch graph", e);
+    return st != HPCG_B200_OK ? st : status_of(e);
+  }
+  st = iteration(B);
+  if (st == HPCG_B200_OK) {
+    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 1);
+    if (cudaGetLastError() != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  }
+  st = end_capture_b(c->stream, st);
+  if (st == HPCG_B200_OK) {
+    e = cudaGraphInstantiate(&B->graph, g, 0);
+    if (e != cudaSuccess) {
+      set_error("cudaGraphInstantiate (batch)", e);
+      st = status_of(e);
+    }
+  }
+  cudaGraphDestroy(g);
+  return st;
+}
+
+void destroy(hpcg_b200_batch* B) {
+  if (!B) return;
+  cudaSetDevice(B->device);
+  if (B->ctx) cudaStreamSynchronize(B->ctx->stream);
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  void* v[] = {B->gs_items, B->res_items, B->tiles, B->vec, B->vtiles, B->vrange, B->partials, B->sc, B->ctl};
+  for (void* q : v) cudaFree(q);
+  if (B->sc_host) cudaFreeHost(B->sc_host);
+  release_accounted(B->bytes);
+  for (hpcg_b200_problem* p : B->probs) free_problem(p);
+  B->magic = 0;
+  delete B;
+}
+
+}  // namespace
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* nz, int device,
+                           hpcg_b200_batch** out) {
+  if (!out || count < 1 || !nx || !ny || !nz) return HPCG_B200_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < count; ++i)  // every level even: all 8 colours present on every level
+    if (nx[i] % 16 || ny[i] % 16 || nz[i] % 16 || nx[i] < 16 || ny[i] < 16 || nz[i] < 16)
+      return HPCG_B200_ERR_UNSUPPORTED;
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_CK(cudaSetDevice(device));
+  hpcg_b200_batch* B = new hpcg_b200_batch;
+  B->magic = kBatchMagic;
+  B->device = device;
+  B->ctx = c;
+  B->m = count;
+  B->gs_items = nullptr; B->res_items = nullptr; B->tiles = nullptr; B->vec = nullptr; B->vtiles = nullptr;
+  B->vrange = nullptr; B->partials = nullptr; B->sc = nullptr; B->sc_host = nullptr; B->ctl = nullptr;
+  B->bytes = 0;
+  B->graph = nullptr;
+  B->nvt = 0;
+  int st = HPCG_B200_OK;
+  for (int i = 0; i < count && st == HPCG_B200_OK; ++i) {
+    hpcg_b200_problem* p = nullptr;
+    st = hpcg_b200_generate(nx[i], ny[i], nz[i], 4, device, &p);
+    if (st == HPCG_B200_OK) {
+      B->probs.push_back(p);
+      st = prepare_f32(p);
+    }
+  }
+  if (st == HPCG_B200_OK) {
+    std::vector<BGs> gs;
+    std::vector<BRes> res;
+    std::vector<BTile> tiles;
+    build_vcycle(B, 0, gs, res, tiles);
+    std::vector<BVec> vec(count);
+    std::vector<BTile> vt;
+    std::vector<int> range(count + 1, 0);
+    for (int p = 0; p < count; ++p) {
+      hpcg_b200_problem* P = B->probs[p];
+      const Level& L = P->lev[0];
+      vec[p] = BVec{L.val, L.col, L.pitch, L.n, P->b, P->x, P->r, P->z, P->zprev, P->p, P->Ap, L.r32, L.x32};
+      range[p] = (int)vt.size();
+      tiles_of(vt, p, 0, L.n);
+    }
+    range[count] = (int)vt.size();
+    B->nvt = (int)vt.size();
+    st = alloc_copy(B, (void**)&B->gs_items, gs.data(), sizeof(BGs) * gs.size());
+    if (!st && !res.empty()) st = alloc_copy(B, (void**)&B->res_items, res.data(), sizeof(BRes) * res.size());
+    if (!st) st = alloc_copy(B, (void**)&B->tiles, tiles.data(), sizeof(BTile) * tiles.size());
+    if (!st) st = alloc_copy(B, (void**)&B->vec, vec.data(), sizeof(BVec) * vec.size());
+    if (!st) st = alloc_copy(B, (void**)&B->vtiles, vt.data(), sizeof(BTile) * vt.size());
+    if (!st) st = alloc_copy(B, (void**)&B->vrange, range.data(), sizeof(int) * range.size());
+    if (!st) st = dev_alloc((void**)&B->partials, sizeof(double) * 2 * B->nvt, &B->bytes);
+    if (!st) st = dev_alloc((void**)&B->sc, sizeof(BScal) * count, &B->bytes);
+    if (!st) st = dev_alloc((void**)&B->ctl, sizeof(BCtl), &B->bytes);
+    if (!st && cudaMallocHost(&B->sc_host, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_NOMEM;
+    if (!st && cudaMemset(B->sc, 0, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  }
+  if (st != HPCG_B200_OK) {
+    destroy(B);
+    return st;
+  }
+  *out = B;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_batch_problem(hpcg_b200_batch* B, int i, hpcg_b200_problem** out) {
+  if (!valid_batch(B)) return HPCG_B200_ERR_HANDLE;
+  if (!out || i < 0 || i >= B->m) return HPCG_B200_ERR_ARG;
+  *out = B->probs[i];
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* B, const double* const* b, double* const* x, int max_iter,
+                             double tolerance, int* niters, double* normr, double* normr0) {
+  if (!valid_batch(B)) return HPCG_B200_ERR_HANDLE;
+  if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
+  for (int p = 0; p < B->m; ++p)
+    if (!b[p] || !x[p]) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(B->device));
+  Context* c = B->ctx;
+  for (int p = 0; p < B->m; ++p) {
+    HB_TRY(load_vector(B->probs[p], 0, b[p], B->probs[p]->b));
+    HB_TRY(load_vector(B->probs[p], 0, x[p], B->probs[p]->x));
+  }
+  // preamble: Ap = A x; r = b - Ap; normr0 (CG.cpp:86-96), every problem
+  const int gv = grid_tiles(c, B->nvt);
+  k_b_setup<<<1, 32, 0, c->stream>>>(B->ctl, max_iter, tolerance);
+  k_b_spmv<false><<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, 0, nullptr, nullptr);
+  k_b_resid<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->partials);
+  HB_CK(cudaGetLastError());
+  HB_TRY(finalize_b(B, kBNorm0));
+  if (!B->graph) HB_TRY(build_graph(B));
+  HB_CK(cudaGraphLaunch(B->graph, c->stream));
+  HB_CK(cudaMemcpyAsync(B->sc_host, B->sc, sizeof(BScal) * B->m, cudaMemcpyDeviceToHost, c->stream));
+  HB_CK(cudaStreamSynchronize(c->stream));
+  for (int p = 0; p < B->m; ++p) {
+    niters[p] = B->sc_host[p].niters;
+    normr[p] = std::sqrt(B->sc_host[p].normr2);
+    normr0[p] = B->sc_host[p].normr0;
+    HB_TRY(store_vector(B->probs[p], 0, B->probs[p]->x, x[p]));
+  }
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_batch_free(hpcg_b200_batch* B) {
+  if (!valid_batch(B)) return HPCG_B200_ERR_HANDLE;
+  destroy(B);
+  return HPCG_B200_OK;
+}
+
+}  // extern "C"

@@ -640,6 +640,8 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
 
 }  // namespace
 
+int prepare_f32(hpcg_b200_problem* p) { return ensure_f32(p); }
+
 // natural-order src (host or device) -> colour-order device dst
 int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
   const Level& L = p->lev[level];

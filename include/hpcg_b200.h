@@ -149,6 +149,27 @@ int hpcg_b200_cg_multi(hpcg_b200_problem* p, int nrhs, const double* b, double* 
  * x_j is bitwise what hpcg_b200_mg gives for r_j. */
 int hpcg_b200_mg_multi(hpcg_b200_problem* p, int nrhs, const double* r, double* x);
 
+/* Many independent problems of different sizes solved together (flexible FP64
+ * CG around the FP32 V-cycle, as hpcg_b200_cg_mixed for each). Every step of an
+ * iteration is one kernel launch over a work list of row tiles spanning all the
+ * problems, and the iteration loop is one CUDA graph launch (a conditional while
+ * node runs while any problem is above its tolerance); converged problems skip
+ * their tiles. Every grid dimension must be a multiple of 16. No reference
+ * counterpart (changed form). */
+typedef struct hpcg_b200_batch hpcg_b200_batch;
+
+/* Generates problem i on the device as hpcg_b200_generate(nx[i], ny[i], nz[i], 4). */
+int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* nz, int device,
+                           hpcg_b200_batch** out);
+/* The problem handle of batch member i (owned by the batch: do not free it). */
+int hpcg_b200_batch_problem(hpcg_b200_batch* batch, int i, hpcg_b200_problem** out);
+/* b[i], x[i]: natural-order vectors of problem i (host or device); x[i] is the
+ * initial guess and receives the solution. Per problem: iterations done while
+ * above `tolerance`, final and initial residual norms. */
+int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* batch, const double* const* b, double* const* x, int max_iter,
+                             double tolerance, int* niters, double* normr, double* normr0);
+int hpcg_b200_batch_free(hpcg_b200_batch* batch);
+
 /* ---- changed form 3: implicit adjoint of the solve ------------------------ */
 
 /* Gradients of a loss L(x) through the solve A x = b, given the converged
