@@ -36,7 +36,7 @@ constexpr uint64_t kMagic = 0x48504347b2000001ull;  // "HPCG" + version
 constexpr int kSweepDefault[kColours] = {7, 6, 3, 5, 4, 1, 2, 0};
 
 // The parity bit pattern a stencil direction flips: bit0 for sx = +-1, bit1 for sy, bit2 for sz.
-__host__ __device__ inline int slot_flip(int k) {
+__host__ __device__ constexpr int slot_flip(int k) {
   const int sx = k % 3 - 1, sy = (k / 3) % 3 - 1, sz = k / 9 - 1;
   return (sx != 0 ? 1 : 0) | (sy != 0 ? 2 : 0) | (sz != 0 ? 4 : 0);
 }
@@ -93,6 +93,20 @@ inline uint32_t first_mask(const ColourGrid& g, int s) {
   return m;
 }
 
+// The same mask for the default sweep order, at compile time (the mask depends
+// only on the sweep order and the colour parities, not on the grid).
+constexpr uint32_t first_mask_default(int s) {
+  int pos[kColours] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < kColours; ++i) pos[kSweepDefault[i]] = i;
+  const int c = kSweepDefault[s];
+  uint32_t m = 0;
+  for (int k = 0; k < kSlots; ++k) {
+    if (k == kDiagSlot) continue;
+    if (pos[c ^ slot_flip(k)] < s) m |= 1u << k;
+  }
+  return m;
+}
+
 struct Level {
   ColourGrid g;
   int n = 0;                 // rows
@@ -112,8 +126,9 @@ struct Level {
   // kernel configuration of this level's row kernels, chosen by the autotuner
   int gs_sched = 1;          // kernel configuration of the Gauss-Seidel phases (FP64)
   int gs_sched32 = 1;        // kernel configuration of the Gauss-Seidel phases (FP32 V-cycle)
+  int gs_first = 1;          // kernel configuration of the first-sweep phases (FP64)
   int mv_sched = 1;          // kernel configuration of SpMV / restriction
-  bool mv_nat = true;        // SpMV visits rows in natural grid order
+  int mv_order = 0;          // SpMV row order: 0 storage, 1 natural, 2 slab (see k_spmv)
   bool tuned = false;
   // level-scheduled natural order (built on first use)
   int* wave_rows = nullptr;  // colour-order rows sorted by ix + 2 iy + 4 iz

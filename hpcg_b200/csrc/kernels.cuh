@@ -45,11 +45,16 @@ __host__ __device__ constexpr int cfg_rows(int cfg) { return cfg == 4 || cfg == 
 
 // Gauss-Seidel colour phase: rows [r0, r1) of one colour, updated in parallel
 // (no two rows of a colour are neighbours).
-template <typename T, typename TR, bool FIRST, int CFG, int SCHED = cfg_sched(CFG), int R = cfg_rows(CFG)>
+// CMASK >= 0: the slot mask is that compile-time constant (the first sweep's
+// masks of the default sweep order), so unused slots drop out of the code;
+// CMASK < 0: the runtime `mask`.
+template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1, int SCHED = cfg_sched(CFG),
+          int R = cfg_rows(CFG)>
 __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* __restrict__ val,
                                                                       const int* __restrict__ col, int64_t pitch,
                                                                       const TR* __restrict__ rhs, T* x, int r0,
-                                                                      int r1, uint32_t mask) {
+                                                                      int r1, uint32_t mask_arg) {
+  const uint32_t mask = CMASK >= 0 ? (uint32_t)CMASK : mask_arg;
   if (R == 1) {
     const int stride = gridDim.x * blockDim.x;
     for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride)
@@ -122,13 +127,16 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
 
 // y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y
 // (the p'Ap of CG.cpp:119, fused).
-// NAT: rows are visited in the natural order of the grid (row q = old2new of the
-// thread's natural index), so consecutive threads touch neighbouring points and
-// the x values they gather stay in a window of a few planes held in L2; in
-// storage order each colour block would gather the other seven colours' x
-// across the whole grid again. Each warp still reads two contiguous runs of a
-// slot (the two parities of ix).
-template <typename T, bool DOT, int CFG, bool NAT, int SCHED = cfg_sched(CFG), int R = NAT ? 1 : cfg_rows(CFG)>
+// ORDER 0: rows in storage order (colour block after colour block). Each colour
+// block then gathers the other seven colours' x across the whole grid again.
+// ORDER 1: natural grid order (row q = old2new of the thread's natural index):
+// the gathered x stay in a window of a few planes held in L2, but each warp
+// reads two short runs of every slot.
+// ORDER 2: slab order: the rows of one z pair in all eight colours, then the
+// next z pair; inside a colour a slab is one contiguous run of storage, so the
+// matrix streams in long runs and the x window still fits in L2 (needs even
+// grid dimensions: every colour then holds (nx/2)(ny/2) rows per z pair).
+template <typename T, bool DOT, int CFG, int ORDER, int SCHED = cfg_sched(CFG), int R = ORDER == 1 ? 1 : cfg_rows(CFG)>
 __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, const T* __restrict__ val,
                                                                   const int* __restrict__ col, int64_t pitch,
                                                                   const T* __restrict__ x, T* __restrict__ y, int n,
@@ -138,9 +146,14 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
     const int stride = gridDim.x * blockDim.x;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
       int q = t;
-      if (NAT) {
+      if (ORDER == 1) {
         const int ix = t % g.nx, iy = (t / g.nx) % g.ny, iz = t / (g.nx * g.ny);
         q = g.old2new(ix, iy, iz);
+      } else if (ORDER == 2) {
+        const int per = (g.nx >> 1) * (g.ny >> 1);  // rows of one colour in one z pair
+        const int h = t / (kColours * per), rem = t - h * (kColours * per);
+        const int s = rem / per;
+        q = g.start[s] + h * per + (rem - s * per);
       }
       T sum = (T)0;
       T xq = (T)0;
@@ -171,8 +184,15 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
     }
   } else {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
-    for (int64_t q0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; q0 < n; q0 += stride) {
-      const int cnt = q0 + R <= n ? R : (int)(n - q0);
+    for (int64_t t0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; t0 < n; t0 += stride) {
+      int64_t q0 = t0;
+      if (ORDER == 2) {  // R rows of one run: per is a multiple of R (checked on the host)
+        const int per = (g.nx >> 1) * (g.ny >> 1);
+        const int64_t h = t0 / (kColours * (int64_t)per), rem = t0 - h * (kColours * (int64_t)per);
+        const int s = (int)(rem / per);
+        q0 = g.start[s] + h * per + (rem - (int64_t)s * per);
+      }
+      const int cnt = t0 + R <= n ? R : (int)(n - t0);
       if (cnt < R) {
         for (int q = (int)q0; q < n; ++q) {
           T sum = (T)0, xq = (T)0;

@@ -19,9 +19,9 @@ inline int red_blocks(const Context* c, int64_t n) {
   return b > kRedBlocksMax / 2 ? kRedBlocksMax / 2 : b;
 }
 
-template <typename T, typename TR, bool FIRST, int CFG>
+template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1>
 void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask) {
-  auto k = k_gs_phase<T, TR, FIRST, CFG>;
+  auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK>;
   const int64_t units = ((int64_t)(r1 - r0) + cfg_rows(CFG) - 1) / cfg_rows(CFG);
   k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask);
 }
@@ -44,18 +44,61 @@ void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rh
   }
 }
 
-template <typename T, bool DOT, int CFG>
-int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
-  if (L.mv_nat) {
-    auto k = k_spmv<T, DOT, CFG, true>;
-    const int g = grid_of(c, k, L.n);
-    k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
-    return g;
+// A first-sweep phase at sweep position s with its mask compiled in (plain
+// configurations; the staged ones take the mask at run time).
+template <typename T, typename TR, int CFG>
+void gs_first_const(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, int s) {
+  switch (s) {
+    case 0: gs_launch<T, TR, true, CFG, first_mask_default(0)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 1: gs_launch<T, TR, true, CFG, first_mask_default(1)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 2: gs_launch<T, TR, true, CFG, first_mask_default(2)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 3: gs_launch<T, TR, true, CFG, first_mask_default(3)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 4: gs_launch<T, TR, true, CFG, first_mask_default(4)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 5: gs_launch<T, TR, true, CFG, first_mask_default(5)>(c, L, val, rhs, x, r0, r1, 0); break;
+    case 6: gs_launch<T, TR, true, CFG, first_mask_default(6)>(c, L, val, rhs, x, r0, r1, 0); break;
+    default: gs_launch<T, TR, true, CFG, first_mask_default(7)>(c, L, val, rhs, x, r0, r1, 0); break;
   }
-  auto k = k_spmv<T, DOT, CFG, false>;
-  const int g = grid_of(c, k, ((int64_t)L.n + cfg_rows(CFG) - 1) / cfg_rows(CFG));
+}
+
+// The first sweep of the default sweep order with compile-time masks; other
+// configurations take the mask at run time.
+template <typename T, typename TR>
+void gs_first_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rhs, T* x, int r0, int r1,
+                       int s, uint32_t mask) {
+  bool default_order = true;
+  for (int i = 0; i < kColours; ++i) default_order = default_order && L.g.sweep[i] == kSweepDefault[i];
+  const int u = usable_cfg(cfg, r0);
+  if (default_order && (u == 0 || u == 1 || u == 4 || u == 5)) {
+    switch (u) {
+      case 0: gs_first_const<T, TR, 0>(c, L, val, rhs, x, r0, r1, s); return;
+      case 1: gs_first_const<T, TR, 1>(c, L, val, rhs, x, r0, r1, s); return;
+      case 4: gs_first_const<T, TR, 4>(c, L, val, rhs, x, r0, r1, s); return;
+      default: gs_first_const<T, TR, 5>(c, L, val, rhs, x, r0, r1, s); return;
+    }
+  }
+  gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, mask);
+}
+
+// Slab order (ORDER 2) needs even grid dimensions and slab runs that split into R-row groups.
+inline bool slab_ok(const Level& L, int R) {
+  const int per = (L.g.nx >> 1) * (L.g.ny >> 1);
+  return L.g.nx % 2 == 0 && L.g.ny % 2 == 0 && L.g.nz % 2 == 0 && per % R == 0;
+}
+
+template <typename T, bool DOT, int CFG, int ORDER>
+int spmv_launch_o(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
+  auto k = k_spmv<T, DOT, CFG, ORDER>;
+  const int r = ORDER == 1 ? 1 : cfg_rows(CFG);
+  const int g = grid_of(c, k, ((int64_t)L.n + r - 1) / r);
   k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
   return g;
+}
+
+template <typename T, bool DOT, int CFG>
+int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
+  if (L.mv_order == 1) return spmv_launch_o<T, DOT, CFG, 1>(c, L, val, x, y, partials);
+  if (L.mv_order == 2 && slab_ok(L, cfg_rows(CFG))) return spmv_launch_o<T, DOT, CFG, 2>(c, L, val, x, y, partials);
+  return spmv_launch_o<T, DOT, CFG, 0>(c, L, val, x, y, partials);
 }
 
 // Launches y = A x on level L; returns the grid (the number of partials written when DOT).
@@ -95,9 +138,9 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
   const int kind = top ? (first ? kProfGsFirst : kProfGsFull) : -1;
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
-  const int cfg = sizeof(T) == 4 ? L.gs_sched32 : L.gs_sched;
+  const int cfg = sizeof(T) == 4 ? L.gs_sched32 : first ? L.gs_first : L.gs_sched;
   if (first)
-    gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, first_mask(L.g, s));
+    gs_first_dispatch<T, TR>(c, L, cfg, val, rhs, x, r0, r1, s, first_mask(L.g, s));
   else
     gs_dispatch<T, TR, false>(c, L, cfg, val, rhs, x, r0, r1, kAllSlots);
   HB_CK(cudaGetLastError());
@@ -211,7 +254,7 @@ int autotune(hpcg_b200_problem* P) {
     L.tuned = true;
     if (force && *force) {
       const int f = std::atoi(force);
-      L.gs_sched = L.mv_sched = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
+      L.gs_sched = L.mv_sched = L.gs_first = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
       continue;
     }
     double* xs = l == 0 ? P->Ap : L.x;
@@ -222,9 +265,9 @@ int autotune(hpcg_b200_problem* P) {
     cudaEvent_t e0, e1;
     HB_CK(cudaEventCreate(&e0));
     HB_CK(cudaEventCreate(&e1));
-    float best_gs = 1e30f, best_mv = 1e30f;
+    float best_gs = 1e30f, best_mv = 1e30f, best_first = 1e30f;
     for (int sched = 0; sched < kConfigs; ++sched) {
-      float t_gs = 1e30f, t_mv[2] = {1e30f, 1e30f};
+      float t_gs = 1e30f, t_mv[3] = {1e30f, 1e30f, 1e30f};
       for (int rep = 0; rep < 3; ++rep) {
         HB_CK(cudaEventRecord(e0, c->stream));
         gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
@@ -234,23 +277,36 @@ int autotune(hpcg_b200_problem* P) {
         HB_CK(cudaEventElapsedTime(&ms, e0, e1));
         t_gs = ms < t_gs ? ms : t_gs;
         const int keep = L.mv_sched;
-        const bool keep_nat = L.mv_nat;
-        for (int nat = 0; nat < 2; ++nat) {
+        const int keep_order = L.mv_order;
+        for (int order = 0; order < 3; ++order) {
           L.mv_sched = sched;
-          L.mv_nat = nat != 0;
+          L.mv_order = order;
           HB_CK(cudaEventRecord(e0, c->stream));
           spmv_dispatch<double, false>(c, L, L.val, xs, ys, nullptr);
           HB_CK(cudaEventRecord(e1, c->stream));
           HB_CK(cudaEventSynchronize(e1));
           HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-          if (ms < t_mv[nat]) t_mv[nat] = ms;
+          if (ms < t_mv[order]) t_mv[order] = ms;
         }
         L.mv_sched = keep;
-        L.mv_nat = keep_nat;
+        L.mv_order = keep_order;
       }
       if (t_gs < best_gs) { best_gs = t_gs; L.gs_sched = sched; }
-      for (int nat = 0; nat < 2; ++nat)
-        if (t_mv[nat] < best_mv) { best_mv = t_mv[nat]; L.mv_sched = sched; L.mv_nat = nat != 0; }
+      // the first-sweep phase of a middle sweep position (about half its slots)
+      float t_f = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        const int f0 = L.g.start[4], f1 = L.g.start[5];
+        HB_CK(cudaEventRecord(e0, c->stream));
+        gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, f0, f1, 4, first_mask(L.g, 4));
+        HB_CK(cudaEventRecord(e1, c->stream));
+        HB_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+        t_f = ms < t_f ? ms : t_f;
+      }
+      if (t_f < best_first) { best_first = t_f; L.gs_first = sched; }
+      for (int order = 0; order < 3; ++order)
+        if (t_mv[order] < best_mv) { best_mv = t_mv[order]; L.mv_sched = sched; L.mv_order = order; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
