@@ -555,6 +555,9 @@ def b200_arm(args, rank, world, local_rank):
                 line["cpu_baseline"] = cpu_baseline(args)
             except Exception as ex:  # reported, not fatal
                 line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    tuning = [P.level_config(l) for l in range(4)]
+    if line:
+        line["config"]["autotuned"] = tuning
     P.free()
     if dist:
         dist.barrier()

@@ -37,7 +37,10 @@ EXPORTS = (
     "hpcg_b200_residual", "hpcg_b200_cg", "hpcg_b200_cg_mixed", "hpcg_b200_level_info",
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
-    "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
+    "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
+    "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
+    "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
+    "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
     "hpcg_b200_last_error",
 )
 
@@ -96,10 +99,23 @@ def lib():
         l.hpcg_b200_adjoint.argtypes = [vp, vp, vp, i, d, vp, vp, C.POINTER(i)]
         l.hpcg_b200_cg_multi.argtypes = [vp, i, vp, vp, i, d, vp, vp, vp]
         l.hpcg_b200_mg_multi.argtypes = [vp, i, vp, vp]
+        l.hpcg_b200_level_config.argtypes = [vp, i, vp]
         l.hpcg_b200_batch_create.argtypes = [i, vp, vp, vp, i, C.POINTER(vp)]
         l.hpcg_b200_batch_problem.argtypes = [vp, i, C.POINTER(vp)]
         l.hpcg_b200_batch_cg_mixed.argtypes = [vp, vp, vp, i, d, vp, vp, vp]
         l.hpcg_b200_batch_free.argtypes = [vp]
+        l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+        l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
+        l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
+        l.hpcg_b200_rank_info.argtypes = [vp, i, vp]
+        l.hpcg_b200_comm_unique_id.argtypes = [vp]
+        l.hpcg_b200_comm_nccl.argtypes = [vp, i, i, vp, C.POINTER(vp)]
+        l.hpcg_b200_comm_local.argtypes = [i, vp, C.POINTER(vp)]
+        l.hpcg_b200_comm_free.argtypes = [vp]
+        for f in (l.hpcg_b200_shard_spmv, l.hpcg_b200_shard_symgs, l.hpcg_b200_shard_mg):
+            f.argtypes = [vp, vp, vp]
+        l.hpcg_b200_shard_dot.argtypes = [vp, vp, vp, C.POINTER(d)]
+        l.hpcg_b200_shard_cg.argtypes = [vp, vp, vp, i, d, i, C.POINTER(i), C.POINTER(d), C.POINTER(d), vp]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -182,6 +198,21 @@ class Problem:
         h = C.c_void_p()
         _check(lib().hpcg_b200_generate(nx, ny, nz, nlevels, device, C.byref(h)), "hpcg_b200_generate")
         return cls(h.value, (nx, ny, nz), nlevels)
+
+    @classmethod
+    def generate_rank(cls, nx, ny, nz, npx, npy, npz, rank, nlevels=4, device=0):
+        """Rank `rank`'s local nx*ny*nz block of an npx*npy*npz run, with its halo
+        plan (the reference's GenerateProblem + SetupHalo on that rank)."""
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_generate_rank(nx, ny, nz, npx, npy, npz, rank, nlevels, device, C.byref(h)),
+               "hpcg_b200_generate_rank")
+        return cls(h.value, (nx, ny, nz), nlevels)
+
+    def rank_info(self, level=0):
+        out = np.zeros(10, np.int32)
+        _check(lib().hpcg_b200_rank_info(self._h, level, out.ctypes.data), "hpcg_b200_rank_info")
+        keys = ("rank", "nranks", "npx", "npy", "npz", "ipx", "ipy", "ipz", "neighbors", "externals")
+        return dict(zip(keys, (int(v) for v in out)))
 
     def free(self):
         if getattr(self, "_owned_by_batch", False):
@@ -289,6 +320,12 @@ class Problem:
                "hpcg_b200_level_info")
         return n.value, pitch.value, starts
 
+    def level_config(self, level):
+        """Autotuner choices of a level: dict(gs, gs_first, gs32, spmv, spmv_order, tuned)."""
+        out = np.zeros(6, np.int32)
+        _check(lib().hpcg_b200_level_config(self._h, level, out.ctypes.data), "hpcg_b200_level_config")
+        return dict(zip(("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned"), (int(v) for v in out)))
+
     def export_level(self, level):
         n, pitch, starts = self.level_info(level)
         n2o = np.zeros(n, np.int32)
@@ -300,6 +337,107 @@ class Problem:
                                             f2c.ctypes.data if nc else None), "hpcg_b200_export_level")
         return dict(n=n, pitch=pitch, starts=starts, new2old=n2o, cols=cols.reshape(27, pitch),
                     vals=vals.reshape(27, pitch), f2c=f2c[:nc] if nc else None)
+
+
+def process_grid(nranks):
+    """The reference's default (npx, npy, npz) for nranks (ComputeOptimalShapeXYZ.cpp)."""
+    a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+    _check(lib().hpcg_b200_process_grid(nranks, C.byref(a), C.byref(b), C.byref(c)), "hpcg_b200_process_grid")
+    return a.value, b.value, c.value
+
+
+def halo_plan(nx, ny, nz, npx, npy, npz, rank):
+    """Host-computed halo plan of one rank's level: dict(neighbors, counts,
+    send_rows (local natural), ext_global), as SetupHalo_ref.cpp stores it."""
+    nnb = C.c_int(0)
+    _check(lib().hpcg_b200_halo_plan(nx, ny, nz, npx, npy, npz, rank, C.byref(nnb), None, None, None, None),
+           "hpcg_b200_halo_plan")
+    nbr = np.zeros(26, np.int32)
+    cnt = np.zeros(26, np.int32)
+    _check(lib().hpcg_b200_halo_plan(nx, ny, nz, npx, npy, npz, rank, C.byref(nnb), nbr.ctypes.data,
+                                     cnt.ctypes.data, None, None), "hpcg_b200_halo_plan")
+    total = int(cnt[: nnb.value].sum())
+    send = np.zeros(max(total, 1), np.int32)
+    ext = np.zeros(max(total, 1), np.int64)
+    _check(lib().hpcg_b200_halo_plan(nx, ny, nz, npx, npy, npz, rank, C.byref(nnb), None, None, send.ctypes.data,
+                                     ext.ctypes.data), "hpcg_b200_halo_plan")
+    k = nnb.value
+    return dict(neighbors=nbr[:k].copy(), counts=cnt[:k].copy(), send_rows=send[:total].copy(),
+                ext_global=ext[:total].copy())
+
+
+def comm_unique_id() -> bytes:
+    """128-byte NCCL id for hpcg_b200_comm_nccl (make it on one rank, broadcast it)."""
+    buf = (C.c_ubyte * 128)()
+    _check(lib().hpcg_b200_comm_unique_id(buf), "hpcg_b200_comm_unique_id")
+    return bytes(buf)
+
+
+class Comm:
+    """The ranks of a run this process drives: one rank over NCCL
+    (Comm.nccl), or every rank on one GPU (Comm.local). The routines take one
+    vector per driven rank, in the rank's local natural order."""
+
+    def __init__(self, handle, problems):
+        self._h = C.c_void_p(handle)
+        self.problems = list(problems)
+
+    @classmethod
+    def local(cls, problems):
+        arr = (C.c_void_p * len(problems))(*[p.handle.value for p in problems])
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_comm_local(len(problems), arr, C.byref(h)), "hpcg_b200_comm_local")
+        return cls(h.value, problems)
+
+    @classmethod
+    def nccl(cls, unique_id: bytes, nranks, rank, problem):
+        buf = (C.c_ubyte * 128).from_buffer_copy(unique_id)
+        h = C.c_void_p()
+        _check(lib().hpcg_b200_comm_nccl(buf, nranks, rank, problem.handle, C.byref(h)), "hpcg_b200_comm_nccl")
+        return cls(h.value, [problem])
+
+    def free(self):
+        if self._h and self._h.value:
+            _check(lib().hpcg_b200_comm_free(self._h), "hpcg_b200_comm_free")
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def _vecs(self, vs):
+        if len(vs) != len(self.problems):
+            raise ValueError(f"{len(self.problems)} vectors expected, got {len(vs)}")
+        return (C.c_void_p * len(vs))(*[_ptr(v, p.nrow) for v, p in zip(vs, self.problems)])
+
+    def ComputeSPMV(self, xs, ys):
+        _check(lib().hpcg_b200_shard_spmv(self._h, self._vecs(xs), self._vecs(ys)), "hpcg_b200_shard_spmv")
+        return 0
+
+    def ComputeSYMGS(self, rs, xs):
+        _check(lib().hpcg_b200_shard_symgs(self._h, self._vecs(rs), self._vecs(xs)), "hpcg_b200_shard_symgs")
+        return 0
+
+    def ComputeMG(self, rs, xs):
+        _check(lib().hpcg_b200_shard_mg(self._h, self._vecs(rs), self._vecs(xs)), "hpcg_b200_shard_mg")
+        return 0
+
+    def ComputeDotProduct(self, xs, ys):
+        r = C.c_double(0)
+        _check(lib().hpcg_b200_shard_dot(self._h, self._vecs(xs), self._vecs(ys), C.byref(r)), "hpcg_b200_shard_dot")
+        return r.value
+
+    def CG(self, bs, xs, max_iter, tolerance, do_preconditioning=True, times=None):
+        ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
+        t = None if times is None else np.ascontiguousarray(times, dtype=np.float64)
+        _check(lib().hpcg_b200_shard_cg(self._h, self._vecs(bs), self._vecs(xs), max_iter, tolerance,
+                                        int(bool(do_preconditioning)), C.byref(ni), C.byref(nr), C.byref(nr0),
+                                        t.ctypes.data if t is not None else None), "hpcg_b200_shard_cg")
+        if times is not None:
+            times[:] = t
+        return ni.value, nr.value, nr0.value
 
 
 def colour_permutation(nx, ny, nz):

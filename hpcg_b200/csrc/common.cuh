@@ -7,8 +7,11 @@
 //     for slot k = (sz+1)*9 + (sy+1)*3 + (sx+1), the stencil direction, so slot 13 is
 //     the diagonal and the slot order is the reference's entry order
 //     (GenerateProblem_ref.cpp:152-172); a direction that leaves the grid holds
-//     val = 0 and col = n, the index of a permanently zero vector entry;
-//   - every colour-order vector has `pitch` >= n+1 entries, entry n always 0.
+//     val = 0 and col = n + next, the index of a permanently zero vector entry;
+//   - a rank of a run over several GPUs also references `next` external columns,
+//     the halo values of its neighbours, stored at [n, n + next) of every vector
+//     the matrix multiplies (refreshed by the halo exchange);
+//   - every colour-order vector has `pitch` >= n+next+1 entries, entry n+next always 0.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -107,10 +110,36 @@ constexpr uint32_t first_mask_default(int s) {
   return m;
 }
 
+// Halo exchange plan of one level of one rank (the data SetupHalo_ref.cpp:121-172
+// builds): neighbours in ascending rank order; neighbour i's externals are
+// entries [n + off[i], n + off[i+1]) and the rows sent to it are
+// send_rows[off[i] .. off[i+1]) (the stencil is symmetric, so a rank sends a
+// neighbour as many entries as it receives from it). Both lists are in
+// ascending global row order, so they pair up across ranks.
+struct HaloPlan {
+  int nnb = 0;
+  int nbr[26];                 // neighbour ranks, ascending
+  int dir[26];                 // their directions (dz+1)*9 + (dy+1)*3 + (dx+1)
+  int off[27];                 // entry offsets per neighbour, off[nnb] = total
+  int ext_off[27];             // by direction: offset of that neighbour's externals, -1 if none
+  int total = 0;
+  int* send_rows = nullptr;    // device [total], colour-order rows
+  double* send_buf = nullptr;  // device [total]
+};
+
+// Position of one rank in the reference's process grid (GenerateGeometry.cpp:89-91).
+struct RankGeom {
+  int size = 1, rank = 0;
+  int npx = 1, npy = 1, npz = 1;
+  int ipx = 0, ipy = 0, ipz = 0;
+};
+
 struct Level {
   ColourGrid g;
   int n = 0;                 // rows
-  int64_t pitch = 0;         // slot stride (>= n+1, multiple of 256)
+  int next = 0;              // external columns (halo), 0 on a single rank
+  HaloPlan* halo = nullptr;  // exchange plan (ranks with neighbours only)
+  int64_t pitch = 0;         // slot stride (>= n+next+1, multiple of 256)
   double* val = nullptr;     // [27][pitch]
   int* col = nullptr;        // [27][pitch]
   float* val32 = nullptr;    // FP32 copy for the mixed-precision V-cycle (built on first use)
@@ -138,6 +167,7 @@ struct Level {
 
 struct Context;
 struct MultiState;
+struct Comm;
 
 }  // namespace hb
 
@@ -153,6 +183,7 @@ struct hpcg_b200_problem {
   hb::MultiState* multi;  // work vectors of the multi-system path (created on first use)
   cudaGraphExec_t cg_graph[2];  // instantiated CG loop, [unpreconditioned, preconditioned]
   bool cg_graph_failed;         // capture was refused once: stay with stream launches
+  hb::RankGeom* geom;  // position in a run over several ranks (nullptr: one rank)
   size_t bytes;  // device bytes held
 };
 
@@ -186,6 +217,19 @@ struct Scalars {
   double normr0, tol;
   int iter;      // iterations completed
   int max_iter;
+};
+
+// Scalar updates that close a reduction (k_finalize and its rank-order twin).
+enum FinOp : int {
+  kFinStore = 0,     // *out = sum
+  kFinNormr = 1,     // s->normr2 = sum
+  kFinRtzFirst = 2,  // s->rtz = sum
+  kFinRtz = 3,       // oldrtz = rtz; rtz = sum; beta = rtz / oldrtz   (CG.cpp:112-114)
+  kFinPap = 4,       // pAp = sum; alpha = rtz / pAp                    (CG.cpp:119-120)
+  kFinFlex = 5,      // oldrtz = rtz; rtz = sum; beta = (rtz - sum2) / oldrtz (flexible PR)
+  kFinMax = 6,       // *out = max of partials
+  kFinNormr0 = 7,    // normr2 = sum; normr0 = sqrt(sum)           (CG.cpp:89-96)
+  kFinRtzIter = 8,   // iteration 1: rtz = sum; later: as kFinRtz  (CG.cpp:107-115)
 };
 
 // Kernel classes timed by the optional launch profiler.
@@ -271,6 +315,13 @@ template <typename K>
 int grid_of(Context* c, K kernel, int64_t rows) {
   return grid_for(c, rows, 256, resident(kernel));
 }
+
+// Index of the zero entry padded slots point at.
+inline int sink_of(const Level& L) { return L.n + L.next; }
+
+// true for a rank of a run over several ranks: the single-rank entry points
+// refuse it (its halo would never be exchanged)
+inline bool is_rank(const hpcg_b200_problem* p) { return p->geom != nullptr && p->geom->size > 1; }
 
 // natural <-> colour order vector movement (solver.cu)
 int load_vector(hpcg_b200_problem* p, int level, const double* src_natural, double* dst_colour);

@@ -346,17 +346,30 @@ __global__ void __launch_bounds__(kThreads) k_maxdiff(int n, const double* __res
 
 // ---- CG scalar bookkeeping on the device -----------------------------------
 
-enum FinOp : int {
-  kFinStore = 0,     // *out = sum
-  kFinNormr = 1,     // s->normr2 = sum
-  kFinRtzFirst = 2,  // s->rtz = sum
-  kFinRtz = 3,       // oldrtz = rtz; rtz = sum; beta = rtz / oldrtz   (CG.cpp:112-114)
-  kFinPap = 4,       // pAp = sum; alpha = rtz / pAp                    (CG.cpp:119-120)
-  kFinFlex = 5,      // oldrtz = rtz; rtz = sum; beta = (rtz - sum2) / oldrtz (flexible PR)
-  kFinMax = 6,       // *out = max of partials
-  kFinNormr0 = 7,    // normr2 = sum; normr0 = sqrt(sum)           (CG.cpp:89-96)
-  kFinRtzIter = 8,   // iteration 1: rtz = sum; later: as kFinRtz  (CG.cpp:107-115)
-};
+
+// The scalar update of `op` given the reduced value(s) (thread 0 only).
+__device__ __forceinline__ void apply_fin(int op, double sum, double sum2, Scalars* s, double* out) {
+  switch (op) {
+    case kFinStore: *out = sum; break;
+    case kFinNormr: s->normr2 = sum; break;
+    case kFinRtzFirst: s->rtz = sum; break;
+    case kFinRtz: s->oldrtz = s->rtz; s->rtz = sum; s->beta = sum / s->oldrtz; break;
+    case kFinPap: s->pAp = sum; s->alpha = s->rtz / sum; break;
+    case kFinFlex: s->oldrtz = s->rtz; s->rtz = sum; s->rzprev = sum2; s->beta = (sum - sum2) / s->oldrtz; break;
+    case kFinMax: *out = sum; break;
+    case kFinNormr0: s->normr2 = sum; s->normr0 = sqrt(sum); break;
+    case kFinRtzIter:
+      if (s->iter == 0) {
+        s->rtz = sum;
+      } else {
+        s->oldrtz = s->rtz;
+        s->rtz = sum;
+        s->beta = sum / s->oldrtz;
+      }
+      break;
+    default: break;
+  }
+}
 
 // One block: fixed-order reduction of nparts partials (and of the second set
 // at partials[nparts..] for kFinFlex), then the scalar update of `op`.
@@ -375,25 +388,17 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const double* __restrict_
   const double sum = block_sum(acc);
   const double sum2 = op == kFinFlex ? block_sum(acc2) : 0.0;
   if (threadIdx.x != 0) return;
-  switch (op) {
-    case kFinStore: *out = sum; break;
-    case kFinNormr: s->normr2 = sum; break;
-    case kFinRtzFirst: s->rtz = sum; break;
-    case kFinRtz: s->oldrtz = s->rtz; s->rtz = sum; s->beta = sum / s->oldrtz; break;
-    case kFinPap: s->pAp = sum; s->alpha = s->rtz / sum; break;
-    case kFinFlex: s->oldrtz = s->rtz; s->rtz = sum; s->rzprev = sum2; s->beta = (sum - sum2) / s->oldrtz; break;
-    case kFinNormr0: s->normr2 = sum; s->normr0 = sqrt(sum); break;
-    case kFinRtzIter:
-      if (s->iter == 0) {
-        s->rtz = sum;
-      } else {
-        s->oldrtz = s->rtz;
-        s->rtz = sum;
-        s->beta = sum / s->oldrtz;
-      }
-      break;
-    default: break;
-  }
+  apply_fin(op, sum, sum2, s, out);
+}
+
+// The ranks' values of one reduction, combined in rank order (a sum, or the
+// maximum for kFinMax), then the scalar update of `op`: the allreduce of
+// ComputeDotProduct_ref.cpp:70 / ComputeResidual.cpp:82 as one left fold.
+__global__ void k_finalize_ranks(const double* __restrict__ vals, int nvals, int op, Scalars* s, double* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double acc = vals[0];
+  for (int i = 1; i < nvals; ++i) acc = op == kFinMax ? fmax(acc, vals[i]) : acc + vals[i];
+  apply_fin(op, acc, 0.0, s, out);
 }
 
 // p = z + beta p (CG.cpp:115 as WAXPBY(1, z, beta, p)), beta from the device scalars.

@@ -275,6 +275,7 @@ extern "C" {
 int hpcg_b200_cg_multi(hpcg_b200_problem* p, int nrhs, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (nrhs < 1 || nrhs > kMaxRhs || !b || !x || !niters || !normr || !normr0 || max_iter < 0)
     return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
@@ -285,6 +286,7 @@ int hpcg_b200_cg_multi(hpcg_b200_problem* p, int nrhs, const double* b, double* 
 
 int hpcg_b200_mg_multi(hpcg_b200_problem* p, int nrhs, const double* r, double* x) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (nrhs < 1 || nrhs > kMaxRhs || !r || !x) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   if (nrhs <= 2) return run_mg_multi<2>(p, nrhs, r, x);

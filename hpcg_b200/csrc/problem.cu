@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "shard.cuh"
 
 namespace hb {
 
@@ -70,8 +71,21 @@ void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)>& body) 
 
 // ---- device generator (GenerateProblem_ref.cpp:131-183 in colour order) -----
 
-__global__ void k_generate(ColourGrid g, int n, int64_t pitch, double* __restrict__ val, int* __restrict__ col,
-                           int* __restrict__ new2old, int* __restrict__ old2new, double* __restrict__ b) {
+// Where this level's block sits in the global grid (one rank: the whole grid).
+struct GenGeom {
+  int gnx, gny, gnz;  // global grid of the level
+  int gx0, gy0, gz0;  // first global coordinate of this rank's block
+  int ext_off[27];    // by direction (dz+1)*9+(dy+1)*3+(dx+1): first external column of that neighbour, -1 none
+  int sink;           // the zero column of padded slots
+};
+
+// Rows, values and columns of one level. A direction inside the global grid but
+// outside this rank's block is a nonzero of the reference's matrix too
+// (GenerateProblem_ref.cpp:152-162 tests the global bounds); its column is the
+// neighbour's external entry, numbered as the halo plan orders them.
+__global__ void k_generate(ColourGrid g, int n, int64_t pitch, GenGeom G, double* __restrict__ val,
+                           int* __restrict__ col, int* __restrict__ new2old, int* __restrict__ old2new,
+                           double* __restrict__ b) {
   const int stride = gridDim.x * blockDim.x;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
     int ix, iy, iz;
@@ -83,8 +97,27 @@ __global__ void k_generate(ColourGrid g, int n, int64_t pitch, double* __restric
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       const int jx = ix + k % 3 - 1, jy = iy + (k / 3) % 3 - 1, jz = iz + k / 9 - 1;
-      const bool in = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
-      col[k * pitch + q] = in ? g.old2new(jx, jy, jz) : n;
+      const bool local = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
+      const int gx = G.gx0 + jx, gy = G.gy0 + jy, gz = G.gz0 + jz;
+      bool in = gx >= 0 && gx < G.gnx && gy >= 0 && gy < G.gny && gz >= 0 && gz < G.gnz;
+      int c = G.sink;
+      if (local) {
+        c = g.old2new(jx, jy, jz);
+      } else if (in) {
+        const int ex = jx < 0 ? -1 : jx >= g.nx ? 1 : 0;
+        const int ey = jy < 0 ? -1 : jy >= g.ny ? 1 : 0;
+        const int ez = jz < 0 ? -1 : jz >= g.nz ? 1 : 0;
+        const int off = G.ext_off[(ez + 1) * 9 + (ey + 1) * 3 + (ex + 1)];
+        if (off >= 0) {
+          const int lx = ex == 0 ? jx : 0, wx = ex == 0 ? g.nx : 1;
+          const int ly = ey == 0 ? jy : 0, wy = ey == 0 ? g.ny : 1;
+          const int lz = ez == 0 ? jz : 0;
+          c = n + off + (lz * wy + ly) * wx + lx;
+        } else {
+          in = false;  // no such neighbour: cannot happen for a block of the process grid
+        }
+      }
+      col[k * pitch + q] = c;
       val[k * pitch + q] = in ? (k == kDiagSlot ? 26.0 : -1.0) : 0.0;
       cnt += in ? 1 : 0;
     }
@@ -169,11 +202,80 @@ int free_problem(hpcg_b200_problem* p) {
   void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
   for (void* q : vs) dev_free(q);
   free_multi(p);
+  free_plans(p);
   for (int i = 0; i < 2; ++i)
     if (p->cg_graph[i]) cudaGraphExecDestroy(p->cg_graph[i]);
   release_accounted(p->bytes);
   p->magic = 0;
   delete p;
+  return HPCG_B200_OK;
+}
+
+// Device generation of the hierarchy of one rank (geom == nullptr: the whole grid
+// on one rank), GenerateProblem_ref.cpp:131-183, GenerateCoarseProblem.cpp:71-104
+// and, for a rank with neighbours, the halo plan of SetupHalo_ref.cpp:69-176.
+int generate_impl(int nx, int ny, int nz, int nlevels, int device, const RankGeom* geom, hpcg_b200_problem** out) {
+  if (!out) return HPCG_B200_ERR_ARG;
+  *out = nullptr;
+  HB_TRY(check_dims(nx, ny, nz, nlevels));
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_CK(cudaSetDevice(device));
+  hpcg_b200_problem* p = new_problem(device, c);
+  p->nlev = nlevels;
+  if (geom) p->geom = new RankGeom(*geom);
+  const RankGeom G = geom ? *geom : RankGeom();
+  std::vector<std::vector<int> > sends(nlevels);
+  for (int l = 0; l < nlevels; ++l) {
+    Level& L = p->lev[l];
+    L.g.init(nx >> l, ny >> l, nz >> l, kSweepDefault);
+    L.n = (nx >> l) * (ny >> l) * (nz >> l);
+    if (G.size > 1) {
+      L.halo = new HaloPlan;
+      plan_level(G, nx >> l, ny >> l, nz >> l, *L.halo, sends[l]);
+      L.next = L.halo->total;
+    }
+    L.pitch = pitch_for(L.n + L.next);
+  }
+  int status = HPCG_B200_OK;
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
+    Level& L = p->lev[l];
+    status = alloc_n(p, &L.val, kSlots * L.pitch);
+    if (!status) status = alloc_n(p, &L.col, kSlots * L.pitch);
+    if (!status) status = alloc_n(p, &L.new2old, L.n);
+    if (!status) status = alloc_n(p, &L.old2new, L.n);
+    if (!status && l + 1 < nlevels) status = alloc_n(p, &L.f2c, p->lev[l + 1].n);
+  }
+  if (status == HPCG_B200_OK) status = alloc_vectors(p);
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
+    Level& L = p->lev[l];
+    // padding columns of the tail [n, pitch) are never read; zero them anyway
+    cudaError_t e = cudaMemsetAsync(L.val, 0, sizeof(double) * kSlots * L.pitch, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.col, 0, sizeof(int) * kSlots * L.pitch, c->stream);
+    if (e != cudaSuccess) { set_error("generate memset", e); status = status_of(e); break; }
+    const int lx = nx >> l, ly = ny >> l, lz = nz >> l;
+    GenGeom gg;
+    gg.gnx = G.npx * lx; gg.gny = G.npy * ly; gg.gnz = G.npz * lz;
+    gg.gx0 = G.ipx * lx; gg.gy0 = G.ipy * ly; gg.gz0 = G.ipz * lz;
+    for (int d = 0; d < 27; ++d) gg.ext_off[d] = L.halo ? L.halo->ext_off[d] : -1;
+    gg.sink = sink_of(L);
+    k_generate<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(L.g, L.n, L.pitch, gg, L.val, L.col, L.new2old,
+                                                                  L.old2new, l == 0 ? p->b : nullptr);
+    if (l + 1 < nlevels) {
+      const Level& C = p->lev[l + 1];
+      k_generate_f2c<<<grid_for(c, C.n, 256, 8), 256, 0, c->stream>>>(L.g, C.g, C.n, L.f2c);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_error("generate", e); status = status_of(e); }
+  }
+  for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) status = upload_plan(p, l, sends[l]);
+  if (status != HPCG_B200_OK) {
+    free_problem(p);
+    return status;
+  }
+  *out = p;
   return HPCG_B200_OK;
 }
 
@@ -287,52 +389,54 @@ int hpcg_b200_optimize(const hpcg_b200_level_desc* desc, int nlevels, int device
 }
 
 int hpcg_b200_generate(int nx, int ny, int nz, int nlevels, int device, hpcg_b200_problem** out) {
+  return generate_impl(nx, ny, nz, nlevels, device, nullptr, out);
+}
+
+int hpcg_b200_generate_rank(int nx, int ny, int nz, int npx, int npy, int npz, int rank, int nlevels, int device,
+                            hpcg_b200_problem** out) {
   if (!out) return HPCG_B200_ERR_ARG;
   *out = nullptr;
-  HB_TRY(check_dims(nx, ny, nz, nlevels));
-  Context* c = context_for(device);
-  if (!c) return HPCG_B200_ERR_CUDA;
-  HB_CK(cudaSetDevice(device));
-  hpcg_b200_problem* p = new_problem(device, c);
-  p->nlev = nlevels;
-  int status = HPCG_B200_OK;
-  for (int l = 0; l < nlevels; ++l) {
-    Level& L = p->lev[l];
-    L.g.init(nx >> l, ny >> l, nz >> l, kSweepDefault);
-    L.n = (nx >> l) * (ny >> l) * (nz >> l);
-    L.pitch = pitch_for(L.n);
+  RankGeom g;
+  if (!make_geom(npx, npy, npz, rank, g)) return HPCG_B200_ERR_ARG;
+  if ((int64_t)npx * nx >= (1 << 30) || (int64_t)npy * ny >= (1 << 30) || (int64_t)npz * nz >= (1 << 30))
+    return HPCG_B200_ERR_UNSUPPORTED;
+  return generate_impl(nx, ny, nz, nlevels, device, &g, out);
+}
+
+int hpcg_b200_process_grid(int nranks, int* npx, int* npy, int* npz) {
+  if (nranks < 1 || !npx || !npy || !npz) return HPCG_B200_ERR_ARG;
+  optimal_shape(nranks, *npx, *npy, *npz);
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_halo_plan(int nx, int ny, int nz, int npx, int npy, int npz, int rank, int* nneighbors,
+                        int* neighbors, int* counts, int* send_rows, long long* ext_global) {
+  RankGeom g;
+  if (!make_geom(npx, npy, npz, rank, g) || nx < 1 || ny < 1 || nz < 1 || !nneighbors) return HPCG_B200_ERR_ARG;
+  HaloPlan h;
+  std::vector<int> send;
+  plan_level(g, nx, ny, nz, h, send);
+  *nneighbors = h.nnb;
+  for (int i = 0; i < h.nnb; ++i) {
+    if (neighbors) neighbors[i] = h.nbr[i];
+    if (counts) counts[i] = h.off[i + 1] - h.off[i];
   }
-  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
-    Level& L = p->lev[l];
-    status = alloc_n(p, &L.val, kSlots * L.pitch);
-    if (!status) status = alloc_n(p, &L.col, kSlots * L.pitch);
-    if (!status) status = alloc_n(p, &L.new2old, L.n);
-    if (!status) status = alloc_n(p, &L.old2new, L.n);
-    if (!status && l + 1 < nlevels) status = alloc_n(p, &L.f2c, p->lev[l + 1].n);
+  if (send_rows) std::copy(send.begin(), send.end(), send_rows);
+  if (ext_global) {
+    std::vector<long long> ext;
+    plan_externals(g, nx, ny, nz, h, ext);
+    std::copy(ext.begin(), ext.end(), ext_global);
   }
-  if (status == HPCG_B200_OK) status = alloc_vectors(p);
-  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) {
-    Level& L = p->lev[l];
-    // padding columns of the tail [n, pitch) are never read; zero them anyway
-    cudaError_t e = cudaMemsetAsync(L.val, 0, sizeof(double) * kSlots * L.pitch, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(L.col, 0, sizeof(int) * kSlots * L.pitch, c->stream);
-    if (e != cudaSuccess) { set_error("generate memset", e); status = status_of(e); break; }
-    k_generate<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(L.g, L.n, L.pitch, L.val, L.col, L.new2old,
-                                                                  L.old2new, l == 0 ? p->b : nullptr);
-    if (l + 1 < nlevels) {
-      const Level& C = p->lev[l + 1];
-      k_generate_f2c<<<grid_for(c, C.n, 256, 8), 256, 0, c->stream>>>(L.g, C.g, C.n, L.f2c);
-    }
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) { set_error("generate", e); status = status_of(e); }
-  }
-  for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
-  if (status != HPCG_B200_OK) {
-    free_problem(p);
-    return status;
-  }
-  *out = p;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_rank_info(const hpcg_b200_problem* p, int level, int* info) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!info || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  const RankGeom g = p->geom ? *p->geom : RankGeom();
+  const Level& L = p->lev[level];
+  const int v[10] = {g.rank, g.size, g.npx, g.npy, g.npz, g.ipx, g.ipy, g.ipz, L.halo ? L.halo->nnb : 0, L.next};
+  std::copy(v, v + 10, info);
   return HPCG_B200_OK;
 }
 

@@ -268,7 +268,7 @@ int autotune(hpcg_b200_problem* P) {
     float best_gs = 1e30f, best_mv = 1e30f, best_first = 1e30f;
     for (int sched = 0; sched < kConfigs; ++sched) {
       float t_gs = 1e30f, t_mv[3] = {1e30f, 1e30f, 1e30f};
-      for (int rep = 0; rep < 3; ++rep) {
+      for (int rep = 0; rep < 4; ++rep) {
         HB_CK(cudaEventRecord(e0, c->stream));
         gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
         HB_CK(cudaEventRecord(e1, c->stream));
@@ -281,8 +281,9 @@ int autotune(hpcg_b200_problem* P) {
         for (int order = 0; order < 3; ++order) {
           L.mv_sched = sched;
           L.mv_order = order;
+          // the variant CG runs: fused with the p'Ap partials
           HB_CK(cudaEventRecord(e0, c->stream));
-          spmv_dispatch<double, false>(c, L, L.val, xs, ys, nullptr);
+          spmv_dispatch<double, true>(c, L, L.val, xs, ys, c->partials);
           HB_CK(cudaEventRecord(e1, c->stream));
           HB_CK(cudaEventSynchronize(e1));
           HB_CK(cudaEventElapsedTime(&ms, e0, e1));
@@ -307,6 +308,8 @@ int autotune(hpcg_b200_problem* P) {
       if (t_f < best_first) { best_first = t_f; L.gs_first = sched; }
       for (int order = 0; order < 3; ++order)
         if (t_mv[order] < best_mv) { best_mv = t_mv[order]; L.mv_sched = sched; L.mv_order = order; }
+      const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
+      if (fo && *fo) L.mv_order = std::atoi(fo);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -698,6 +701,90 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
 
 int prepare_f32(hpcg_b200_problem* p) { return ensure_f32(p); }
 
+// ---- pieces of the single-rank path the sharded drivers reuse (shard.cuh) ----
+
+int autotune_problem(hpcg_b200_problem* p) { return autotune(p); }
+
+// a launch error as the negative status (the success value of the reducing
+// launchers is their partial count)
+int neg_status(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return 0;
+  set_error(what, e);
+  return -status_of(e);
+}
+
+int spmv_level(hpcg_b200_problem* p, int l, const double* x, double* y, bool dot) {
+  Context* c = p->ctx;
+  const Level& L = p->lev[l];
+  const int parts = dot ? spmv_dispatch<double, true>(c, L, L.val, x, y, c->partials)
+                        : spmv_dispatch<double, false>(c, L, L.val, x, y, nullptr);
+  const int e = neg_status("spmv");
+  if (e) return dot ? e : -e;
+  return dot ? parts : HPCG_B200_OK;
+}
+
+int restrict_level(hpcg_b200_problem* p, int l, const double* rf, const double* xf, double* rc) {
+  const Level& L = p->lev[l];
+  restrict_dispatch<double>(p->ctx, L, L.val, rf, xf, rc, p->lev[l + 1].n);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int prolong_level(hpcg_b200_problem* p, int l, const double* xc, double* xf) {
+  const Level& L = p->lev[l];
+  const int nc = p->lev[l + 1].n;
+  Context* c = p->ctx;
+  k_prolong<double><<<grid_for(c, nc, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, xc, xf, nc);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int symgs_step(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero) {
+  return symgs_level(p, l, rhs, x, x_is_zero);
+}
+
+int reduction_blocks(const Context* c, int64_t n) { return red_blocks(c, n); }
+
+int launch_residual(Context* c, int n, const double* b, const double* Ap, double* r) {
+  const int nb = red_blocks(c, n);
+  k_waxpby<true><<<nb, kThreads, 0, c->stream>>>(n, 1.0, b, -1.0, Ap, r, c->partials);
+  const int e = neg_status("launch_residual");
+  return e ? e : nb;
+}
+
+int launch_dot(Context* c, int n, const double* x, const double* y) {
+  const int nb = red_blocks(c, n);
+  k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, x, y, nullptr, c->partials);
+  const int e = neg_status("launch_dot");
+  return e ? e : nb;
+}
+
+int launch_update_p(Context* c, int n, const double* z, double* p) {
+  k_update_p<<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, z, p, c->scal);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int launch_update_xr(Context* c, int n, double* x, const double* p, double* r, const double* Ap) {
+  const int nb = red_blocks(c, n);
+  k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, x, p, r, Ap, c->scal, c->partials);
+  const int e = neg_status("launch_update_xr");
+  return e ? e : nb;
+}
+
+int launch_finalize(Context* c, int nparts, int op, double* out) {
+  k_finalize<<<1, kThreads, 0, c->stream>>>(c->partials, nparts, op, c->scal, out);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
+int launch_finalize_ranks(Context* c, const double* vals, int nvals, int op, double* out) {
+  k_finalize_ranks<<<1, 32, 0, c->stream>>>(vals, nvals, op, c->scal, out);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
+}
+
 // natural-order src (host or device) -> colour-order device dst
 int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
   const Level& L = p->lev[level];
@@ -755,6 +842,7 @@ extern "C" {
 
 int hpcg_b200_spmv(hpcg_b200_problem* p, const double* x, double* y) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!x || !y) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   const Level& L = p->lev[0];
@@ -768,6 +856,7 @@ int hpcg_b200_spmv(hpcg_b200_problem* p, const double* x, double* y) {
 
 int hpcg_b200_symgs(hpcg_b200_problem* p, const double* r, double* x) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!r || !x) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, r, p->r));
@@ -779,6 +868,7 @@ int hpcg_b200_symgs(hpcg_b200_problem* p, const double* r, double* x) {
 
 int hpcg_b200_mg(hpcg_b200_problem* p, const double* r, double* x) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!r || !x) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, r, p->r));
@@ -790,6 +880,7 @@ int hpcg_b200_mg(hpcg_b200_problem* p, const double* r, double* x) {
 int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                  int do_preconditioning, int* niters, double* normr, double* normr0, double* times) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, b, p->b));
@@ -801,6 +892,7 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
 int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   HB_TRY(load_vector(p, 0, b, p->b));
@@ -812,6 +904,7 @@ int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max
 int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, int max_iter, double tolerance,
                       double* grad_b, double* grad_values27, int* niters) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!x || !g || !grad_b || !grad_values27 || !niters || max_iter < 0) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
   const Level& L = p->lev[0];
@@ -837,6 +930,19 @@ int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, in
     set_error("hpcg_b200_adjoint", e);
     return status_of(e);
   }
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!config || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  const Level& L = p->lev[level];
+  config[0] = L.gs_sched;
+  config[1] = L.gs_first;
+  config[2] = L.gs_sched32;
+  config[3] = L.mv_sched;
+  config[4] = L.mv_order;
+  config[5] = L.tuned ? 1 : 0;
   return HPCG_B200_OK;
 }
 

@@ -199,6 +199,65 @@ int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, in
 #define HPCG_B200_DOT_NOALLOC_MAX_N 268435456
 int hpcg_b200_dot_noalloc(int n, const double* x, const double* y, double* result, void* stream);
 
+/* ---- several ranks, one per GPU ----------------------------------------------
+ *
+ * The reference's MPI decomposition: npx*npy*npz ranks, each owning an
+ * nx*ny*nz block of the (npx*nx) x (npy*ny) x (npz*nz) grid, rank r at
+ * (r % npx, (r / npx) % npy, r / (npx*npy)) (src/GenerateGeometry.cpp:89-91).
+ * Each rank's matrix has the rows of its block and, as external columns, the
+ * neighbours' points next to it (src/SetupHalo_ref.cpp:69-176). Every SpMV and
+ * every symmetric Gauss-Seidel step starts with a halo exchange
+ * (src/ComputeSPMV_ref.cpp:53, src/ComputeSYMGS_ref.cpp:59, src/ExchangeHalo.cpp),
+ * every dot product ends with an allreduce (src/ComputeDotProduct_ref.cpp:70).
+ * The single-rank entry points above refuse a rank of a run over several ranks
+ * (HPCG_B200_ERR_UNSUPPORTED); the hpcg_b200_shard_* routines drive it. */
+
+/* The reference's default process grid for nranks (src/ComputeOptimalShapeXYZ.cpp). */
+int hpcg_b200_process_grid(int nranks, int* npx, int* npy, int* npz);
+
+/* Generates rank `rank`'s block and hierarchy on `device`, with the halo plan of
+ * every level (the reference's GenerateProblem + SetupHalo + GenerateCoarseProblem
+ * run by that rank). nx, ny, nz are the LOCAL block sides. */
+int hpcg_b200_generate_rank(int nx, int ny, int nz, int npx, int npy, int npz, int rank, int nlevels, int device,
+                            hpcg_b200_problem** out);
+
+/* The halo plan of one rank's level with local sides nx, ny, nz, computed on
+ * the host (no GPU): neighbour ranks in ascending order, the entries exchanged
+ * with each (sent = received), the local natural rows sent in that order
+ * (elementsToSend), and the global row of every external column in local column
+ * order (SetupHalo_ref.cpp:121-140). Arrays may be NULL; neighbors/counts hold
+ * up to 26, the two lists the sum of counts. */
+int hpcg_b200_halo_plan(int nx, int ny, int nz, int npx, int npy, int npz, int rank, int* nneighbors,
+                        int* neighbors, int* counts, int* send_rows, long long* ext_global);
+
+/* 10 ints for one level: rank, nranks, npx, npy, npz, ipx, ipy, ipz,
+ * neighbours, external columns. */
+int hpcg_b200_rank_info(const hpcg_b200_problem* p, int level, int* info);
+
+/* Communicators. NCCL: one rank per process; every rank passes the same
+ * 128-byte id, made once by hpcg_b200_comm_unique_id and broadcast by the
+ * caller (MPI_Bcast, torch.distributed, ...); libnccl.so.2 is opened at run
+ * time. Local: all nranks ranks of the run in this process, on one GPU, in rank
+ * order (halo by device copies, reductions folded in rank order). */
+typedef struct hpcg_b200_comm hpcg_b200_comm;
+#define HPCG_B200_COMM_ID_BYTES 128
+int hpcg_b200_comm_unique_id(void* id);
+int hpcg_b200_comm_nccl(const void* id, int nranks, int rank, hpcg_b200_problem* p, hpcg_b200_comm** out);
+int hpcg_b200_comm_local(int nranks, hpcg_b200_problem* const* ranks, hpcg_b200_comm** out);
+int hpcg_b200_comm_free(hpcg_b200_comm* comm);
+
+/* The routines over every rank of the run. Each takes one vector per rank this
+ * process drives (one for a NCCL communicator, nranks for a local one), in the
+ * rank's local natural row order, host or device memory; x of symgs is in/out.
+ * Every process of a NCCL run calls the same routine with the same arguments. */
+int hpcg_b200_shard_spmv(hpcg_b200_comm* comm, const double* const* x, double* const* y);
+int hpcg_b200_shard_symgs(hpcg_b200_comm* comm, const double* const* r, double* const* x);
+int hpcg_b200_shard_mg(hpcg_b200_comm* comm, const double* const* r, double* const* x);
+int hpcg_b200_shard_dot(hpcg_b200_comm* comm, const double* const* x, const double* const* y, double* result);
+int hpcg_b200_shard_cg(hpcg_b200_comm* comm, const double* const* b, double* const* x, int max_iter,
+                       double tolerance, int do_preconditioning, int* niters, double* normr, double* normr0,
+                       double* times);
+
 /* ---- inspection (tests) -------------------------------------------------- */
 
 /* Rows, padded pitch and colour-block boundaries (9 ints) of one level. */
@@ -209,6 +268,12 @@ int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64
  * next level] (colour order, NULL allowed). */
 int hpcg_b200_export_level(const hpcg_b200_problem* p, int level, int* new2old, int* cols, double* vals,
                            int* f2c);
+
+/* The autotuner's choices for one level (6 ints): kernel configuration of the
+ * Gauss-Seidel phases, of the first-sweep phases, of the FP32 phases, of the
+ * SpMV/restriction, the SpMV row order (0 storage, 1 natural, 2 slab), and
+ * whether the level has been tuned yet (tuning happens on first use). */
+int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config);
 
 /* The row order the library uses for an (nx, ny, nz) grid, computed on the host
  * (no GPU needed): new2old[q] = natural row of colour-order row q, and

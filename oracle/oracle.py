@@ -471,3 +471,152 @@ class Reference:
         a, b, c = C.c_double(0), C.c_double(0), C.c_int(0)
         self.l.ref_test_symmetry(self.h, seed, C.byref(a), C.byref(b), C.byref(c))
         return dict(depsym_spmv=a.value, depsym_mg=b.value, count_fail=c.value)
+
+
+REF_MPI_LIB = os.path.join(HERE, "_ref", "libhpcg_ref_mpi.so")
+
+
+def have_reference_ranks() -> bool:
+    return os.path.exists(REF_MPI_LIB)
+
+
+class ReferenceRanks:
+    """The reference run as npx*npy*npz MPI ranks (its MPI branch, compiled
+    against the thread-based MPI stand-in in mpi_shim/): every call runs the
+    reference routine on all ranks at once. Vectors are lists with one array per
+    rank, in the rank's local row order."""
+
+    _lib = None
+
+    @classmethod
+    def _load(cls):
+        if cls._lib is None:
+            l = C.CDLL(REF_MPI_LIB)
+            vp, i = C.c_void_p, C.c_int
+            pp = C.POINTER(C.POINTER(C.c_double))
+            l.refmpi_create.restype = vp
+            l.refmpi_create.argtypes = [i] * 6
+            l.refmpi_destroy.argtypes = [vp]
+            l.refmpi_level_sizes.argtypes = [vp, i, i, _i32p]
+            l.refmpi_export_level.argtypes = [vp, i, i] + [vp] * 10
+            l.refmpi_get_b.argtypes = [vp, i, _f64p]
+            l.refmpi_set_b.argtypes = [vp, i, _f64p]
+            for f in (l.refmpi_spmv, l.refmpi_symgs, l.refmpi_mg):
+                f.restype = i
+                f.argtypes = [vp, i, pp, pp]
+            l.refmpi_dot.restype = C.c_double
+            l.refmpi_dot.argtypes = [vp, pp, pp]
+            l.refmpi_cg.restype = i
+            l.refmpi_cg.argtypes = [vp, pp, i, C.c_double, i, C.POINTER(i), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double)]
+            l.refmpi_permute.argtypes = [vp, i, C.POINTER(C.POINTER(C.c_int))]
+            l.refmpi_optimal_shape.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+            cls._lib = l
+        return cls._lib
+
+    @classmethod
+    def optimal_shape(cls, size):
+        """ComputeOptimalShapeXYZ(size) of the reference."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        cls._load().refmpi_optimal_shape(size, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def __init__(self, npx, npy, npz, nx, ny=None, nz=None):
+        self.l = self._load()
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        self.grid = (npx, npy, npz)
+        self.dims = (nx, ny, nz)
+        self.nranks = npx * npy * npz
+        self.h = self.l.refmpi_create(npx, npy, npz, nx, ny, nz)
+
+    def close(self):
+        if self.h:
+            self.l.refmpi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sizes(self, rank, lev=0):
+        """(nrow, ncol, neighbours, entries sent) of one rank's level."""
+        s = np.zeros(4, np.int32)
+        self.l.refmpi_level_sizes(self.h, rank, lev, s)
+        return tuple(int(v) for v in s)
+
+    def export(self, rank, lev=0):
+        n, ncol, nnb, nsend = self.sizes(rank, lev)
+        nc = self.sizes(rank, lev + 1)[0] if lev < 3 else 0
+        out = dict(nnz=np.zeros(n, np.int32), cols=np.zeros(n * SLOTS, np.int32), vals=np.zeros(n * SLOTS),
+                   f2c=np.zeros(max(nc, 1), np.int32), neighbors=np.zeros(max(nnb, 1), np.int32),
+                   recv_len=np.zeros(max(nnb, 1), np.int32), send_len=np.zeros(max(nnb, 1), np.int32),
+                   send_rows=np.zeros(max(nsend, 1), np.int32), ext_global=np.zeros(max(ncol - n, 1), np.int64),
+                   l2g=np.zeros(n, np.int64))
+        keys = ("nnz", "cols", "vals", "f2c", "neighbors", "recv_len", "send_len", "send_rows", "ext_global", "l2g")
+        self.l.refmpi_export_level(self.h, rank, lev, *[out[k].ctypes.data for k in keys])
+        out["f2c"] = out["f2c"][:nc] if nc else None
+        for k, m in (("neighbors", nnb), ("recv_len", nnb), ("send_len", nnb), ("send_rows", nsend),
+                     ("ext_global", ncol - n)):
+            out[k] = out[k][:m]
+        out.update(n=n, ncol=ncol)
+        return out
+
+    def get_b(self, rank):
+        b = np.zeros(self.sizes(rank)[0])
+        self.l.refmpi_get_b(self.h, rank, b)
+        return b
+
+    def set_b(self, rank, b):
+        self.l.refmpi_set_b(self.h, rank, np.ascontiguousarray(b, np.float64))
+
+    def _cols(self, vecs, lev):
+        """Per-rank copies with ncol entries (externals zero), and their pointer array."""
+        full = []
+        for r, v in enumerate(vecs):
+            n, ncol = self.sizes(r, lev)[:2]
+            f = np.zeros(ncol)
+            f[:n] = v[:n]
+            full.append(f)
+        return full, self._ptrs(full)
+
+    @staticmethod
+    def _ptrs(arrs):
+        return (C.POINTER(C.c_double) * len(arrs))(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs])
+
+    def spmv(self, xs, lev=0):
+        xf, xp = self._cols(xs, lev)
+        ys = [np.zeros(self.sizes(r, lev)[0]) for r in range(self.nranks)]
+        assert self.l.refmpi_spmv(self.h, lev, xp, self._ptrs(ys)) == 0
+        return ys
+
+    def symgs(self, rs, xs, lev=0):
+        rs = [np.ascontiguousarray(r, np.float64) for r in rs]
+        xf, xp = self._cols(xs, lev)
+        assert self.l.refmpi_symgs(self.h, lev, self._ptrs(rs), xp) == 0
+        return [x[: self.sizes(r, lev)[0]].copy() for r, x in enumerate(xf)]
+
+    def mg(self, rs, lev=0):
+        rs = [np.ascontiguousarray(r, np.float64) for r in rs]
+        xf, xp = self._cols([np.zeros(self.sizes(r, lev)[0]) for r in range(self.nranks)], lev)
+        assert self.l.refmpi_mg(self.h, lev, self._ptrs(rs), xp) == 0
+        return [x[: self.sizes(r, lev)[0]].copy() for r, x in enumerate(xf)]
+
+    def dot(self, xs, ys):
+        xs = [np.ascontiguousarray(v, np.float64) for v in xs]
+        ys = [np.ascontiguousarray(v, np.float64) for v in ys]
+        return self.l.refmpi_dot(self.h, self._ptrs(xs), self._ptrs(ys))
+
+    def cg(self, max_iter, tol, do_prec=True):
+        xf, xp = self._cols([np.zeros(self.sizes(r)[0]) for r in range(self.nranks)], 0)
+        ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
+        assert self.l.refmpi_cg(self.h, xp, max_iter, tol, int(do_prec), C.byref(ni), C.byref(nr),
+                                C.byref(nr0)) == 0
+        return [x[: self.sizes(r)[0]].copy() for r, x in enumerate(xf)], ni.value, nr.value, nr0.value
+
+    def permute(self, rank, new2old_per_level):
+        keep = [np.ascontiguousarray(a, np.int32) for a in new2old_per_level]
+        arr = (C.POINTER(C.c_int) * len(keep))(*[a.ctypes.data_as(C.POINTER(C.c_int)) for a in keep])
+        self.l.refmpi_permute(self.h, rank, arr)
