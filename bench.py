@@ -7,10 +7,14 @@ One step = one HPCG CG set (50 preconditioned CG iterations from x = 0, toleranc
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Prints one JSON line on rank 0. Under torchrun each rank (one per GPU) solves
-its own 512^3 problem; the path has no cross-problem exchange on one process
-per GPU, so N ranks are N replicas ("scaling": "weak") and the value is the
-summed work over the slowest rank's time.
+Prints one JSON line on rank 0. Under torchrun (N > 1) the ranks, one per GPU,
+are the reference's MPI decomposition: each owns a 512^3 block of the
+(npx*512) x (npy*512) x (npz*512) grid (process grid as the reference factors
+N), exchanges halos with its neighbours over NCCL before every SpMV and
+symmetric Gauss-Seidel step and allreduces every dot product, as HPCG's weak
+scaling runs do ("scaling": "weak"); the value is the global problem's HPCG
+flops over the slowest rank's time. --replicas instead solves N independent
+512^3 problems.
 
 value: HPCG GFLOP/s (the reference FLOP model, src/ReportResults.cpp:75-99) with
 b and x resident in HBM. e2e: the same metric through the C ABI with pinned
@@ -51,6 +55,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 128^3 implicit-adjoint timing")
     ap.add_argument("--no-multi", action="store_true", help="skip the 256^3, 8 right-hand-side comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 16-problem batched comparison")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 GPUs: N independent problems instead of one decomposed problem")
     return ap.parse_args()
 
 
@@ -567,6 +573,116 @@ def b200_arm(args, rank, world, local_rank):
     return 0
 
 
+def shard_launches_per_set(iters, nlevels=4):
+    """Kernels one rank launches for one sharded CG call (its own kernels only)."""
+    # per non-coarsest level: first sweep (15 phases), halo pack, restriction,
+    # prolongation, halo pack, post sweep (15 phases); coarsest: 15 phases
+    per_mg = (15 + 1 + 1 + 1 + 1 + 15) * (nlevels - 1) + 15
+    # r'z (dot, store, rank fold), p update (k > 1), halo pack, SpMV + store + fold, x/r update + store + fold
+    per_iter = per_mg + 3 + 1 + 1 + 3 + 3
+    return iters * per_iter - 1 + 3 + (1 + 3)  # k = 1 copies; loads/stores; preamble pack + SpMV/residual/folds
+
+
+def shard_arm(args, rank, world, local_rank):
+    """One rank of the decomposition over `world` GPUs (NCCL halo + allreduce)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from hpcg_b200 import binding as B
+    from hpcg_b200 import metrics
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    n = args.n
+    nrow = n ** 3
+    npx, npy, npz = B.process_grid(world)
+    t_setup = time.perf_counter()
+    P = B.Problem.generate_rank(n, n, n, npx, npy, npz, rank, 4, dev)
+    obj = [B.comm_unique_id() if rank == 0 else None]
+    dist.broadcast_object_list(obj, src=0)
+    C = B.Comm.nccl(obj[0], world, rank, P)
+    t_setup = time.perf_counter() - t_setup
+    b = torch.from_numpy(P.get_rhs()).to(f"cuda:{dev}")
+    x = torch.zeros(nrow, dtype=torch.float64, device=f"cuda:{dev}")
+    lib_stream = torch.cuda.ExternalStream(B.stream(dev), device=dev)
+
+    def step(bv, xv):
+        xv.zero_()
+        if xv.is_cuda:
+            torch.cuda.current_stream().synchronize()
+        return C.CG([bv], [xv], args.iters, 0.0, True)
+
+    def timed_steps(bv, xv):
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        r = None
+        for _ in range(args.steps):
+            r = step(bv, xv)
+        e1.record(lib_stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), r
+
+    for _ in range(args.warmup):
+        step(b, x)
+    B.profile(True, dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ms, res = timed_steps(b, x)
+    clk = clocks.stop()
+    gs_ms, gs_launch, gs_rows = B.profile_read(B.PROF_GS_FULL, dev)
+    B.profile(False, dev)
+    gflop = metrics.hpcg_flops(npx * n, npy * n, npz * n, args.iters) * args.steps / 1e9
+    value = gflop / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        bh = b.cpu().pin_memory()
+        xh = torch.zeros(nrow, dtype=torch.float64).pin_memory()
+        step(bh, xh)
+        ems, _ = timed_steps(bh, xh)
+        e2e = {"value": round(gflop / (ems * 1e-3), 3), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": world * 2 * nrow * 8, "d2h_bytes_per_step": world * nrow * 8,
+               "ms_per_step": round(ems / args.steps, 3)}
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow)
+        achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"HPCG CG set over {world} ranks: {args.iters} preconditioned CG iterations, "
+                                   f"{n}^3 block per rank, 4 MG levels, 27-point stencil, 8-colour SYMGS, FP64",
+                       "grid": [npx * n, npy * n, npz * n], "local_grid": [n, n, n], "rows": world * nrow,
+                       "process_grid": [npx, npy, npz], "mg_levels": 4, "iters_per_step": args.iters,
+                       "parallelism": f"halo{world}: NCCL halo exchange + allreduce",
+                       "l2": "inputs larger than L2 (43 GB matrix per rank)", "setup_s": round(t_setup, 3)},
+            "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None, "traffic": None,
+                         "kernel": "k_gs_phase<double,double,false> (level 0, rank 0)",
+                         "peak_kind": peak_kind, "launches": gs_launch},
+            "gpu_launches": shard_launches_per_set(args.iters) * args.steps,
+            "clocks": clk,
+        }
+        if e2e:
+            line["e2e"] = e2e
+    C.free()
+    P.free()
+    dist.barrier()
+    dist.destroy_process_group()
+    if line:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -574,6 +690,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank)
+    if world > 1 and not args.replicas:
+        return shard_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)
 
 

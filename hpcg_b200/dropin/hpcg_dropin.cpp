@@ -15,6 +15,16 @@
 // every call takes its vectors from the host arrays, and the calls that use
 // the fine matrix first compare its diagonal with the copy last sent to the
 // device and resend it if the host changed it.
+//
+// MPI builds (HPCG_NO_MPI undefined) with more than one rank: each rank's block
+// and halo plan are generated on its GPU (hpcg_b200_generate_rank, the same
+// matrix GenerateProblem_ref + SetupHalo_ref built on the host), the ranks are
+// joined by a NCCL communicator whose id rank 0 broadcasts with MPI_Bcast, and
+// SPMV/SYMGS/MG/CG run as hpcg_b200_shard_* calls; dot products and the residual
+// keep the reference's local-result-plus-MPI_Allreduce structure.
+#ifndef HPCG_NO_MPI
+#include <mpi.h>
+#endif
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -40,6 +50,7 @@ namespace {
 // State the drop-in keeps per optimised matrix, reached through A.optimizationData.
 struct DropinState {
   hpcg_b200_problem* problem;
+  hpcg_b200_comm* comm;           // ranks of an MPI run (NULL on one rank)
   std::vector<double> diag_sent;  // fine diagonal as last sent to the device
 };
 
@@ -72,8 +83,53 @@ int sync_diagonal(const SparseMatrix& A, DropinState* st) {
 
 }  // namespace
 
+#ifndef HPCG_NO_MPI
+// One rank of an MPI run: the rank's hierarchy generated on its GPU, and the
+// NCCL communicator of all ranks.
+int optimize_rank(SparseMatrix& A, DropinState* st) {
+  const Geometry& g = *A.geom;
+  if (g.npartz != 1) return HPCG_B200_ERR_UNSUPPORTED;  // equal local blocks only
+  int nlevels = 0;
+  for (const SparseMatrix* m = &A; m; m = m->Ac) ++nlevels;
+  int device = device_index();
+  if (!std::getenv("HPCG_B200_DEVICE")) {  // one rank per GPU: the launcher's node-local rank
+    const char* local = std::getenv("OMPI_COMM_WORLD_LOCAL_RANK");
+    if (!local) local = std::getenv("MPI_LOCALRANKID");
+    if (!local) local = std::getenv("SLURM_LOCALID");
+    device = local ? std::atoi(local) : 0;
+  }
+  int s = hpcg_b200_generate_rank(g.nx, g.ny, g.nz, g.npx, g.npy, g.npz, g.rank, nlevels, device, &st->problem);
+  if (s) return s;
+  unsigned char id[HPCG_B200_COMM_ID_BYTES];
+  std::memset(id, 0, sizeof(id));
+  if (g.rank == 0) s = hpcg_b200_comm_unique_id(id);
+  MPI_Bcast(&s, 1, MPI_INT, 0, MPI_COMM_WORLD);
+  if (s) return s;
+  MPI_Bcast(id, (int)sizeof(id), MPI_CHAR, 0, MPI_COMM_WORLD);
+  return hpcg_b200_comm_nccl(id, g.size, g.rank, st->problem, &st->comm);
+}
+#endif
+
 int OptimizeProblem(SparseMatrix& A, CGData& data, Vector& b, Vector& x, Vector& xexact) {
   (void)data; (void)b; (void)x; (void)xexact;
+#ifndef HPCG_NO_MPI
+  if (A.geom->size > 1) {
+    DropinState* st = new DropinState;
+    st->problem = 0;
+    st->comm = 0;
+    const int status = optimize_rank(A, st);
+    if (status) {
+      log_error("OptimizeProblem", status);
+      if (st->problem) hpcg_b200_free(st->problem);
+      delete st;
+      return status;
+    }
+    st->diag_sent.resize(A.localNumberOfRows);
+    for (local_int_t i = 0; i < A.localNumberOfRows; ++i) st->diag_sent[i] = *A.matrixDiagonal[i];
+    A.optimizationData = st;
+    return 0;
+  }
+#endif
   std::vector<hpcg_b200_level_desc> levels;
   for (const SparseMatrix* m = &A; m; m = m->Ac) {
     hpcg_b200_level_desc d;
@@ -89,6 +145,7 @@ int OptimizeProblem(SparseMatrix& A, CGData& data, Vector& b, Vector& x, Vector&
     levels.push_back(d);
   }
   DropinState* st = new DropinState;
+  st->comm = 0;
   const int status = hpcg_b200_optimize(&levels[0], (int)levels.size(), device_index(), &st->problem);
   if (status) {
     log_error("OptimizeProblem", status);
@@ -110,7 +167,8 @@ int ComputeSPMV(const SparseMatrix& A, Vector& x, Vector& y) {
   DropinState* st = state_of(A);
   if (!st) return HPCG_B200_ERR_HANDLE;
   int s = sync_diagonal(A, st);
-  if (!s) s = hpcg_b200_spmv(st->problem, x.values, y.values);
+  if (!s) s = st->comm ? hpcg_b200_shard_spmv(st->comm, &x.values, &y.values)
+                       : hpcg_b200_spmv(st->problem, x.values, y.values);
   if (s) log_error("ComputeSPMV", s);
   return s;
 }
@@ -119,7 +177,8 @@ int ComputeSYMGS(const SparseMatrix& A, const Vector& r, Vector& x) {
   DropinState* st = state_of(A);
   if (!st) return HPCG_B200_ERR_HANDLE;
   int s = sync_diagonal(A, st);
-  if (!s) s = hpcg_b200_symgs(st->problem, r.values, x.values);
+  if (!s) s = st->comm ? hpcg_b200_shard_symgs(st->comm, &r.values, &x.values)
+                       : hpcg_b200_symgs(st->problem, r.values, x.values);
   if (s) log_error("ComputeSYMGS", s);
   return s;
 }
@@ -128,7 +187,8 @@ int ComputeMG(const SparseMatrix& A, const Vector& r, Vector& x) {
   DropinState* st = state_of(A);
   if (!st) return HPCG_B200_ERR_HANDLE;
   int s = sync_diagonal(A, st);
-  if (!s) s = hpcg_b200_mg(st->problem, r.values, x.values);
+  if (!s) s = st->comm ? hpcg_b200_shard_mg(st->comm, &r.values, &x.values)
+                       : hpcg_b200_mg(st->problem, r.values, x.values);
   if (s) log_error("ComputeMG", s);
   return s;
 }
@@ -136,9 +196,19 @@ int ComputeMG(const SparseMatrix& A, const Vector& r, Vector& x) {
 int ComputeDotProduct(const local_int_t n, const Vector& x, const Vector& y, double& result,
                       double& time_allreduce, bool& isOptimized) {
   (void)isOptimized;  // left true: this is the optimised version
-  time_allreduce += 0.0;  // one process: no allreduce
-  const int s = hpcg_b200_dot(n, x.values, y.values, &result);
+  double local = 0.0;
+  const int s = hpcg_b200_dot(n, x.values, y.values, &local);
   if (s) log_error("ComputeDotProduct", s);
+#ifndef HPCG_NO_MPI
+  const double t0 = MPI_Wtime();  // ComputeDotProduct_ref.cpp:66-73
+  double global = 0.0;
+  MPI_Allreduce(&local, &global, 1, MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
+  result = global;
+  time_allreduce += MPI_Wtime() - t0;
+#else
+  time_allreduce += 0.0;  // one process: no allreduce
+  result = local;
+#endif
   return s;
 }
 
@@ -151,8 +221,14 @@ int ComputeWAXPBY(const local_int_t n, const double alpha, const Vector& x, cons
 }
 
 int ComputeResidual(const local_int_t n, const Vector& v1, const Vector& v2, double& residual) {
-  const int s = hpcg_b200_residual(n, v1.values, v2.values, &residual);
+  double local = 0.0;
+  const int s = hpcg_b200_residual(n, v1.values, v2.values, &local);
   if (s) log_error("ComputeResidual", s);
+#ifndef HPCG_NO_MPI
+  MPI_Allreduce(&local, &residual, 1, MPI_DOUBLE, MPI_MAX, MPI_COMM_WORLD);  // ComputeResidual.cpp:79-83
+#else
+  residual = local;
+#endif
   return s;
 }
 
@@ -165,7 +241,10 @@ int CG(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const in
   if (!doPreconditioning && A.geom->rank == 0)
     HPCG_fout << "WARNING: PERFORMING UNPRECONDITIONED ITERATIONS" << std::endl;  // as src/CG.cpp:75
   int s = sync_diagonal(A, st);
-  if (!s)
+  if (!s && st->comm)
+    s = hpcg_b200_shard_cg(st->comm, &b.values, &x.values, max_iter, tolerance, doPreconditioning ? 1 : 0,
+                           &niters, &normr, &normr0, times);
+  else if (!s)
     s = hpcg_b200_cg(st->problem, b.values, x.values, max_iter, tolerance, doPreconditioning ? 1 : 0, &niters,
                      &normr, &normr0, times);
   if (s) log_error("CG", s);
