@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the 16-problem batched comparison")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1 GPUs: N independent problems instead of one decomposed problem")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="run the decomposed (halo + allreduce) arm even on one GPU (a one-rank grid)")
     return ap.parse_args()
 
 
@@ -593,6 +595,11 @@ def shard_arm(args, rank, world, local_rank):
 
     dev = local_rank
     torch.cuda.set_device(dev)
+    if world == 1:  # --decomposed on one GPU, without a launcher
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
     dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", dev))
     n = args.n
     nrow = n ** 3
@@ -690,7 +697,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank)
-    if world > 1 and not args.replicas:
+    if (world > 1 and not args.replicas) or args.decomposed:
         return shard_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)
 

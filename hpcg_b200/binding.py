@@ -324,7 +324,8 @@ class Problem:
         """Autotuner choices of a level: dict(gs, gs_first, gs32, spmv, spmv_order, tuned)."""
         out = np.zeros(6, np.int32)
         _check(lib().hpcg_b200_level_config(self._h, level, out.ctypes.data), "hpcg_b200_level_config")
-        return dict(zip(("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned"), (int(v) for v in out)))
+        keys = ("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned")
+        return dict(zip(keys, (int(v) for v in out)))
 
     def export_level(self, level):
         n, pitch, starts = self.level_info(level)

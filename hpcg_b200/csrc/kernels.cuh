@@ -125,6 +125,16 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
   }
 }
 
+// Storage row of the t-th row in slab order: z pair after z pair, inside a z
+// pair colour after colour (each one run of storage). Needs even grid dimensions.
+__device__ __forceinline__ int64_t slab_row(const ColourGrid& g, int64_t t) {
+  const int64_t per = (int64_t)(g.nx >> 1) * (g.ny >> 1);  // rows of one colour in one z pair
+  const int64_t h = t / (kColours * per);
+  const int64_t rem = t - h * kColours * per;
+  const int s = (int)(rem / per);
+  return g.start[s] + h * per + (rem - s * per);
+}
+
 // y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y
 // (the p'Ap of CG.cpp:119, fused).
 // ORDER 0: rows in storage order (colour block after colour block). Each colour
@@ -150,10 +160,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
         const int ix = t % g.nx, iy = (t / g.nx) % g.ny, iz = t / (g.nx * g.ny);
         q = g.old2new(ix, iy, iz);
       } else if (ORDER == 2) {
-        const int per = (g.nx >> 1) * (g.ny >> 1);  // rows of one colour in one z pair
-        const int h = t / (kColours * per), rem = t - h * (kColours * per);
-        const int s = rem / per;
-        q = g.start[s] + h * per + (rem - s * per);
+        q = (int)slab_row(g, t);
       }
       T sum = (T)0;
       T xq = (T)0;
@@ -186,12 +193,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
     const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
     for (int64_t t0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; t0 < n; t0 += stride) {
       int64_t q0 = t0;
-      if (ORDER == 2) {  // R rows of one run: per is a multiple of R (checked on the host)
-        const int per = (g.nx >> 1) * (g.ny >> 1);
-        const int64_t h = t0 / (kColours * (int64_t)per), rem = t0 - h * (kColours * (int64_t)per);
-        const int s = (int)(rem / per);
-        q0 = g.start[s] + h * per + (rem - (int64_t)s * per);
-      }
+      // R rows of one run: per is a multiple of R (checked on the host)
+      if (ORDER == 2) q0 = slab_row(g, t0);
       const int cnt = t0 + R <= n ? R : (int)(n - t0);
       if (cnt < R) {
         for (int q = (int)q0; q < n; ++q) {

@@ -265,52 +265,54 @@ int autotune(hpcg_b200_problem* P) {
     cudaEvent_t e0, e1;
     HB_CK(cudaEventCreate(&e0));
     HB_CK(cudaEventCreate(&e1));
+    // Repetitions run round-robin over the configurations, so that a drift of
+    // the clocks during tuning (the power cap settling) biases none of them.
+    const int kOrders = 3;  // SpMV row orders: storage, natural, slab
+    float t_gs[kConfigs], t_first[kConfigs], t_mv[kConfigs][kOrders];
+    for (int k = 0; k < kConfigs; ++k) {
+      t_gs[k] = t_first[k] = 1e30f;
+      for (int v = 0; v < kOrders; ++v) t_mv[k][v] = 1e30f;
+    }
+    auto time_it = [&](float& best, auto&& launch) -> int {
+      HB_CK(cudaEventRecord(e0, c->stream));
+      launch();
+      HB_CK(cudaEventRecord(e1, c->stream));
+      HB_CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) best = ms;
+      return HPCG_B200_OK;
+    };
+    const int keep_sched = L.mv_sched, keep_order = L.mv_order;
+    for (int rep = 0; rep < 4; ++rep) {
+      for (int sched = 0; sched < kConfigs; ++sched) {
+        HB_TRY(time_it(t_gs[sched], [&] {
+          gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
+        }));
+        // the first-sweep phase of a middle sweep position (about half its slots)
+        HB_TRY(time_it(t_first[sched], [&] {
+          gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, L.g.start[4], L.g.start[5], 4,
+                                            first_mask(L.g, 4));
+        }));
+        for (int v = 0; v < kOrders; ++v) {
+          L.mv_sched = sched;
+          L.mv_order = v;
+          // the variant CG runs: fused with the p'Ap partials
+          HB_TRY(time_it(t_mv[sched][v], [&] { spmv_dispatch<double, true>(c, L, L.val, xs, ys, c->partials); }));
+        }
+      }
+    }
+    L.mv_sched = keep_sched;
+    L.mv_order = keep_order;
     float best_gs = 1e30f, best_mv = 1e30f, best_first = 1e30f;
     for (int sched = 0; sched < kConfigs; ++sched) {
-      float t_gs = 1e30f, t_mv[3] = {1e30f, 1e30f, 1e30f};
-      for (int rep = 0; rep < 4; ++rep) {
-        HB_CK(cudaEventRecord(e0, c->stream));
-        gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
-        HB_CK(cudaEventRecord(e1, c->stream));
-        HB_CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-        t_gs = ms < t_gs ? ms : t_gs;
-        const int keep = L.mv_sched;
-        const int keep_order = L.mv_order;
-        for (int order = 0; order < 3; ++order) {
-          L.mv_sched = sched;
-          L.mv_order = order;
-          // the variant CG runs: fused with the p'Ap partials
-          HB_CK(cudaEventRecord(e0, c->stream));
-          spmv_dispatch<double, true>(c, L, L.val, xs, ys, c->partials);
-          HB_CK(cudaEventRecord(e1, c->stream));
-          HB_CK(cudaEventSynchronize(e1));
-          HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-          if (ms < t_mv[order]) t_mv[order] = ms;
-        }
-        L.mv_sched = keep;
-        L.mv_order = keep_order;
-      }
-      if (t_gs < best_gs) { best_gs = t_gs; L.gs_sched = sched; }
-      // the first-sweep phase of a middle sweep position (about half its slots)
-      float t_f = 1e30f;
-      for (int rep = 0; rep < 3; ++rep) {
-        const int f0 = L.g.start[4], f1 = L.g.start[5];
-        HB_CK(cudaEventRecord(e0, c->stream));
-        gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, f0, f1, 4, first_mask(L.g, 4));
-        HB_CK(cudaEventRecord(e1, c->stream));
-        HB_CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-        t_f = ms < t_f ? ms : t_f;
-      }
-      if (t_f < best_first) { best_first = t_f; L.gs_first = sched; }
-      for (int order = 0; order < 3; ++order)
-        if (t_mv[order] < best_mv) { best_mv = t_mv[order]; L.mv_sched = sched; L.mv_order = order; }
-      const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
-      if (fo && *fo) L.mv_order = std::atoi(fo);
+      if (t_gs[sched] < best_gs) { best_gs = t_gs[sched]; L.gs_sched = sched; }
+      if (t_first[sched] < best_first) { best_first = t_first[sched]; L.gs_first = sched; }
+      for (int v = 0; v < kOrders; ++v)
+        if (t_mv[sched][v] < best_mv) { best_mv = t_mv[sched][v]; L.mv_sched = sched; L.mv_order = v; }
     }
+    const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
+    if (fo && *fo) L.mv_order = std::atoi(fo);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     HB_CK(cudaGetLastError());
@@ -605,20 +607,22 @@ int ensure_f32(hpcg_b200_problem* P) {
       cudaEvent_t e0, e1;
       HB_CK(cudaEventCreate(&e0));
       HB_CK(cudaEventCreate(&e1));
-      float best = 1e30f;
-      for (int cfg = 0; cfg < kConfigs; ++cfg) {
-        float t = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {
+      float t[kConfigs];
+      for (int cfg = 0; cfg < kConfigs; ++cfg) t[cfg] = 1e30f;
+      for (int rep = 0; rep < 4; ++rep) {  // round-robin over the configurations, as in autotune
+        for (int cfg = 0; cfg < kConfigs; ++cfg) {
           HB_CK(cudaEventRecord(e0, c->stream));
           gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
           HB_CK(cudaEventRecord(e1, c->stream));
           HB_CK(cudaEventSynchronize(e1));
           float ms = 0.f;
           HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-          t = ms < t ? ms : t;
+          if (ms < t[cfg]) t[cfg] = ms;
         }
-        if (t < best) { best = t; L.gs_sched32 = cfg; }
       }
+      float best = 1e30f;
+      for (int cfg = 0; cfg < kConfigs; ++cfg)
+        if (t[cfg] < best) { best = t[cfg]; L.gs_sched32 = cfg; }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       HB_CK(cudaGetLastError());

@@ -143,6 +143,27 @@ def test_spmv_bitwise(oracle, case32):
     assert np.array_equal(y, P.b)
 
 
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_spmv_every_row_order_bitwise(oracle, binding, monkeypatch, order):
+    """Every row order of the SpMV (storage, natural, slab) computes the
+    reference's bits on a 32 x 24 x 48 grid; the CG's fused p'Ap variant runs in each."""
+    monkeypatch.setenv("HPCG_B200_SPMV_ORDER", str(order))
+    L = oracle.generate(32, 24, 48).levels
+    D = binding.Problem.generate(32, 24, 48)
+    try:
+        x = np.random.default_rng(order).standard_normal(L[0].n)
+        y = np.zeros_like(x)
+        D.ComputeSPMV(x, y)
+        assert D.level_config(0)["spmv_order"] == order
+        assert np.array_equal(y, oracle.spmv(L[0], x))
+        b = D.get_rhs()
+        x1 = np.zeros_like(b)
+        D.CG(b, x1, 3, 0.0)  # the fused p'Ap path in this order
+        assert np.all(np.isfinite(x1))
+    finally:
+        D.free()
+
+
 def test_spmv_matches_reference_golden(oracle, case16):
     P, D, _, _ = case16
     g = np.load(os.path.join(GOLD, "golden_16.npz"))
