@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--mixed-tol", type=float, default=1e-9)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 128^3 implicit-adjoint timing")
     ap.add_argument("--no-multi", action="store_true", help="skip the 256^3, 8 right-hand-side comparison")
+    ap.add_argument("--multi-n", type=int, default=256, help="grid side of the 8 right-hand-side comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the 16-problem batched comparison")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1 GPUs: N independent problems instead of one decomposed problem")
@@ -344,11 +345,14 @@ def batched(dev, count=16, tol=1e-9, max_iter=2000):
         bt.free()
 
 
-def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000):
+def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
     """Time to a relative residual `tol` from x = 0: FP64 PCG (hpcg_b200_cg) against
-    FP64 flexible PCG around the FP32 V-cycle (hpcg_b200_cg_mixed)."""
+    FP64 flexible PCG around the FP32 V-cycle (hpcg_b200_cg_mixed). Then
+    `profile_iters` more FP32 iterations with the launch profiler on give the
+    level-0 FP32 Gauss-Seidel phases' achieved bandwidth."""
     import torch
     from hpcg_b200 import binding as B
+    from hpcg_b200 import metrics
     n = b.numel()
     x64 = torch.zeros_like(b)
     (it64, nr64, nr064), t64 = timed(lib_stream, lambda: P.CG(b, x64, max_iter, tol, True))
@@ -359,10 +363,30 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000):
     P.ComputeSPMV(x32, ax)
     torch.cuda.synchronize()
     res = B.ComputeDotProduct(n, b - ax, b - ax) ** 0.5 / B.ComputeDotProduct(n, b, b) ** 0.5
+    dev = b.device.index or 0
+    B.profile(True, dev)
+    x32.zero_()
+    torch.cuda.synchronize()
+    P.CG_mixed(b, x32, profile_iters, 0.0)
+    fu_ms, fu_l, fu_rows = B.profile_read(B.PROF_GS32_FULL, dev)
+    fi_ms, fi_l, fi_rows = B.profile_read(B.PROF_GS32_FIRST, dev)
+    B.profile(False, dev)
+    peak, _ = measured_peak_hbm()
+    full_gbs = metrics.gs_phase_bytes(fu_rows, n, vb=4) / (fu_ms * 1e-3) / 1e9 if fu_ms else None
+    first_gbs = metrics.first_sweep_bytes(fi_rows, vb=4) / (fi_ms * 1e-3) / 1e9 if fi_ms else None
     return {"fp64": {"iters": it64, "seconds": round(t64, 3), "scaled_residual": nr64 / nr064},
             "fp32_vcycle": {"iters": it32, "seconds": round(t32, 3), "scaled_residual": nr32 / nr032,
                             "true_residual": res},
-            "time_ratio": round(t32 / t64, 4), "x_rel_diff_vs_fp64": err}
+            "time_ratio": round(t32 / t64, 4), "x_rel_diff_vs_fp64": err,
+            "fp32_level0_phases": {
+                "iters_profiled": profile_iters,
+                "full_ms_per_iter": round(fu_ms / profile_iters, 3),
+                "full_gbs": round(full_gbs, 1) if full_gbs else None,
+                "full_frac": round(full_gbs / peak, 4) if full_gbs else None,
+                "first_ms_per_iter": round(fi_ms / profile_iters, 3),
+                "first_gbs": round(first_gbs, 1) if first_gbs else None,
+                "bytes_per_row": {"full": 252, "first_sweep": 130}}}
+
 
 def gpu_launches_per_set(iters, nlevels=4):
     """Kernels the library launches for one CG call (its own kernels only)."""
@@ -501,7 +525,7 @@ def b200_arm(args, rank, world, local_rank):
         adjoint = adjoint_timing(dev)
     multi = None
     if not args.no_multi:
-        multi = multi_rhs(dev)
+        multi = multi_rhs(dev, n=args.multi_n)
     batch = None
     if not args.no_batch:
         batch = batched(dev)
@@ -539,6 +563,7 @@ def b200_arm(args, rank, world, local_rank):
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
             "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
                      "gbs": round((sp_rows * (27 * 12 + 8 + 8)) / (sp_ms * 1e-3) / 1e9, 1) if sp_ms else None},
+            "first_sweep_gbs": round(metrics.first_sweep_bytes(gf_rows) / (gf_ms * 1e-3) / 1e9, 1) if gf_ms else None,
             "kernel_ms_per_iter": {
                 "gs_full_l0": round(gs_ms / (args.iters * args.steps), 3),
                 "gs_first_l0": round(gf_ms / (args.iters * args.steps), 3),

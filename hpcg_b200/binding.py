@@ -41,7 +41,7 @@ EXPORTS = (
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
-    "hpcg_b200_last_error",
+    "hpcg_b200_mg_f32", "hpcg_b200_last_error",
 )
 
 
@@ -116,6 +116,7 @@ def lib():
             f.argtypes = [vp, vp, vp]
         l.hpcg_b200_shard_dot.argtypes = [vp, vp, vp, C.POINTER(d)]
         l.hpcg_b200_shard_cg.argtypes = [vp, vp, vp, i, d, i, C.POINTER(i), C.POINTER(d), C.POINTER(d), vp]
+        l.hpcg_b200_mg_f32.argtypes = [vp, vp, vp]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -284,6 +285,11 @@ class Problem:
         _check(lib().hpcg_b200_cg_mixed(self._h, _ptr(b, self.nrow), _ptr(x, self.nrow), max_iter, tolerance,
                                         C.byref(ni), C.byref(nr), C.byref(nr0)), "CG_mixed")
         return ni.value, nr.value, nr0.value
+
+    def ComputeMG_f32(self, r, x):
+        """x = widen(MG32(narrow(r))): the FP32 V-cycle of CG_mixed alone."""
+        _check(lib().hpcg_b200_mg_f32(self._h, _ptr(r, self.nrow), _ptr(x, self.nrow)), "hpcg_b200_mg_f32")
+        return 0
 
     def CG_multi(self, b, x, max_iter, tolerance):
         """nrhs = len(b) / nrow systems (b, x: [nrhs, nrow] contiguous float64).
@@ -498,7 +504,7 @@ class Batch:
             pass
 
 
-PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT = 0, 1, 2, 3
+PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT, PROF_GS32_FULL, PROF_GS32_FIRST = 0, 1, 2, 3, 4, 5
 
 
 def stream(device=0):

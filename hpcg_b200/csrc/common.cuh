@@ -209,7 +209,10 @@ int status_of(cudaError_t e);
   } while (0)
 
 // ---- per-device context ------------------------------------------------------
-constexpr int kRedBlocksMax = 4096;  // reduction partial slots
+constexpr int kRedBlocksMax = 16384;  // reduction partial slots
+// Partial slots per colour position of the Gauss-Seidel phases that also reduce
+// r'z (kColours * kDotStride <= kRedBlocksMax); a phase's grid is capped to it.
+constexpr int kDotStride = 2048;
 
 struct Scalars {
   double rtz, oldrtz, alpha, beta, pAp, normr2, rzprev, tmp;
@@ -238,7 +241,9 @@ enum ProfKind : int {
   kProfGsFirst = 1,  // first forward sweep on level 0 (x = 0, masked slots)
   kProfSpmv = 2,     // CG SpMV + p'Ap on level 0
   kProfRestrict = 3, // residual + restriction, level 0 -> 1
-  kProfKinds = 4,
+  kProfGs32Full = 4,   // FP32 V-cycle: Gauss-Seidel colour phase on level 0, all 27 slots
+  kProfGs32First = 5,  // FP32 V-cycle: first forward sweep on level 0
+  kProfKinds = 6,
 };
 
 struct Context {
@@ -254,9 +259,9 @@ struct Context {
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;                   // free events
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_open[kProfKinds];
-  double prof_ms[kProfKinds] = {0, 0, 0, 0};
-  long prof_launches[kProfKinds] = {0, 0, 0, 0};
-  int64_t prof_rows[kProfKinds] = {0, 0, 0, 0};      // rows processed by the timed launches
+  double prof_ms[kProfKinds] = {};
+  long prof_launches[kProfKinds] = {};
+  int64_t prof_rows[kProfKinds] = {};                 // rows processed by the timed launches
 };
 
 // Event pair around one launch of `kind` (no-op unless profiling); prof_end after the launch.

@@ -36,35 +36,102 @@ namespace hb {
 //  - the minimum resident 256-thread blocks per SM, which caps registers per
 //    thread (4 -> 64, 2 -> 128, 1 -> 255).
 
-constexpr int kConfigs = 7;
+//  - interleaved rows (Gauss-Seidel phases only, configurations 7 and 8): a
+//    thread updates R rows 32 apart, so every load of a warp is one coalesced
+//    run (no vector loads, no strided gathers) and each thread still has R
+//    independent rows' loads in flight.
+constexpr int kConfigs = 7;    // configurations of the SpMV and the restriction
+constexpr int kGsConfigs = 9;  // configurations of the Gauss-Seidel phases
 __host__ __device__ constexpr int cfg_sched(int cfg) { return cfg == 2 || cfg == 3 ? kStaged : kPlain; }
 __host__ __device__ constexpr int cfg_minb(int cfg) {
   return cfg == 0 || cfg == 4 ? 4 : cfg == 2 ? 1 : 2;
 }
-__host__ __device__ constexpr int cfg_rows(int cfg) { return cfg == 4 || cfg == 5 ? 2 : cfg == 6 ? 4 : 1; }
+__host__ __device__ constexpr int cfg_rows(int cfg) {
+  return cfg == 4 || cfg == 5 || cfg == 7 ? 2 : cfg == 6 || cfg == 8 ? 4 : 1;
+}
+__host__ __device__ constexpr bool cfg_interleaved(int cfg) { return cfg >= 7; }
 
 // Gauss-Seidel colour phase: rows [r0, r1) of one colour, updated in parallel
 // (no two rows of a colour are neighbours).
 // CMASK >= 0: the slot mask is that compile-time constant (the first sweep's
 // masks of the default sweep order), so unused slots drop out of the code;
 // CMASK < 0: the runtime `mask`.
+// DOT: the phase also writes block partials of sum_i rhs_i * x_i over its rows
+// (the new x) to dot[blockIdx.x]: run on the phases that write each colour's
+// final value, they give the CG's r'z without another pass over r and z.
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1, int SCHED = cfg_sched(CFG),
-          int R = cfg_rows(CFG)>
+          int R = cfg_rows(CFG), bool DOT = false>
 __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* __restrict__ val,
                                                                       const int* __restrict__ col, int64_t pitch,
                                                                       const TR* __restrict__ rhs, T* x, int r0,
-                                                                      int r1, uint32_t mask_arg) {
+                                                                      int r1, uint32_t mask_arg,
+                                                                      double* __restrict__ dot) {
   const uint32_t mask = CMASK >= 0 ? (uint32_t)CMASK : mask_arg;
+  double acc = 0.0;
+  if (cfg_interleaved(CFG)) {
+    // tiles of blockDim.x * R rows; warp w takes 32 * R of them, lane l rows l + 32 r
+    const int64_t tile = (int64_t)blockDim.x * R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t b0 = r0 + (int64_t)blockIdx.x * tile; b0 < r1; b0 += (int64_t)gridDim.x * tile) {
+      const int64_t q0 = b0 + (int64_t)warp * 32 * R + lane;
+      T sum[R], xd[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        sum[r] = q0 + 32 * r < r1 ? (T)rhs[q0 + 32 * r] : (T)0;
+        xd[r] = (T)0;
+      }
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        if (mask & (1u << k)) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int64_t q = q0 + 32 * r;
+            if (q < r1) {
+              const T a = val[k * pitch + q];
+              const T xv = __ldg(x + col[k * pitch + q]);
+              sum[r] -= a * xv;
+              if (k == kDiagSlot) xd[r] = xv;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t q = q0 + 32 * r;
+        if (q < r1) {
+          const T d = val[kDiagSlot * pitch + q];
+          if (!FIRST) sum[r] += xd[r] * d;
+          const T out = sum[r] / d;
+          x[q] = out;
+          if (DOT) acc += (double)rhs[q] * (double)out;
+        }
+      }
+    }
+    if (DOT) {
+      const double s = block_sum(acc);
+      if (threadIdx.x == 0) dot[blockIdx.x] = s;
+    }
+    return;
+  }
   if (R == 1) {
     const int stride = gridDim.x * blockDim.x;
-    for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride)
-      gs_row<T, TR, FIRST, SCHED>(val, col, pitch, rhs, x, q, mask);
+    for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride) {
+      const T out = gs_row<T, TR, FIRST, SCHED>(val, col, pitch, rhs, x, q, mask);
+      if (DOT) acc += (double)rhs[q] * (double)out;
+    }
+    if (DOT) {
+      const double s = block_sum(acc);
+      if (threadIdx.x == 0) dot[blockIdx.x] = s;
+    }
     return;
   }
   const int64_t stride = (int64_t)gridDim.x * blockDim.x * R;
   for (int64_t q0 = r0 + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * R; q0 < r1; q0 += stride) {
     if (q0 + R > r1) {
-      for (int q = (int)q0; q < r1; ++q) gs_row<T, TR, FIRST, kPlain>(val, col, pitch, rhs, x, q, mask);
+      for (int q = (int)q0; q < r1; ++q) {
+        const T out = gs_row<T, TR, FIRST, kPlain>(val, col, pitch, rhs, x, q, mask);
+        if (DOT) acc += (double)rhs[q] * (double)out;
+      }
       continue;
     }
     TR rv[R];
@@ -96,8 +163,13 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
     for (int r = 0; r < R; ++r) {
       if (!FIRST) sum[r] += xd[r] * d[r];
       out[r] = sum[r] / d[r];
+      if (DOT) acc += (double)rv[r] * (double)out[r];
     }
     store_vec<T, R>(x + q0, out);
+  }
+  if (DOT) {
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) dot[blockIdx.x] = s;
   }
 }
 
@@ -334,6 +406,32 @@ __global__ void __launch_bounds__(kThreads) k_dot(int n, const double* __restric
   }
 }
 
+// Flexible-CG step of the mixed form: z = widen(x32) together with the partials
+// of r'z (and of r'zprev for TWO) in k_dot<TWO>'s layout and order, so the
+// conversion pass and the copy of z into zprev go away (z and zprev are two
+// buffers whose roles alternate).
+template <bool TWO>
+__global__ void __launch_bounds__(kThreads) k_widen_dot(int n, const float* __restrict__ x32,
+                                                        const double* __restrict__ r, double* __restrict__ z,
+                                                        const double* __restrict__ zprev,
+                                                        double* __restrict__ partials) {
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0, acc2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double zi = (double)x32[i];
+    z[i] = zi;
+    const double ri = r[i];
+    acc += ri * zi;
+    if (TWO) acc2 += ri * zprev[i];
+  }
+  const double s = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (TWO) {
+    const double s2 = block_sum(acc2);
+    if (threadIdx.x == 0) partials[gridDim.x + blockIdx.x] = s2;
+  }
+}
+
 // partial maxima of |v1 - v2| (ComputeResidual.cpp:70-75)
 __global__ void __launch_bounds__(kThreads) k_maxdiff(int n, const double* __restrict__ a,
                                                       const double* __restrict__ b, double* __restrict__ partials) {
@@ -440,9 +538,10 @@ __global__ void k_cg_setup(Scalars* s, int max_iter, double tol) {
 }
 
 // x = x + alpha p; r = r + (-alpha) Ap (CG.cpp:121-122); partials of r'r (CG.cpp:123).
+// r32 (the mixed form): also r narrowed to FP32 for the next V-cycle.
 __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const double* __restrict__ p, double* r,
                                                         const double* __restrict__ Ap, const Scalars* __restrict__ s,
-                                                        double* __restrict__ partials) {
+                                                        double* __restrict__ partials, float* __restrict__ r32 = nullptr) {
   const double alpha = s->alpha, malpha = -s->alpha;
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
@@ -450,6 +549,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const 
     x[i] = x[i] + alpha * p[i];
     const double ri = r[i] + malpha * Ap[i];
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   const double sum = block_sum(acc);

@@ -42,104 +42,121 @@ __device__ __forceinline__ void store_k(double* __restrict__ p, const double (&v
 }
 
 // Gauss-Seidel colour phase for K systems (ComputeSYMGS_ref.cpp:72-80 per system).
-template <int K, bool FIRST>
+// LANES threads share a row, each with S = K/LANES of its systems: every lane
+// re-reads the row's values and columns (one transaction for the lanes of a
+// row) and gathers S-entry runs of x. More lanes, fewer registers per thread
+// and more rows' loads in flight per SM.
+template <int K, int LANES, bool FIRST>
 __global__ void __launch_bounds__(kThreads) k_gs_phase_m(const double* __restrict__ val, const int* __restrict__ col,
                                                          int64_t pitch, const double* __restrict__ rhs, double* x,
                                                          int r0, int r1, uint32_t mask) {
-  const int stride = gridDim.x * blockDim.x;
-  for (int q = r0 + blockIdx.x * blockDim.x + threadIdx.x; q < r1; q += stride) {
-    double sum[K], xd[K];
-    load_k<K>(rhs + (int64_t)q * K, sum);
+  constexpr int S = K / LANES;
+  const int64_t work = (int64_t)(r1 - r0) * LANES;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < work; t += stride) {
+    const int q = r0 + (int)(t / LANES);
+    const int off = (int)(t % LANES) * S;
+    double sum[S], xd[S];
+    load_k<S>(rhs + (int64_t)q * K + off, sum);
 #pragma unroll
-    for (int j = 0; j < K; ++j) xd[j] = 0.0;
+    for (int j = 0; j < S; ++j) xd[j] = 0.0;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       if (mask & (1u << k)) {
         const double a = val[k * pitch + q];
-        double xv[K];
-        load_k<K>(x + (int64_t)col[k * pitch + q] * K, xv);
+        double xv[S];
+        load_k<S>(x + (int64_t)col[k * pitch + q] * K + off, xv);
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
+        for (int j = 0; j < S; ++j) {
           sum[j] -= a * xv[j];
           if (k == kDiagSlot) xd[j] = xv[j];
         }
       }
     }
     const double d = val[kDiagSlot * pitch + q];
-    double out[K];
+    double out[S];
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
+    for (int j = 0; j < S; ++j) {
       if (!FIRST) sum[j] += xd[j] * d;
       out[j] = sum[j] / d;
     }
-    store_k<K>(x + (int64_t)q * K, out);
+    store_k<S>(x + (int64_t)q * K + off, out);
   }
 }
 
 // y = A x for K systems; DOT: partials of x_j'y_j at partials[j*gridDim.x + block].
-template <int K, bool DOT>
+// LANES as in k_gs_phase_m.
+template <int K, int LANES, bool DOT>
 __global__ void __launch_bounds__(kThreads) k_spmv_m(const double* __restrict__ val, const int* __restrict__ col,
                                                      int64_t pitch, const double* __restrict__ x,
                                                      double* __restrict__ y, int n, double* __restrict__ partials) {
-  const int stride = gridDim.x * blockDim.x;
-  double acc[K];
+  constexpr int S = K / LANES;
+  const int64_t work = (int64_t)n * LANES;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int off = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) % LANES) * S;  // stride % LANES == 0
+  double acc[S];
 #pragma unroll
-  for (int j = 0; j < K; ++j) acc[j] = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
-    double sum[K], xq[K];
+  for (int j = 0; j < S; ++j) acc[j] = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < work; t += stride) {
+    const int q = (int)(t / LANES);
+    double sum[S], xq[S];
 #pragma unroll
-    for (int j = 0; j < K; ++j) sum[j] = xq[j] = 0.0;
+    for (int j = 0; j < S; ++j) sum[j] = xq[j] = 0.0;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       const double a = val[k * pitch + q];
-      double xv[K];
-      load_k<K>(x + (int64_t)col[k * pitch + q] * K, xv);
+      double xv[S];
+      load_k<S>(x + (int64_t)col[k * pitch + q] * K + off, xv);
 #pragma unroll
-      for (int j = 0; j < K; ++j) {
+      for (int j = 0; j < S; ++j) {
         sum[j] += a * xv[j];
         if (k == kDiagSlot) xq[j] = xv[j];
       }
     }
-    store_k<K>(y + (int64_t)q * K, sum);
+    store_k<S>(y + (int64_t)q * K + off, sum);
     if (DOT) {
 #pragma unroll
-      for (int j = 0; j < K; ++j) acc[j] += xq[j] * sum[j];
+      for (int j = 0; j < S; ++j) acc[j] += xq[j] * sum[j];
     }
   }
   if (DOT) {
 #pragma unroll
     for (int j = 0; j < K; ++j) {
-      const double s = block_sum(acc[j]);
+      const double s = block_sum(off == (j / S) * S ? acc[j % S] : 0.0);
       if (threadIdx.x == 0) partials[j * gridDim.x + blockIdx.x] = s;
     }
   }
 }
 
-// rc = (rf - A xf) at the injected rows (sorted transfer pairs), K systems.
-template <int K>
+// rc = (rf - A xf) at the injected rows (sorted transfer pairs), K systems; LANES as in k_gs_phase_m.
+template <int K, int LANES>
 __global__ void __launch_bounds__(kThreads) k_restrict_m(const double* __restrict__ val, const int* __restrict__ col,
                                                          int64_t pitch, const double* __restrict__ rf,
                                                          const double* __restrict__ xf, const int* __restrict__ tf,
                                                          const int* __restrict__ tq, double* __restrict__ rc, int nc) {
-  const int stride = gridDim.x * blockDim.x;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += stride) {
+  constexpr int S = K / LANES;
+  const int64_t work = (int64_t)nc * LANES;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < work; w += stride) {
+    const int t = (int)(w / LANES);
+    const int off = (int)(w % LANES) * S;
     const int f = tf[t];
-    double sum[K];
+    double sum[S];
 #pragma unroll
-    for (int j = 0; j < K; ++j) sum[j] = 0.0;
+    for (int j = 0; j < S; ++j) sum[j] = 0.0;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       const double a = val[k * pitch + f];
-      double xv[K];
-      load_k<K>(xf + (int64_t)col[k * pitch + f] * K, xv);
+      double xv[S];
+      load_k<S>(xf + (int64_t)col[k * pitch + f] * K + off, xv);
 #pragma unroll
-      for (int j = 0; j < K; ++j) sum[j] += a * xv[j];
+      for (int j = 0; j < S; ++j) sum[j] += a * xv[j];
     }
-    double r[K], out[K];
-    load_k<K>(rf + (int64_t)f * K, r);
+    double r[S], out[S];
+    load_k<S>(rf + (int64_t)f * K + off, r);
 #pragma unroll
-    for (int j = 0; j < K; ++j) out[j] = r[j] - sum[j];
-    store_k<K>(rc + (int64_t)tq[t] * K, out);
+    for (int j = 0; j < S; ++j) out[j] = r[j] - sum[j];
+    store_k<S>(rc + (int64_t)tq[t] * K + off, out);
   }
 }
 

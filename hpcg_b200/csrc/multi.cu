@@ -2,6 +2,7 @@
 // K systems with the same matrix advance in lockstep through the kernels of
 // kernels_multi.cuh; each matrix row is read once per sweep for all K.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "kernels_multi.cuh"
@@ -13,6 +14,7 @@ void release_accounted(size_t bytes);
 // Work vectors of the multi-system path, interleaved [row][K], per level.
 struct MultiState {
   int K = 0;
+  int lanes = 1;  // threads per row of the matrix kernels (K/lanes systems each), tuned on creation
   double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
   double* lr[kMaxLevels] = {nullptr};  // coarse right-hand sides (levels > 0)
   double* lx[kMaxLevels] = {nullptr};  // coarse solutions (levels > 0)
@@ -47,6 +49,63 @@ int alloc_z(MultiState* m, double** p, size_t count, cudaStream_t st) {
   return HPCG_B200_OK;
 }
 
+template <int K, int LANES>
+int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first);
+
+// One symmetric sweep of level 0 with LANES threads per row.
+template <int K, int LANES>
+int time_sweep(Context* c, const Level& L, MultiState* m, cudaEvent_t e0, cudaEvent_t e1, float* best) {
+  HB_CK(cudaEventRecord(e0, c->stream));
+  HB_TRY((gs_colour_m<K, LANES>(c, L, m->r, m->x, false)));
+  HB_CK(cudaEventRecord(e1, c->stream));
+  HB_CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+  if (ms < *best) *best = ms;
+  return HPCG_B200_OK;
+}
+
+// Threads per row of the matrix kernels: the fastest symmetric sweep on level 0
+// (round-robin repetitions), or HPCG_B200_MULTI_LANES. Same bits either way.
+int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
+  const int K = m->K;
+  const char* force = std::getenv("HPCG_B200_MULTI_LANES");
+  if (force && *force) {
+    const int f = std::atoi(force);
+    m->lanes = f >= 4 && K >= 8 ? 4 : f >= 2 && K >= 4 ? 2 : 1;
+    return HPCG_B200_OK;
+  }
+  const Level& L = P->lev[0];
+  Context* c = P->ctx;
+  cudaEvent_t e0, e1;
+  HB_CK(cudaEventCreate(&e0));
+  HB_CK(cudaEventCreate(&e1));
+  float t[3] = {1e30f, 1e30f, 1e30f};  // lanes 1, 2, 4
+  int st = HPCG_B200_OK;
+  for (int rep = 0; rep < 3 && st == HPCG_B200_OK; ++rep) {
+    if (K == 2) st = time_sweep<2, 1>(c, L, m, e0, e1, &t[0]);
+    if (K == 4) {
+      st = time_sweep<4, 1>(c, L, m, e0, e1, &t[0]);
+      if (!st) st = time_sweep<4, 2>(c, L, m, e0, e1, &t[1]);
+    }
+    if (K == 8) {
+      st = time_sweep<8, 1>(c, L, m, e0, e1, &t[0]);
+      if (!st) st = time_sweep<8, 2>(c, L, m, e0, e1, &t[1]);
+      if (!st) st = time_sweep<8, 4>(c, L, m, e0, e1, &t[2]);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  HB_TRY(st);
+  int best = 0;
+  for (int i = 1; i < 3; ++i)
+    if (t[i] < t[best]) best = i;
+  m->lanes = 1 << best;
+  // the timed phases wrote m->x: every solve loads its own x, every V-cycle starts from zero
+  HB_CK(cudaMemsetAsync(m->x, 0, sizeof(double) * (size_t)P->lev[0].pitch * K, c->stream));
+  return HPCG_B200_OK;
+}
+
 // The state for K systems (re-created when K changes). Vectors are zeroed, so
 // the zero row n of every level (padded stencil slots) reads 0 for all K.
 int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
@@ -70,53 +129,56 @@ int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
   HB_TRY(dev_alloc((void**)&m->s, sizeof(MScalars), &m->bytes));
   HB_CK(cudaMemsetAsync(m->s, 0, sizeof(MScalars), st));
   HB_CK(cudaMallocHost(&m->s_host, sizeof(MScalars)));
+  HB_TRY(tune_lanes(P, m));
   *out = m;
   return HPCG_B200_OK;
 }
 
-template <int K>
+template <int K, int LANES>
 int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first) {
   int last = -1;
   for (int s = 0; s < kColours; ++s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
     last = s;
+    const int64_t work = (int64_t)(r1 - r0) * LANES;
     if (first) {
-      auto k = k_gs_phase_m<K, true>;
-      k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1,
-                                                              first_mask(L.g, s));
+      auto k = k_gs_phase_m<K, LANES, true>;
+      k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, first_mask(L.g, s));
     } else {
-      auto k = k_gs_phase_m<K, false>;
-      k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+      auto k = k_gs_phase_m<K, LANES, false>;
+      k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
     }
   }
   // backward sweep, without repeating the last colour (as the single-system path)
   for (int s = last - 1; s >= 0; --s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
-    auto k = k_gs_phase_m<K, false>;
-    k<<<grid_of(c, k, r1 - r0), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
+    auto k = k_gs_phase_m<K, LANES, false>;
+    k<<<grid_of(c, k, (int64_t)(r1 - r0) * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1,
+                                                                               kAllSlots);
   }
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
 }
 
 // ComputeMG_ref.cpp:39-63 for K systems on level l (colour order, interleaved).
-template <int K>
+template <int K, int LANES>
 int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x) {
   const Level& L = P->lev[l];
   Context* c = P->ctx;
-  HB_TRY(gs_colour_m<K>(c, L, r, x, true));
+  HB_TRY((gs_colour_m<K, LANES>(c, L, r, x, true)));
   if (l + 1 < P->nlev) {
     const Level& C = P->lev[l + 1];
-    auto kr = k_restrict_m<K>;
-    kr<<<grid_of(c, kr, C.n), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x, L.tf, L.tq, m->lr[l + 1], C.n);
+    auto kr = k_restrict_m<K, LANES>;
+    kr<<<grid_of(c, kr, (int64_t)C.n * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x, L.tf, L.tq,
+                                                                          m->lr[l + 1], C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY(mg_m<K>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1]));
+    HB_TRY((mg_m<K, LANES>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1])));
     auto kp = k_prolong_m<K>;
     kp<<<grid_of(c, kp, C.n), kThreads, 0, c->stream>>>(L.tf, L.tq, m->lx[l + 1], x, C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY(gs_colour_m<K>(c, L, r, x, false));
+    HB_TRY((gs_colour_m<K, LANES>(c, L, r, x, false)));
   }
   return HPCG_B200_OK;
 }
@@ -180,13 +242,13 @@ int finalize_m(Context* c, MultiState* m, int op, int iter, double tol) {
 // CG.cpp:59-143 for K systems in lockstep; a system stops updating once its
 // scaled residual is at or below the tolerance; the loop ends when none is left
 // or after max_iter iterations.
-template <int K>
+template <int K, int LANES>
 int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any_iters) {
   const Level& L = P->lev[0];
   Context* c = P->ctx;
   const int n = L.n;
-  auto ks = k_spmv_m<K, false>;
-  ks<<<grid_of(c, ks, n), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->x, m->Ap, n, nullptr);
+  auto ks = k_spmv_m<K, LANES, false>;
+  ks<<<grid_of(c, ks, (int64_t)n * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->x, m->Ap, n, nullptr);
   k_resid_m<K><<<kParts, kThreads, 0, c->stream>>>(m->b, m->Ap, m->r, n, m->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize_m<K>(c, m, kMNorm0, 0, tol));
@@ -197,7 +259,7 @@ int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any
     bool any = false;
     for (int j = 0; j < K; ++j) any = any || m->s_host->active[j];
     if (!any) break;
-    HB_TRY(mg_m<K>(P, m, 0, m->r, m->z));
+    HB_TRY((mg_m<K, LANES>(P, m, 0, m->r, m->z)));
     k_dot_m<K><<<kParts, kThreads, 0, c->stream>>>(m->r, m->z, n, m->partials);
     HB_CK(cudaGetLastError());
     if (k == 1) {
@@ -208,7 +270,7 @@ int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any
       k_update_p_m<K><<<kParts, kThreads, 0, c->stream>>>(m->z, m->p, n, m->s);
       HB_CK(cudaGetLastError());
     }
-    k_spmv_m<K, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, n, m->partials);
+    k_spmv_m<K, LANES, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, n, m->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize_m<K>(c, m, kMPap, k, tol));
     k_update_xr_m<K><<<kParts, kThreads, 0, c->stream>>>(m->x, m->p, m->r, m->Ap, n, m->s, m->partials);
@@ -229,7 +291,13 @@ int run_cg_multi(hpcg_b200_problem* P, int nrhs, const double* b, double* x, int
   HB_TRY(load_m<K>(P, m, nrhs, b, m->b));
   HB_TRY(load_m<K>(P, m, nrhs, x, m->x));
   int done = 0;
-  HB_TRY(cg_m<K>(P, m, max_iter, tol, &done));
+  if (m->lanes == 4) {
+    if constexpr (K >= 8) HB_TRY((cg_m<K, 4>(P, m, max_iter, tol, &done)));
+  } else if (m->lanes == 2) {
+    if constexpr (K >= 4) HB_TRY((cg_m<K, 2>(P, m, max_iter, tol, &done)));
+  } else {
+    HB_TRY((cg_m<K, 1>(P, m, max_iter, tol, &done)));
+  }
   HB_TRY(store_m<K>(P, m, nrhs, m->x, x));
   for (int j = 0; j < nrhs; ++j) {
     niters[j] = m->s_host->niters[j];
@@ -244,7 +312,13 @@ int run_mg_multi(hpcg_b200_problem* P, int nrhs, const double* r, double* x) {
   MultiState* m = nullptr;
   HB_TRY(ensure_state(P, K, &m));
   HB_TRY(load_m<K>(P, m, nrhs, r, m->r));
-  HB_TRY(mg_m<K>(P, m, 0, m->r, m->z));
+  if (m->lanes == 4) {
+    if constexpr (K >= 8) HB_TRY((mg_m<K, 4>(P, m, 0, m->r, m->z)));
+  } else if (m->lanes == 2) {
+    if constexpr (K >= 4) HB_TRY((mg_m<K, 2>(P, m, 0, m->r, m->z)));
+  } else {
+    HB_TRY((mg_m<K, 1>(P, m, 0, m->r, m->z)));
+  }
   return store_m<K>(P, m, nrhs, m->z, x);
 }
 

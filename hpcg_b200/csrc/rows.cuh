@@ -11,9 +11,10 @@ enum LoadSchedule : int { kPlain = 0, kStaged = 1 };
 // One Gauss-Seidel row update, ComputeSYMGS_ref.cpp:72-80: sum = r_i - sum_j a_ij x_j
 // (diagonal included, slot order), sum += x_i a_ii, x_i = sum / a_ii. FIRST: x
 // enters as zero; the masked-out slots (and the diagonal) multiply a zero.
+// Returns the new x_i.
 template <typename T, typename TR, bool FIRST, int SCHED>
-__device__ __forceinline__ void gs_row(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
-                                       const TR* __restrict__ rhs, T* x, int q, uint32_t mask) {
+__device__ __forceinline__ T gs_row(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                                    const TR* __restrict__ rhs, T* x, int q, uint32_t mask) {
   T sum = (T)rhs[q];
   T xd = (T)0;
   if (SCHED == kStaged) {
@@ -50,7 +51,9 @@ __device__ __forceinline__ void gs_row(const T* __restrict__ val, const int* __r
   }
   const T d = val[kDiagSlot * pitch + q];
   if (!FIRST) sum += xd * d;
-  x[q] = sum / d;
+  const T out = sum / d;
+  x[q] = out;
+  return out;
 }
 
 }  // namespace hb

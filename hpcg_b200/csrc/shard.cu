@@ -170,7 +170,9 @@ int read_scal(Context* c) {
 }
 
 // ComputeMG_ref.cpp:39-63 on every driven rank, colour-order vectors of level l.
-int mg_ranks(Comm* C, int l, double* const* r, double* const* x) {
+// rtz (level 0): each rank's post-smoother also leaves its r'z in red[i], as the
+// single-rank CG takes it from the smoother.
+int mg_ranks(Comm* C, int l, double* const* r, double* const* x, bool rtz = false) {
   Context* c = C->ctx;
   const int nl = (int)C->ranks.size();
   std::vector<double*> xc(nl), rc(nl);
@@ -193,7 +195,15 @@ int mg_ranks(Comm* C, int l, double* const* r, double* const* x) {
   HB_TRY(mg_ranks(C, l + 1, rc.data(), xc.data()));
   for (int i = 0; i < nl; ++i) HB_TRY(prolong_level(C->ranks[i], l, xc[i], x[i]));
   HB_TRY(exchange(C, l, x));  // ComputeSYMGS_ref.cpp:59
-  for (int i = 0; i < nl; ++i) HB_TRY(symgs_step(C->ranks[i], l, r[i], x[i], false));
+  for (int i = 0; i < nl; ++i) {
+    if (rtz) {
+      HB_CK(cudaMemsetAsync(c->partials, 0, sizeof(double) * kColours * kDotStride, c->stream));
+      HB_TRY(symgs_step(C->ranks[i], l, r[i], x[i], false, c->partials));
+      HB_TRY(store_partial(C, i, kColours * kDotStride));
+    } else {
+      HB_TRY(symgs_step(C->ranks[i], l, r[i], x[i], false));
+    }
+  }
   return HPCG_B200_OK;
 }
 
@@ -230,16 +240,18 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
   double normr = std::sqrt(c->scal_host->normr2);
   const double normr0 = normr;
   *niters = 0;
+  const bool fused = prec && rtz_from_smoother(C->ranks[0]);
   for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
     if (prec) {
-      HB_TRY(mg_ranks(C, 0, rs.data(), zs.data()));  // CG.cpp:103
+      HB_TRY(mg_ranks(C, 0, rs.data(), zs.data(), fused));  // CG.cpp:103
     } else {
       for (int i = 0; i < nl; ++i)
         HB_CK(cudaMemcpyAsync(zs[i], rs[i], sizeof(double) * C->ranks[i]->lev[0].n, cudaMemcpyDeviceToDevice,
                               c->stream));
     }
-    for (int i = 0; i < nl; ++i) {  // rtz = r'z   (:110 / :113)
-      HB_TRY(store_partial(C, i, launch_dot(c, C->ranks[i]->lev[0].n, rs[i], zs[i])));
+    if (!fused) {
+      for (int i = 0; i < nl; ++i)  // rtz = r'z   (:110 / :113)
+        HB_TRY(store_partial(C, i, launch_dot(c, C->ranks[i]->lev[0].n, rs[i], zs[i])));
     }
     HB_TRY(reduce(C, k == 1 ? kFinRtzFirst : kFinRtz));
     for (int i = 0; i < nl; ++i) {

@@ -43,8 +43,12 @@ int spmv_level(hpcg_b200_problem* p, int l, const double* x, double* y, bool dot
 int restrict_level(hpcg_b200_problem* p, int l, const double* rf, const double* xf, double* rc);
 // xf += xc at the injected rows (ComputeProlongation_ref.cpp:49)
 int prolong_level(hpcg_b200_problem* p, int l, const double* xc, double* xf);
-// one symmetric Gauss-Seidel step of level l, in the problem's mode
-int symgs_step(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero);
+// one symmetric Gauss-Seidel step of level l, in the problem's mode; dot (colour
+// mode, x entering nonzero): r'x block partials of the final writes at
+// dot[0 .. kColours * kDotStride), which the caller zeroes first
+int symgs_step(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero, double* dot = nullptr);
+// true when the CG takes r'z from the post-smoother (colour mode, two or more levels)
+bool rtz_from_smoother(const hpcg_b200_problem* p);
 // grid of the reductions over n rows (number of partials)
 int reduction_blocks(const Context* c, int64_t n);
 

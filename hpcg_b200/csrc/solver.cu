@@ -19,28 +19,45 @@ inline int red_blocks(const Context* c, int64_t n) {
   return b > kRedBlocksMax / 2 ? kRedBlocksMax / 2 : b;
 }
 
+// dot != nullptr: the phase also writes its r'z block partials there (FP64
+// full-slot phases only; the grid is capped at kDotStride blocks).
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1>
-void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask) {
-  auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK>;
+void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
+               double* dot = nullptr) {
   const int64_t units = ((int64_t)(r1 - r0) + cfg_rows(CFG) - 1) / cfg_rows(CFG);
-  k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask);
+  if constexpr (!FIRST && CMASK < 0 && sizeof(T) == 8) {
+    if (dot) {
+      auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK, cfg_sched(CFG), cfg_rows(CFG), true>;
+      int g = grid_of(c, k, units);
+      if (g > kDotStride) g = kDotStride;
+      k<<<g, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, dot);
+      return;
+    }
+  }
+  auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK>;
+  k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, nullptr);
 }
 
-// A configuration with R rows per thread needs the row range to start on a
-// multiple of R (vector loads); otherwise the scalar configuration 1 runs.
-inline int usable_cfg(int cfg, int r0) { return r0 % cfg_rows(cfg) == 0 ? cfg : 1; }
+// A configuration with R contiguous rows per thread needs the row range to start
+// on a multiple of R (vector loads); otherwise the scalar configuration 1 runs.
+// Interleaved rows need no alignment.
+inline int usable_cfg(int cfg, int r0) {
+  return cfg_interleaved(cfg) || r0 % cfg_rows(cfg) == 0 ? cfg : 1;
+}
 
 template <typename T, typename TR, bool FIRST>
 void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rhs, T* x, int r0, int r1,
-                 uint32_t mask) {
+                 uint32_t mask, double* dot = nullptr) {
   switch (usable_cfg(cfg, r0)) {
-    case 0: gs_launch<T, TR, FIRST, 0>(c, L, val, rhs, x, r0, r1, mask); break;
-    case 1: gs_launch<T, TR, FIRST, 1>(c, L, val, rhs, x, r0, r1, mask); break;
-    case 2: gs_launch<T, TR, FIRST, 2>(c, L, val, rhs, x, r0, r1, mask); break;
-    case 3: gs_launch<T, TR, FIRST, 3>(c, L, val, rhs, x, r0, r1, mask); break;
-    case 4: gs_launch<T, TR, FIRST, 4>(c, L, val, rhs, x, r0, r1, mask); break;
-    case 5: gs_launch<T, TR, FIRST, 5>(c, L, val, rhs, x, r0, r1, mask); break;
-    default: gs_launch<T, TR, FIRST, 6>(c, L, val, rhs, x, r0, r1, mask); break;
+    case 0: gs_launch<T, TR, FIRST, 0>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 1: gs_launch<T, TR, FIRST, 1>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 2: gs_launch<T, TR, FIRST, 2>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 3: gs_launch<T, TR, FIRST, 3>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 4: gs_launch<T, TR, FIRST, 4>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 5: gs_launch<T, TR, FIRST, 5>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 6: gs_launch<T, TR, FIRST, 6>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 7: gs_launch<T, TR, FIRST, 7>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    default: gs_launch<T, TR, FIRST, 8>(c, L, val, rhs, x, r0, r1, mask, dot); break;
   }
 }
 
@@ -68,12 +85,14 @@ void gs_first_dispatch(Context* c, const Level& L, int cfg, const T* val, const 
   bool default_order = true;
   for (int i = 0; i < kColours; ++i) default_order = default_order && L.g.sweep[i] == kSweepDefault[i];
   const int u = usable_cfg(cfg, r0);
-  if (default_order && (u == 0 || u == 1 || u == 4 || u == 5)) {
+  if (default_order && (u == 0 || u == 1 || u == 4 || u == 5 || u == 7 || u == 8)) {
     switch (u) {
       case 0: gs_first_const<T, TR, 0>(c, L, val, rhs, x, r0, r1, s); return;
       case 1: gs_first_const<T, TR, 1>(c, L, val, rhs, x, r0, r1, s); return;
       case 4: gs_first_const<T, TR, 4>(c, L, val, rhs, x, r0, r1, s); return;
-      default: gs_first_const<T, TR, 5>(c, L, val, rhs, x, r0, r1, s); return;
+      case 5: gs_first_const<T, TR, 5>(c, L, val, rhs, x, r0, r1, s); return;
+      case 7: gs_first_const<T, TR, 7>(c, L, val, rhs, x, r0, r1, s); return;
+      default: gs_first_const<T, TR, 8>(c, L, val, rhs, x, r0, r1, s); return;
     }
   }
   gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, mask);
@@ -132,17 +151,20 @@ void restrict_dispatch(Context* c, const Level& L, const T* val, const T* rf, co
 }
 
 template <typename T, typename TR>
-int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int s, bool first, bool top) {
+int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int s, bool first, bool top,
+                 double* dot = nullptr) {
   const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
   if (r1 <= r0) return HPCG_B200_OK;
-  const int kind = top ? (first ? kProfGsFirst : kProfGsFull) : -1;
+  const int kind = !top ? -1
+                   : sizeof(T) == 4 ? (first ? kProfGs32First : kProfGs32Full)
+                                    : (first ? kProfGsFirst : kProfGsFull);
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
   const int cfg = sizeof(T) == 4 ? L.gs_sched32 : first ? L.gs_first : L.gs_sched;
   if (first)
     gs_first_dispatch<T, TR>(c, L, cfg, val, rhs, x, r0, r1, s, first_mask(L.g, s));
   else
-    gs_dispatch<T, TR, false>(c, L, cfg, val, rhs, x, r0, r1, kAllSlots);
+    gs_dispatch<T, TR, false>(c, L, cfg, val, rhs, x, r0, r1, kAllSlots, dot);
   HB_CK(cudaGetLastError());
   return prof_end(c, kind, ev0, r1 - r0);
 }
@@ -152,14 +174,21 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
 // not repeated at the start of the backward sweep: its rows read only other
 // colours, none of which changed in between, so a repeat would rewrite the
 // same bits. first: x enters as zero (ComputeMG_ref.cpp:42).
+// dot (x entering nonzero only): the phase that writes each colour's final
+// value (the last colour's forward phase, every other colour's backward phase)
+// also writes r'x block partials at dot + kDotStride * (sweep position); the
+// caller zeroes the kColours * kDotStride slots first.
 template <typename T, typename TR>
-int gs_colour(Context* c, const Level& L, const T* val, const TR* rhs, T* x, bool first, bool top) {
+int gs_colour(Context* c, const Level& L, const T* val, const TR* rhs, T* x, bool first, bool top,
+              double* dot = nullptr) {
   int last = -1;
-  for (int s = 0; s < kColours; ++s) {
+  for (int s = 0; s < kColours; ++s)
     if (L.g.start[s + 1] > L.g.start[s]) last = s;
-    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, first, top)));
-  }
-  for (int s = last - 1; s >= 0; --s) HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, false, top)));
+  for (int s = 0; s < kColours; ++s)
+    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, first, top,
+                                dot && !first && s == last ? dot + (int64_t)kDotStride * s : nullptr)));
+  for (int s = last - 1; s >= 0; --s)
+    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, false, top, dot ? dot + (int64_t)kDotStride * s : nullptr)));
   return HPCG_B200_OK;
 }
 
@@ -210,18 +239,21 @@ int gs_natural(Context* c, Level& L, const double* rhs, double* x) {
   return HPCG_B200_OK;
 }
 
-int symgs_level(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero) {
+// dot: see gs_colour (colour mode only).
+int symgs_level(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero, double* dot = nullptr) {
   Level& L = p->lev[l];
   Context* c = p->ctx;
   if (p->symgs_mode == HPCG_B200_SYMGS_NATURAL) {
     if (x_is_zero) HB_CK(cudaMemsetAsync(x, 0, sizeof(double) * L.n, c->stream));
     return gs_natural(c, L, rhs, x);
   }
-  return gs_colour<double, double>(c, L, L.val, rhs, x, x_is_zero, l == 0);
+  return gs_colour<double, double>(c, L, L.val, rhs, x, x_is_zero, l == 0, dot);
 }
 
-// ComputeMG_ref.cpp:39-63 on colour-order device vectors of level l.
-int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x) {
+// ComputeMG_ref.cpp:39-63 on colour-order device vectors of level l. rtz (level
+// 0, colour mode): the post-smoother also leaves the block partials of r'x in
+// rtz[0 .. kColours * kDotStride), zeroed here first.
+int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x, double* rtz = nullptr) {
   Level& L = p->lev[l];
   Context* c = p->ctx;
   HB_TRY(symgs_level(p, l, r, x, true));
@@ -235,10 +267,14 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x) {
     HB_TRY(mg_level(p, l + 1, C.r, C.x));
     k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x, x, C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY(symgs_level(p, l, r, x, false));
+    if (rtz) HB_CK(cudaMemsetAsync(rtz, 0, sizeof(double) * kColours * kDotStride, c->stream));
+    HB_TRY(symgs_level(p, l, r, x, false, rtz));
   }
   return HPCG_B200_OK;
 }
+
+// The CG's r'z comes out of the post-smoother (colour mode, more than one level).
+bool rtz_fused(const hpcg_b200_problem* P) { return P->symgs_mode == HPCG_B200_SYMGS_COLOUR && P->nlev > 1; }
 
 // Autotuner: per level, times each kernel configuration (load schedule x
 // registers per thread) of the Gauss-Seidel phase and of the SpMV on scratch
@@ -254,7 +290,8 @@ int autotune(hpcg_b200_problem* P) {
     L.tuned = true;
     if (force && *force) {
       const int f = std::atoi(force);
-      L.gs_sched = L.mv_sched = L.gs_first = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
+      L.gs_sched = L.gs_first = f < 0 ? 0 : f >= kGsConfigs ? kGsConfigs - 1 : f;
+      L.mv_sched = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
       continue;
     }
     double* xs = l == 0 ? P->Ap : L.x;
@@ -268,10 +305,11 @@ int autotune(hpcg_b200_problem* P) {
     // Repetitions run round-robin over the configurations, so that a drift of
     // the clocks during tuning (the power cap settling) biases none of them.
     const int kOrders = 3;  // SpMV row orders: storage, natural, slab
-    float t_gs[kConfigs], t_first[kConfigs], t_mv[kConfigs][kOrders];
-    for (int k = 0; k < kConfigs; ++k) {
+    float t_gs[kGsConfigs], t_first[kGsConfigs], t_mv[kConfigs][kOrders];
+    for (int k = 0; k < kGsConfigs; ++k) {
       t_gs[k] = t_first[k] = 1e30f;
-      for (int v = 0; v < kOrders; ++v) t_mv[k][v] = 1e30f;
+      if (k < kConfigs)
+        for (int v = 0; v < kOrders; ++v) t_mv[k][v] = 1e30f;
     }
     auto time_it = [&](float& best, auto&& launch) -> int {
       HB_CK(cudaEventRecord(e0, c->stream));
@@ -285,7 +323,7 @@ int autotune(hpcg_b200_problem* P) {
     };
     const int keep_sched = L.mv_sched, keep_order = L.mv_order;
     for (int rep = 0; rep < 4; ++rep) {
-      for (int sched = 0; sched < kConfigs; ++sched) {
+      for (int sched = 0; sched < kGsConfigs; ++sched) {
         HB_TRY(time_it(t_gs[sched], [&] {
           gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
         }));
@@ -294,7 +332,7 @@ int autotune(hpcg_b200_problem* P) {
           gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, L.g.start[4], L.g.start[5], 4,
                                             first_mask(L.g, 4));
         }));
-        for (int v = 0; v < kOrders; ++v) {
+        for (int v = 0; v < kOrders && sched < kConfigs; ++v) {
           L.mv_sched = sched;
           L.mv_order = v;
           // the variant CG runs: fused with the p'Ap partials
@@ -305,10 +343,10 @@ int autotune(hpcg_b200_problem* P) {
     L.mv_sched = keep_sched;
     L.mv_order = keep_order;
     float best_gs = 1e30f, best_mv = 1e30f, best_first = 1e30f;
-    for (int sched = 0; sched < kConfigs; ++sched) {
+    for (int sched = 0; sched < kGsConfigs; ++sched) {
       if (t_gs[sched] < best_gs) { best_gs = t_gs[sched]; L.gs_sched = sched; }
       if (t_first[sched] < best_first) { best_first = t_first[sched]; L.gs_first = sched; }
-      for (int v = 0; v < kOrders; ++v)
+      for (int v = 0; v < kOrders && sched < kConfigs; ++v)
         if (t_mv[sched][v] < best_mv) { best_mv = t_mv[sched][v]; L.mv_sched = sched; L.mv_order = v; }
     }
     const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
@@ -362,14 +400,19 @@ int cg_iteration_body(hpcg_b200_problem* P, bool prec) {
   const int n = L.n;
   const int nb = red_blocks(c, n);
   const int gv = grid_for(c, n, kThreads, kPerSm);
-  if (prec) {
-    HB_TRY(mg_level(P, 0, P->r, P->z));
+  if (prec && rtz_fused(P)) {
+    HB_TRY(mg_level(P, 0, P->r, P->z, c->partials));
+    HB_TRY(finalize(c, kColours * kDotStride, kFinRtzIter));
   } else {
-    HB_CK(cudaMemcpyAsync(P->z, P->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (prec) {
+      HB_TRY(mg_level(P, 0, P->r, P->z));
+    } else {
+      HB_CK(cudaMemcpyAsync(P->z, P->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);
+    HB_CK(cudaGetLastError());
+    HB_TRY(finalize(c, nb, kFinRtzIter));
   }
-  k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);
-  HB_CK(cudaGetLastError());
-  HB_TRY(finalize(c, nb, kFinRtzIter));
   k_update_p_iter<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);
   HB_CK(cudaGetLastError());
   const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
@@ -519,19 +562,23 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
   *niters = 0;
   for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
     HB_TRY(mark());
+    const bool fused = prec && rtz_fused(P);
     if (prec) {
-      HB_TRY(mg_level(P, 0, P->r, P->z));                                   // CG.cpp:103
+      HB_TRY(mg_level(P, 0, P->r, P->z, fused ? c->partials : nullptr));  // CG.cpp:103 (and r'z, :110 / :113)
     } else {
       HB_CK(cudaMemcpyAsync(P->z, P->r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :105
     }
     HB_TRY(mark());
-    k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);  // :110 / :113
-    HB_CK(cudaGetLastError());
+    const int rz_parts = fused ? kColours * kDotStride : nb;
+    if (!fused) {
+      k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);  // :110 / :113
+      HB_CK(cudaGetLastError());
+    }
     if (k == 1) {
-      HB_TRY(finalize(c, nb, kFinRtzFirst));
+      HB_TRY(finalize(c, rz_parts, kFinRtzFirst));
       HB_CK(cudaMemcpyAsync(P->p, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :109
     } else {
-      HB_TRY(finalize(c, nb, kFinRtz));
+      HB_TRY(finalize(c, rz_parts, kFinRtz));
       k_update_p<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);  // :115
       HB_CK(cudaGetLastError());
     }
@@ -599,7 +646,7 @@ int ensure_f32(hpcg_b200_problem* P) {
       const char* force = std::getenv("HPCG_B200_CONFIG");
       if (force && *force) {
         const int f = std::atoi(force);
-        L.gs_sched32 = f < 0 ? 0 : f >= kConfigs ? kConfigs - 1 : f;
+        L.gs_sched32 = f < 0 ? 0 : f >= kGsConfigs ? kGsConfigs - 1 : f;
         continue;
       }
       const int r0 = L.g.start[1], r1 = L.g.start[2];
@@ -607,10 +654,10 @@ int ensure_f32(hpcg_b200_problem* P) {
       cudaEvent_t e0, e1;
       HB_CK(cudaEventCreate(&e0));
       HB_CK(cudaEventCreate(&e1));
-      float t[kConfigs];
-      for (int cfg = 0; cfg < kConfigs; ++cfg) t[cfg] = 1e30f;
+      float t[kGsConfigs];
+      for (int cfg = 0; cfg < kGsConfigs; ++cfg) t[cfg] = 1e30f;
       for (int rep = 0; rep < 4; ++rep) {  // round-robin over the configurations, as in autotune
-        for (int cfg = 0; cfg < kConfigs; ++cfg) {
+        for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
           HB_CK(cudaEventRecord(e0, c->stream));
           gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
           HB_CK(cudaEventRecord(e1, c->stream));
@@ -621,8 +668,11 @@ int ensure_f32(hpcg_b200_problem* P) {
         }
       }
       float best = 1e30f;
-      for (int cfg = 0; cfg < kConfigs; ++cfg)
-        if (t[cfg] < best) { best = t[cfg]; L.gs_sched32 = cfg; }
+      for (int cfg = 0; cfg < kGsConfigs; ++cfg)
+        if (t[cfg] < best) {
+          best = t[cfg];
+          L.gs_sched32 = cfg;
+        }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       HB_CK(cudaGetLastError());
@@ -635,7 +685,7 @@ int ensure_f32(hpcg_b200_problem* P) {
 int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
   Level& L = p->lev[l];
   Context* c = p->ctx;
-  HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, true, false)));
+  HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, true, l == 0)));
   if (l + 1 < p->nlev) {
     Level& C = p->lev[l + 1];
     restrict_dispatch<float>(c, L, L.val32, r, x, C.r32, C.n);
@@ -643,7 +693,7 @@ int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
     HB_TRY(mg32_level(p, l + 1, C.r32, C.x32));
     k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x32, x, C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, false, false)));
+    HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, false, l == 0)));
   }
   return HPCG_B200_OK;
 }
@@ -667,29 +717,32 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
   double normr = std::sqrt(c->scal_host->normr2);
   const double normr0 = normr;
   *niters = 0;
-  for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
+  // z and zprev alternate between two buffers; r32 is refreshed by the x/r update
+  double* zc = P->z;
+  double* zp = P->zprev;
+  if (max_iter >= 1 && normr / normr0 > tol) {
     k_convert<float, double><<<gv, kThreads, 0, c->stream>>>(L.r32, P->r, n);
     HB_CK(cudaGetLastError());
+  }
+  for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
     HB_TRY(mg32_level(P, 0, L.r32, L.x32));
-    k_convert<double, float><<<gv, kThreads, 0, c->stream>>>(P->z, L.x32, n);
-    HB_CK(cudaGetLastError());
     if (k == 1) {
-      k_dot<false><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, nullptr, c->partials);
+      k_widen_dot<false><<<nb, kThreads, 0, c->stream>>>(n, L.x32, P->r, zc, nullptr, c->partials);
       HB_CK(cudaGetLastError());
       HB_TRY(finalize(c, nb, kFinRtzFirst));
-      HB_CK(cudaMemcpyAsync(P->p, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+      HB_CK(cudaMemcpyAsync(P->p, zc, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
     } else {
-      k_dot<true><<<nb, kThreads, 0, c->stream>>>(n, P->r, P->z, P->zprev, c->partials);
+      k_widen_dot<true><<<nb, kThreads, 0, c->stream>>>(n, L.x32, P->r, zc, zp, c->partials);
       HB_CK(cudaGetLastError());
       HB_TRY(finalize(c, nb, kFinFlex));
-      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);
+      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, zc, P->p, c->scal);
       HB_CK(cudaGetLastError());
     }
-    HB_CK(cudaMemcpyAsync(P->zprev, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    std::swap(zc, zp);
     const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, gs, kFinPap));
-    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);
+    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials, L.r32);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, nb, kFinNormr));
     HB_TRY(read_scalars(c));
@@ -744,9 +797,11 @@ int prolong_level(hpcg_b200_problem* p, int l, const double* xc, double* xf) {
   return HPCG_B200_OK;
 }
 
-int symgs_step(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero) {
-  return symgs_level(p, l, rhs, x, x_is_zero);
+int symgs_step(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool x_is_zero, double* dot) {
+  return symgs_level(p, l, rhs, x, x_is_zero, dot);
 }
+
+bool rtz_from_smoother(const hpcg_b200_problem* p) { return rtz_fused(p); }
 
 int reduction_blocks(const Context* c, int64_t n) { return red_blocks(c, n); }
 
@@ -903,6 +958,24 @@ int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max
   HB_TRY(load_vector(p, 0, x, p->x));
   HB_TRY(run_cg_mixed(p, max_iter, tolerance, niters, normr, normr0));
   return store_vector(p, 0, p->x, x);
+}
+
+int hpcg_b200_mg_f32(hpcg_b200_problem* p, const double* r, double* x) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
+  if (!r || !x) return HPCG_B200_ERR_ARG;
+  Setter dev(p->device);
+  HB_TRY(ensure_f32(p));
+  Level& L = p->lev[0];
+  Context* c = p->ctx;
+  const int gv = grid_for(c, L.n, kThreads, kPerSm);
+  HB_TRY(load_vector(p, 0, r, p->r));
+  k_convert<float, double><<<gv, kThreads, 0, c->stream>>>(L.r32, p->r, L.n);
+  HB_CK(cudaGetLastError());
+  HB_TRY(mg32_level(p, 0, L.r32, L.x32));
+  k_convert<double, float><<<gv, kThreads, 0, c->stream>>>(p->z, L.x32, L.n);
+  HB_CK(cudaGetLastError());
+  return store_vector(p, 0, p->z, x);
 }
 
 int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, int max_iter, double tolerance,

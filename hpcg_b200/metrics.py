@@ -99,3 +99,14 @@ def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8):
     colours hold an eighth of the rows each)."""
     per_row = SLOTS * (vb + 4) + 2 * vb
     return rows_in_phase * per_row + 7.0 * rows_in_phase * vb
+
+
+def first_sweep_bytes(rows, vb=8):
+    """Algorithmic bytes of the first forward sweeps (x = 0) that together
+    updated `rows` rows, summed over whole sweeps (all eight colours): a phase
+    reads only the slots of colours swept before it, 13 of the 27 per row on
+    average (each neighbouring pair of colours once: 8 colours x 26 neighbours
+    / 2 / 8), plus the diagonal value, the right-hand side, the x write and the
+    swept colours' x (28 colour-eighths over 8 phases = 3.5 entries per row)."""
+    return rows * (13 * (vb + 4) + vb + 2 * vb + 3.5 * vb)
+

@@ -133,6 +133,10 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
 int hpcg_b200_cg_mixed(hpcg_b200_problem* p, const double* b, double* x, int max_iter, double tolerance,
                        int* niters, double* normr, double* normr0);
 
+/* The FP32 V-cycle alone, as hpcg_b200_cg_mixed applies it:
+ * x = widen(MG32(narrow(r))), natural order, host or device vectors. */
+int hpcg_b200_mg_f32(hpcg_b200_problem* p, const double* r, double* x);
+
 /* ---- changed form 2: several right-hand sides at once ---------------------- */
 
 /* Preconditioned CG (CG.cpp:59-143 semantics) for nrhs <= 8 systems with the
@@ -293,11 +297,14 @@ void* hpcg_b200_stream(int device);
 /* Launch profiler: with enable != 0, CUDA events are recorded around each launch
  * of the timed kernel classes; enabling resets the totals. Kinds:
  * 0 Gauss-Seidel colour phase on level 0 (all slots), 1 first forward sweep on
- * level 0, 2 CG SpMV on level 0, 3 residual+restriction from level 0. */
+ * level 0, 2 CG SpMV on level 0, 3 residual+restriction from level 0, 4 and 5
+ * the same two phase kinds of the FP32 V-cycle. */
 #define HPCG_B200_PROF_GS_FULL 0
 #define HPCG_B200_PROF_GS_FIRST 1
 #define HPCG_B200_PROF_SPMV 2
 #define HPCG_B200_PROF_RESTRICT 3
+#define HPCG_B200_PROF_GS32_FULL 4   /* FP32 V-cycle (hpcg_b200_cg_mixed): colour phase on level 0 */
+#define HPCG_B200_PROF_GS32_FIRST 5  /* FP32 V-cycle: first forward sweep on level 0 */
 int hpcg_b200_profile(int device, int enable);
 int hpcg_b200_profile_read(int device, int kind, double* total_ms, int64_t* launches, int64_t* rows);
 

@@ -257,13 +257,20 @@ static inline float gs_row_f32(const ora_level_f32* A, int i, const float* r, co
   return s / d;
 }
 
-static void symgs_f32(const ora_level_f32* A, const float* r, float* x) {
+/* skip: rows at the end of the forward sweep not repeated at the start of the
+ * backward one (0: ComputeSYMGS_ref.cpp:67-100 exactly); see ora_symgs_skip. */
+static void symgs_f32(const ora_level_f32* A, const float* r, float* x, int skip) {
   for (int i = 0; i < A->n; ++i) x[i] = gs_row_f32(A, i, r, x);
-  for (int i = A->n - 1; i >= 0; --i) x[i] = gs_row_f32(A, i, r, x);
+  for (int i = A->n - 1 - skip; i >= 0; --i) x[i] = gs_row_f32(A, i, r, x);
 }
 
 int ora_mg_f32(const ora_level_f32* L, int nlev, int lev, const float* r, float* x) {
+  return ora_mg_f32_skip(L, nlev, lev, r, x, NULL);
+}
+
+int ora_mg_f32_skip(const ora_level_f32* L, int nlev, int lev, const float* r, float* x, const int* skip) {
   const ora_level_f32* A = &L[lev];
+  const int sk = skip ? skip[lev] : 0;
   memset(x, 0, sizeof(float) * (size_t)A->n);
   if (lev + 1 < nlev) {
     const int nc = L[lev + 1].n;
@@ -271,7 +278,7 @@ int ora_mg_f32(const ora_level_f32* L, int nlev, int lev, const float* r, float*
     float* rc = (float*)malloc(sizeof(float) * (size_t)nc);
     float* xc = (float*)malloc(sizeof(float) * (size_t)nc);
     if (!Axf || !rc || !xc) { free(Axf); free(rc); free(xc); return 1; }
-    symgs_f32(A, r, x);
+    symgs_f32(A, r, x, sk);
     for (int i = 0; i < A->n; ++i) {
       const int* c = A->cols + (int64_t)i * ORA_SLOTS;
       const float* v = A->vals + (int64_t)i * ORA_SLOTS;
@@ -280,15 +287,15 @@ int ora_mg_f32(const ora_level_f32* L, int nlev, int lev, const float* r, float*
       Axf[i] = s;
     }
     for (int q = 0; q < nc; ++q) rc[q] = r[A->f2c[q]] - Axf[A->f2c[q]];
-    int err = ora_mg_f32(L, nlev, lev + 1, rc, xc);
+    int err = ora_mg_f32_skip(L, nlev, lev + 1, rc, xc, skip);
     if (!err) {
       for (int q = 0; q < nc; ++q) x[A->f2c[q]] += xc[q];
-      symgs_f32(A, r, x);
+      symgs_f32(A, r, x, sk);
     }
     free(Axf); free(rc); free(xc);
     return err;
   }
-  symgs_f32(A, r, x);
+  symgs_f32(A, r, x, sk);
   return 0;
 }
 

@@ -117,6 +117,9 @@ typedef struct ora_level_f32 {
   const int* f2c;
 } ora_level_f32;
 int ora_mg_f32(const ora_level_f32* levels, int nlev, int lev, const float* r, float* x);
+/* The same with the last `skip[lev]` rows of each level's forward sweep not repeated
+ * at the start of its backward sweep (the B200 colour order's last colour). */
+int ora_mg_f32_skip(const ora_level_f32* levels, int nlev, int lev, const float* r, float* x, const int* skip);
 
 /* Flexible PCG (Polak-Ribiere beta = r'(z - z_prev)/oldrtz) in FP64 with the
  * FP32 V-cycle as preconditioner: r is converted to float, the V-cycle runs in

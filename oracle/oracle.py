@@ -79,6 +79,8 @@ def _load_oracle():
     lib.ora_permute_f2c.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p]
     lib.ora_mg_f32.restype = C.c_int
     lib.ora_mg_f32.argtypes = [C.POINTER(_Level32), C.c_int, C.c_int, _f32p, _f32p]
+    lib.ora_mg_f32_skip.restype = C.c_int
+    lib.ora_mg_f32_skip.argtypes = [C.POINTER(_Level32), C.c_int, C.c_int, _f32p, _f32p, _i32p]
     lib.ora_cg_mixed.restype = C.c_int
     lib.ora_cg_mixed.argtypes = [C.POINTER(_Level), C.POINTER(_Level32), C.c_int, _f64p, _f64p, C.c_int,
                                  C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double),
@@ -265,9 +267,15 @@ def _levels32_c(l32):
     return arr
 
 
-def mg_f32(l32, r):
+def mg_f32(l32, r, skip=None):
+    """FP32 V-cycle (ComputeMG_ref.cpp:39-63 in float); skip: per-level rows not
+    repeated at the turn of each symmetric sweep (None: the reference's sweep)."""
     x = np.zeros(l32[0]["n"], np.float32)
-    err = lib().ora_mg_f32(_levels32_c(l32), len(l32), 0, np.ascontiguousarray(r, np.float32), x)
+    if skip is None:
+        err = lib().ora_mg_f32(_levels32_c(l32), len(l32), 0, np.ascontiguousarray(r, np.float32), x)
+    else:
+        sk = np.ascontiguousarray(skip, np.int32)
+        err = lib().ora_mg_f32_skip(_levels32_c(l32), len(l32), 0, np.ascontiguousarray(r, np.float32), x, sk)
     assert err == 0
     return x
 

@@ -220,6 +220,29 @@ def test_mg_colour_bitwise(oracle, binding, case32):
     assert np.max(np.abs(z - ref)) <= 1e-14 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("cfg", [str(c) for c in range(9)])
+def test_mg_colour_every_config_bitwise(oracle, binding, monkeypatch, cfg):
+    """Every kernel configuration of the phases (load schedules, registers, 2 or 4
+    contiguous rows with vector loads, 2 or 4 interleaved rows) computes the same
+    V-cycle bits; the coarsest level (3 x 2 x 5) has colour blocks of odd sizes
+    starting off multiples of 4."""
+    monkeypatch.setenv("HPCG_B200_CONFIG", cfg)
+    P = oracle.generate(24, 16, 40)
+    D = binding.Problem.generate(24, 16, 40)
+    try:
+        perms = perms_of(binding, P)
+        PL = oracle.permute(P.levels, perms)
+        r = np.random.default_rng(int(cfg)).standard_normal(P.levels[0].n)
+        z = np.zeros_like(r)
+        D.ComputeMG(r, z)
+        assert D.level_config(0)["gs"] == int(cfg)
+        exp = np.empty_like(z)
+        exp[perms[0]] = oracle.mg(PL, r[perms[0]], skip=skip_of(binding, P))
+        assert np.array_equal(z, exp)
+    finally:
+        D.free()
+
+
 def test_mg_natural_is_reference_bitwise(oracle, binding, case16):
     P, D, _, _ = case16
     g = np.load(os.path.join(GOLD, "golden_16.npz"))
@@ -421,6 +444,32 @@ def test_symmetry_departure(binding, case32):
     D.ComputeMG(x, z)
     ytMx = binding.ComputeDotProduct(n, y, z)
     assert abs(xtMy - ytMx) / ((xn * 52 * yn + yn * 52 * xn) * eps) <= 1.0
+
+
+@pytest.mark.parametrize("cfg", [None, "1", "6", "7", "8"])
+def test_fp32_vcycle_bitwise(oracle, binding, monkeypatch, cfg):
+    """The FP32 V-cycle (autotuned, or one kernel configuration forced: rows per
+    thread 1, 4 contiguous, 2 and 4 interleaved) is bitwise the oracle's FP32
+    V-cycle on the colour order with the last colour not repeated at the turn of
+    each sweep."""
+    if cfg is not None:
+        monkeypatch.setenv("HPCG_B200_CONFIG", cfg)
+    P = oracle.generate(32, 24, 16)
+    D = binding.Problem.generate(32, 24, 16)
+    try:
+        perms = perms_of(binding, P)
+        PL = oracle.permute(P.levels, perms)
+        r = np.random.default_rng(3).standard_normal(P.levels[0].n)
+        x = np.zeros_like(r)
+        D.ComputeMG_f32(r, x)
+        if cfg is not None:
+            assert D.level_config(0)["gs32"] == int(cfg)
+        z = oracle.mg_f32(oracle.to_f32(PL), r[perms[0]].astype(np.float32), skip=skip_of(binding, P))
+        exp = np.empty_like(r)
+        exp[perms[0]] = z.astype(np.float64)
+        assert np.array_equal(x, exp)
+    finally:
+        D.free()
 
 
 def test_mixed_precision_vs_oracle(oracle, binding, case32):
