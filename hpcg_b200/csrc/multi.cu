@@ -50,13 +50,18 @@ int alloc_z(MultiState* m, double** p, size_t count, cudaStream_t st) {
 }
 
 template <int K, int LANES>
-int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first);
+int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x);
 
-// One symmetric sweep of level 0 with LANES threads per row.
+// The matrix work of one CG iteration with LANES threads per row: a V-cycle and
+// the SpMV with its p'Ap partials.
 template <int K, int LANES>
-int time_sweep(Context* c, const Level& L, MultiState* m, cudaEvent_t e0, cudaEvent_t e1, float* best) {
+int time_iteration(hpcg_b200_problem* P, MultiState* m, cudaEvent_t e0, cudaEvent_t e1, float* best) {
+  Context* c = P->ctx;
+  const Level& L = P->lev[0];
   HB_CK(cudaEventRecord(e0, c->stream));
-  HB_TRY((gs_colour_m<K, LANES>(c, L, m->r, m->x, false)));
+  HB_TRY((mg_m<K, LANES>(P, m, 0, m->r, m->z)));
+  k_spmv_m<K, LANES, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, L.n, m->partials);
+  HB_CK(cudaGetLastError());
   HB_CK(cudaEventRecord(e1, c->stream));
   HB_CK(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -65,8 +70,8 @@ int time_sweep(Context* c, const Level& L, MultiState* m, cudaEvent_t e0, cudaEv
   return HPCG_B200_OK;
 }
 
-// Threads per row of the matrix kernels: the fastest symmetric sweep on level 0
-// (round-robin repetitions), or HPCG_B200_MULTI_LANES. Same bits either way.
+// Threads per row of the matrix kernels: the fastest V-cycle + SpMV (round-robin
+// repetitions), or HPCG_B200_MULTI_LANES. Same V-cycle bits either way.
 int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
   const int K = m->K;
   const char* force = std::getenv("HPCG_B200_MULTI_LANES");
@@ -75,23 +80,22 @@ int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
     m->lanes = f >= 4 && K >= 8 ? 4 : f >= 2 && K >= 4 ? 2 : 1;
     return HPCG_B200_OK;
   }
-  const Level& L = P->lev[0];
   Context* c = P->ctx;
   cudaEvent_t e0, e1;
   HB_CK(cudaEventCreate(&e0));
   HB_CK(cudaEventCreate(&e1));
-  float t[3] = {1e30f, 1e30f, 1e30f};  // lanes 1, 2, 4
+  float t_[3] = {1e30f, 1e30f, 1e30f};  // lanes 1, 2, 4
   int st = HPCG_B200_OK;
   for (int rep = 0; rep < 3 && st == HPCG_B200_OK; ++rep) {
-    if (K == 2) st = time_sweep<2, 1>(c, L, m, e0, e1, &t[0]);
+    if (K == 2) st = time_iteration<2, 1>(P, m, e0, e1, &t_[0]);
     if (K == 4) {
-      st = time_sweep<4, 1>(c, L, m, e0, e1, &t[0]);
-      if (!st) st = time_sweep<4, 2>(c, L, m, e0, e1, &t[1]);
+      st = time_iteration<4, 1>(P, m, e0, e1, &t_[0]);
+      if (!st) st = time_iteration<4, 2>(P, m, e0, e1, &t_[1]);
     }
     if (K == 8) {
-      st = time_sweep<8, 1>(c, L, m, e0, e1, &t[0]);
-      if (!st) st = time_sweep<8, 2>(c, L, m, e0, e1, &t[1]);
-      if (!st) st = time_sweep<8, 4>(c, L, m, e0, e1, &t[2]);
+      st = time_iteration<8, 1>(P, m, e0, e1, &t_[0]);
+      if (!st) st = time_iteration<8, 2>(P, m, e0, e1, &t_[1]);
+      if (!st) st = time_iteration<8, 4>(P, m, e0, e1, &t_[2]);
     }
   }
   cudaEventDestroy(e0);
@@ -99,10 +103,16 @@ int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
   HB_TRY(st);
   int best = 0;
   for (int i = 1; i < 3; ++i)
-    if (t[i] < t[best]) best = i;
+    if (t_[i] < t_[best]) best = i;
   m->lanes = 1 << best;
-  // the timed phases wrote m->x: every solve loads its own x, every V-cycle starts from zero
-  HB_CK(cudaMemsetAsync(m->x, 0, sizeof(double) * (size_t)P->lev[0].pitch * K, c->stream));
+  // the timed work wrote z, Ap and the coarse vectors: every solve loads its own
+  // b and x and every V-cycle starts from zero, but leave the state as created
+  HB_CK(cudaMemsetAsync(m->z, 0, sizeof(double) * (size_t)P->lev[0].pitch * K, c->stream));
+  HB_CK(cudaMemsetAsync(m->Ap, 0, sizeof(double) * (size_t)P->lev[0].pitch * K, c->stream));
+  for (int l = 1; l < P->nlev; ++l) {
+    HB_CK(cudaMemsetAsync(m->lr[l], 0, sizeof(double) * (size_t)P->lev[l].pitch * K, c->stream));
+    HB_CK(cudaMemsetAsync(m->lx[l], 0, sizeof(double) * (size_t)P->lev[l].pitch * K, c->stream));
+  }
   return HPCG_B200_OK;
 }
 
@@ -135,28 +145,32 @@ int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
 }
 
 template <int K, int LANES>
+void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, int r0, int r1, bool first,
+                    uint32_t mask) {
+  const int64_t work = (int64_t)(r1 - r0) * LANES;
+  if (first) {
+    auto k = k_gs_phase_m<K, LANES, true>;
+    k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask);
+  } else {
+    auto k = k_gs_phase_m<K, LANES, false>;
+    k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask);
+  }
+}
+
+template <int K, int LANES>
 int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first) {
   int last = -1;
   for (int s = 0; s < kColours; ++s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
     last = s;
-    const int64_t work = (int64_t)(r1 - r0) * LANES;
-    if (first) {
-      auto k = k_gs_phase_m<K, LANES, true>;
-      k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, first_mask(L.g, s));
-    } else {
-      auto k = k_gs_phase_m<K, LANES, false>;
-      k<<<grid_of(c, k, work), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, kAllSlots);
-    }
+    launch_phase_m<K, LANES>(c, L, rhs, x, r0, r1, first, first ? first_mask(L.g, s) : kAllSlots);
   }
   // backward sweep, without repeating the last colour (as the single-system path)
   for (int s = last - 1; s >= 0; --s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
-    auto k = k_gs_phase_m<K, LANES, false>;
-    k<<<grid_of(c, k, (int64_t)(r1 - r0) * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1,
-                                                                               kAllSlots);
+    launch_phase_m<K, LANES>(c, L, rhs, x, r0, r1, false, kAllSlots);
   }
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
