@@ -40,8 +40,11 @@ namespace hb {
 //    thread updates R rows 32 apart, so every load of a warp is one coalesced
 //    run (no vector loads, no strided gathers) and each thread still has R
 //    independent rows' loads in flight.
-constexpr int kConfigs = 7;    // configurations of the SpMV and the restriction
-constexpr int kGsConfigs = 9;  // configurations of the Gauss-Seidel phases
+//  - tiled (configuration 9, Gauss-Seidel phases only): see k_gs_tile.
+constexpr int kConfigs = 7;     // configurations of the SpMV and the restriction
+constexpr int kGsConfigs = 10;  // configurations of the Gauss-Seidel phases
+constexpr int kTileCfg = 9;     // the tiled configuration
+__host__ __device__ constexpr bool cfg_tiled(int cfg) { return cfg >= kTileCfg; }
 __host__ __device__ constexpr int cfg_sched(int cfg) { return cfg == 2 || cfg == 3 ? kStaged : kPlain; }
 __host__ __device__ constexpr int cfg_minb(int cfg) {
   return cfg == 0 || cfg == 4 ? 4 : cfg == 2 ? 1 : 2;
@@ -49,7 +52,7 @@ __host__ __device__ constexpr int cfg_minb(int cfg) {
 __host__ __device__ constexpr int cfg_rows(int cfg) {
   return cfg == 4 || cfg == 5 || cfg == 7 ? 2 : cfg == 6 || cfg == 8 ? 4 : 1;
 }
-__host__ __device__ constexpr bool cfg_interleaved(int cfg) { return cfg >= 7; }
+__host__ __device__ constexpr bool cfg_interleaved(int cfg) { return cfg == 7 || cfg == 8; }
 
 // Gauss-Seidel colour phase: rows [r0, r1) of one colour, updated in parallel
 // (no two rows of a colour are neighbours).
@@ -166,6 +169,118 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
       if (DOT) acc += (double)rv[r] * (double)out[r];
     }
     store_vec<T, R>(x + q0, out);
+  }
+  if (DOT) {
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) dot[blockIdx.x] = s;
+  }
+}
+
+// ---- tiled Gauss-Seidel phase (configuration 9) -----------------------------
+// One thread per row; a block walks tiles of TILE rows. The values and columns
+// of the next STAGES-1 tiles stream into shared memory with asynchronous 16-byte
+// copies (cp.async) while the current tile computes, so the matrix loads are
+// never waited on by the row arithmetic, and each thread issues its 27 gathers
+// of x back to back from columns already on chip. STAGES x 27 slots x TILE rows
+// x (value + column) bytes of dynamic shared memory. Tiles start on a 4-row
+// boundary (16 bytes for both float and double); rows of a tile outside
+// [r0, r1) are copied (in bounds) or skipped (at and beyond r1 rounded up to 4,
+// which never exceeds the pitch) and never computed. The arithmetic is
+// gs_row's, in slot order: the same bits.
+// Measured at 512^3 it runs level 0 at half the speed of the plain
+// configurations (two blocks per SM leave too few threads to cover the gathers'
+// latency; three or four stages, one block per SM, ran three times slower), so
+// the autotuner picks it only on some coarse levels.
+
+// tile rows and pipeline stages of the tiled configuration
+template <typename T>
+__host__ __device__ constexpr int gs_tile_rows(int) {
+  return sizeof(T) == 8 ? 128 : 256;
+}
+__host__ __device__ constexpr int gs_tile_stages(int) { return 2; }
+
+template <typename T>
+__host__ __device__ constexpr int gs_tile_smem(int cfg) {
+  return gs_tile_stages(cfg) * kSlots * gs_tile_rows<T>(cfg) * (int)(sizeof(T) + sizeof(int));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// returns once at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1, bool DOT = false>
+__global__ void __launch_bounds__(gs_tile_rows<T>(CFG)) k_gs_tile(const T* __restrict__ val,
+                                                                  const int* __restrict__ col, int64_t pitch,
+                                                                  const TR* __restrict__ rhs, T* x, int r0, int r1,
+                                                                  uint32_t mask_arg, double* __restrict__ dot) {
+  constexpr int TILE = gs_tile_rows<T>(CFG);
+  constexpr int STAGES = gs_tile_stages(CFG);
+  constexpr int VCH = TILE * (int)sizeof(T) / 16;  // 16-byte chunks of one slot's values in a tile
+  constexpr int CCH = TILE * 4 / 16;               // ... of its columns
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* sval = reinterpret_cast<T*>(smem);                                            // [STAGES][27][TILE]
+  int* scol = reinterpret_cast<int*>(smem + STAGES * kSlots * TILE * sizeof(T));  // [STAGES][27][TILE]
+  const uint32_t mask = CMASK >= 0 ? (uint32_t)CMASK : mask_arg;
+  const int a0 = r0 & ~3;
+  const int lim = (r1 + 3) & ~3;
+  const int ntiles = (r1 - a0 + TILE - 1) / TILE;
+  // all (slot, chunk) pairs of a tile spread over the block's threads; the first
+  // sweep copies only its masked slots' values and columns and the diagonal value
+  auto issue = [&](int tile, int buf) {
+    const int b0 = a0 + tile * TILE;
+    for (int i = threadIdx.x; i < kSlots * VCH; i += TILE) {
+      const int k = i / VCH, ch = i - k * VCH;
+      const int row = b0 + ch * (16 / (int)sizeof(T));
+      if (((mask >> k) & 1u || (FIRST && k == kDiagSlot)) && row < lim)
+        cp_async16(sval + (buf * kSlots + k) * TILE + ch * (16 / sizeof(T)), val + k * pitch + row);
+    }
+    for (int i = threadIdx.x; i < kSlots * CCH; i += TILE) {
+      const int k = i / CCH, ch = i - k * CCH;
+      const int row = b0 + ch * 4;
+      if ((mask >> k) & 1u && row < lim) cp_async16(scol + (buf * kSlots + k) * TILE + ch * 4, col + k * pitch + row);
+    }
+  };
+  double acc = 0.0;
+  // prologue: the first STAGES-1 tiles of this block, one commit group each
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    const int t = blockIdx.x + s * gridDim.x;
+    if (t < ntiles) issue(t, s);
+    cp_async_commit();
+  }
+  int tile = blockIdx.x;
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    const int next = tile + (STAGES - 1) * gridDim.x;
+    if (next < ntiles) issue(next, (it + STAGES - 1) % STAGES);
+    cp_async_commit();
+    cp_async_wait<STAGES - 1>();  // this thread's copies of the current tile have landed
+    __syncthreads();              // and every other thread's
+    const int buf = it % STAGES;
+    const int q = a0 + tile * TILE + threadIdx.x;
+    if (q >= r0 && q < r1) {
+      T sum = (T)rhs[q];
+      T xd = (T)0;
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        if (mask & (1u << k)) {
+          const T a = sval[(buf * kSlots + k) * TILE + threadIdx.x];
+          const T xv = __ldg(x + scol[(buf * kSlots + k) * TILE + threadIdx.x]);
+          sum -= a * xv;
+          if (k == kDiagSlot) xd = xv;
+        }
+      }
+      const T d = sval[(buf * kSlots + kDiagSlot) * TILE + threadIdx.x];
+      if (!FIRST) sum += xd * d;
+      const T out = sum / d;
+      x[q] = out;
+      if (DOT) acc += (double)rhs[q] * (double)out;
+    }
+    __syncthreads();  // the buffer is refilled by the next iteration's copies
   }
   if (DOT) {
     const double s = block_sum(acc);

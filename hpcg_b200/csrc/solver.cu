@@ -6,6 +6,8 @@
 #include <cmath>
 #include <vector>
 
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace hb {
@@ -21,9 +23,43 @@ inline int red_blocks(const Context* c, int64_t n) {
 
 // dot != nullptr: the phase also writes its r'z block partials there (FP64
 // full-slot phases only; the grid is capped at kDotStride blocks).
+// The tiled phase (configuration 9): one block per SM-resident slot, walking
+// tiles of rows; its dynamic shared memory is enabled on first launch.
+template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK, bool DOT>
+void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
+                    double* dot) {
+  auto k = k_gs_tile<T, TR, FIRST, CFG, CMASK, DOT>;
+  constexpr int smem = gs_tile_smem<T>(CFG);
+  constexpr int rows = gs_tile_rows<T>(CFG);
+  static int per_sm = 0;  // resident blocks per SM with that shared memory (one device's figure)
+  if (per_sm == 0) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rows, smem) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+  }
+  const int a0 = r0 & ~3;
+  const int64_t tiles = ((int64_t)r1 - a0 + rows - 1) / rows;
+  int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms * per_sm);
+  if (DOT && g > kDotStride) g = kDotStride;
+  k<<<g, rows, smem, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, dot);
+}
+
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1>
 void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                double* dot = nullptr) {
+  if constexpr (cfg_tiled(CFG)) {
+    if (r1 <= r0) return;
+    if constexpr (!FIRST && CMASK < 0 && sizeof(T) == 8) {
+      if (dot) {
+        gs_tile_launch<T, TR, FIRST, CFG, CMASK, true>(c, L, val, rhs, x, r0, r1, mask, dot);
+        return;
+      }
+    }
+    gs_tile_launch<T, TR, FIRST, CFG, CMASK, false>(c, L, val, rhs, x, r0, r1, mask, nullptr);
+    return;
+  }
   const int64_t units = ((int64_t)(r1 - r0) + cfg_rows(CFG) - 1) / cfg_rows(CFG);
   if constexpr (!FIRST && CMASK < 0 && sizeof(T) == 8) {
     if (dot) {
@@ -42,7 +78,7 @@ void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, in
 // on a multiple of R (vector loads); otherwise the scalar configuration 1 runs.
 // Interleaved rows need no alignment.
 inline int usable_cfg(int cfg, int r0) {
-  return cfg_interleaved(cfg) || r0 % cfg_rows(cfg) == 0 ? cfg : 1;
+  return cfg_tiled(cfg) || cfg_interleaved(cfg) || r0 % cfg_rows(cfg) == 0 ? cfg : 1;
 }
 
 template <typename T, typename TR, bool FIRST>
@@ -57,7 +93,8 @@ void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rh
     case 5: gs_launch<T, TR, FIRST, 5>(c, L, val, rhs, x, r0, r1, mask, dot); break;
     case 6: gs_launch<T, TR, FIRST, 6>(c, L, val, rhs, x, r0, r1, mask, dot); break;
     case 7: gs_launch<T, TR, FIRST, 7>(c, L, val, rhs, x, r0, r1, mask, dot); break;
-    default: gs_launch<T, TR, FIRST, 8>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 8: gs_launch<T, TR, FIRST, 8>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    default: gs_launch<T, TR, FIRST, 9>(c, L, val, rhs, x, r0, r1, mask, dot); break;
   }
 }
 
@@ -85,14 +122,15 @@ void gs_first_dispatch(Context* c, const Level& L, int cfg, const T* val, const 
   bool default_order = true;
   for (int i = 0; i < kColours; ++i) default_order = default_order && L.g.sweep[i] == kSweepDefault[i];
   const int u = usable_cfg(cfg, r0);
-  if (default_order && (u == 0 || u == 1 || u == 4 || u == 5 || u == 7 || u == 8)) {
+  if (default_order && (u == 0 || u == 1 || u == 4 || u == 5 || u == 7 || u == 8 || cfg_tiled(u))) {
     switch (u) {
       case 0: gs_first_const<T, TR, 0>(c, L, val, rhs, x, r0, r1, s); return;
       case 1: gs_first_const<T, TR, 1>(c, L, val, rhs, x, r0, r1, s); return;
       case 4: gs_first_const<T, TR, 4>(c, L, val, rhs, x, r0, r1, s); return;
       case 5: gs_first_const<T, TR, 5>(c, L, val, rhs, x, r0, r1, s); return;
       case 7: gs_first_const<T, TR, 7>(c, L, val, rhs, x, r0, r1, s); return;
-      default: gs_first_const<T, TR, 8>(c, L, val, rhs, x, r0, r1, s); return;
+      case 8: gs_first_const<T, TR, 8>(c, L, val, rhs, x, r0, r1, s); return;
+      default: gs_first_const<T, TR, 9>(c, L, val, rhs, x, r0, r1, s); return;
     }
   }
   gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, mask);

@@ -220,10 +220,11 @@ def test_mg_colour_bitwise(oracle, binding, case32):
     assert np.max(np.abs(z - ref)) <= 1e-14 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("cfg", [str(c) for c in range(9)])
+@pytest.mark.parametrize("cfg", [str(c) for c in range(10)])
 def test_mg_colour_every_config_bitwise(oracle, binding, monkeypatch, cfg):
     """Every kernel configuration of the phases (load schedules, registers, 2 or 4
-    contiguous rows with vector loads, 2 or 4 interleaved rows) computes the same
+    contiguous rows with vector loads, 2 or 4 interleaved rows, shared-memory
+    tiles filled by asynchronous copies) computes the same
     V-cycle bits; the coarsest level (3 x 2 x 5) has colour blocks of odd sizes
     starting off multiples of 4."""
     monkeypatch.setenv("HPCG_B200_CONFIG", cfg)
@@ -446,10 +447,10 @@ def test_symmetry_departure(binding, case32):
     assert abs(xtMy - ytMx) / ((xn * 52 * yn + yn * 52 * xn) * eps) <= 1.0
 
 
-@pytest.mark.parametrize("cfg", [None, "1", "6", "7", "8"])
+@pytest.mark.parametrize("cfg", [None, "1", "6", "7", "8", "9"])
 def test_fp32_vcycle_bitwise(oracle, binding, monkeypatch, cfg):
     """The FP32 V-cycle (autotuned, or one kernel configuration forced: rows per
-    thread 1, 4 contiguous, 2 and 4 interleaved) is bitwise the oracle's FP32
+    thread 1, 4 contiguous, 2 and 4 interleaved, shared-memory tiles) is bitwise the oracle's FP32
     V-cycle on the colour order with the last colour not repeated at the turn of
     each sweep."""
     if cfg is not None:
