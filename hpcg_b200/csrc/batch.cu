@@ -88,9 +88,9 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
     const int q = tl.start + threadIdx.x;
     if (q >= it.r1) continue;
     if (it.first)
-      gs_row<float, float, true, kPlain>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+      gs_row<float, float, true, kPlain, false>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
     else
-      gs_row<float, float, false, kPlain>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+      gs_row<float, float, false, kPlain, false>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
   }
 }
 
@@ -107,7 +107,8 @@ __global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict_
     const int f = it.tf[u];
     float sum = 0.0f;
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) sum += it.val[k * it.pitch + f] * __ldg(it.xf + it.col[k * it.pitch + f]);
+    for (int k = 0; k < kSlots; ++k)
+      sum += it.val[mat_index<float, false>(k, f, it.pitch)] * __ldg(it.xf + it.col[mat_index<float, false>(k, f, it.pitch)]);
     it.rc[it.tq[u]] = it.rf[f] - sum;
   }
 }
@@ -355,6 +356,10 @@ struct hpcg_b200_batch {
   hb::BScal* sc;
   hb::BScal* sc_host;
   hb::BCtl* ctl;
+  // slot-major FP32 values of every problem's levels, [problem * kMaxLevels + level]:
+  // the batched kernels walk tiles of 256 rows, for which the single-problem
+  // path's blocked FP32 layout was measured slower
+  std::vector<float*> val32;
   size_t bytes;
   cudaGraphExec_t graph;
 };
@@ -368,6 +373,12 @@ int alloc_copy(hpcg_b200_batch* B, void** dst, const void* src, size_t bytes) {
   HB_TRY(dev_alloc(dst, bytes, &B->bytes));
   HB_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
   return HPCG_B200_OK;
+}
+
+// FP32 copy of FP64 values, element for element (round to nearest).
+__global__ void k_narrow(float* __restrict__ dst, const double* __restrict__ src, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (float)src[i];
 }
 
 void tiles_of(std::vector<BTile>& tiles, int item, int r0, int r1) {
@@ -386,7 +397,7 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       const Level& L = B->probs[p]->lev[l];
       const int item = (int)gs.size();
       BGs it;
-      it.val = L.val32;
+      it.val = B->val32[p * kMaxLevels + l];
       it.col = L.col;
       it.pitch = L.pitch;
       it.rhs = L.r32;
@@ -413,7 +424,7 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       const Level& C = B->probs[p]->lev[l + 1];
       const int item = (int)res.size();
       BRes it;
-      it.val = L.val32;
+      it.val = B->val32[p * kMaxLevels + l];
       it.col = L.col;
       it.pitch = L.pitch;
       it.tf = L.tf;
@@ -557,6 +568,7 @@ void destroy(hpcg_b200_batch* B) {
   if (B->graph) cudaGraphExecDestroy(B->graph);
   void* v[] = {B->gs_items, B->res_items, B->tiles, B->vec, B->vtiles, B->vrange, B->partials, B->sc, B->ctl};
   for (void* q : v) cudaFree(q);
+  for (float* q : B->val32) cudaFree(q);
   if (B->sc_host) cudaFreeHost(B->sc_host);
   release_accounted(B->bytes);
   for (hpcg_b200_problem* p : B->probs) free_problem(p);
@@ -598,6 +610,19 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
     if (st == HPCG_B200_OK) {
       B->probs.push_back(p);
       st = prepare_f32(p);
+    }
+    for (int l = 0; l < kMaxLevels && st == HPCG_B200_OK; ++l) {
+      float* v = nullptr;
+      if (l < p->nlev) {
+        const Level& L = p->lev[l];
+        const int64_t cnt = (int64_t)kSlots * L.pitch;
+        st = dev_alloc((void**)&v, sizeof(float) * cnt, &B->bytes);
+        if (st == HPCG_B200_OK) {
+          k_narrow<<<grid_for(c, cnt, kThreads, 8), kThreads, 0, c->stream>>>(v, L.val, cnt);
+          if (cudaGetLastError() != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+        }
+      }
+      B->val32.push_back(v);
     }
   }
   if (st == HPCG_B200_OK) {

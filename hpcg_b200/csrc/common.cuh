@@ -31,6 +31,31 @@ constexpr int kColours = 8;
 constexpr int kMaxLevels = 4;
 constexpr uint64_t kMagic = 0x48504347b2000001ull;  // "HPCG" + version
 
+// Rows per block of the FP32 V-cycle's matrix copy (see mat_index).
+constexpr int kRowBlock32 = 1024;
+
+// Position of slot k of row q in a level's matrix arrays (values and columns).
+// The FP64 arrays are slot-major: 27 runs of `pitch` entries, so a warp's 32
+// rows read one coalesced run of a slot. The FP32 copy of the V-cycle (values
+// and its own columns) is stored in blocks of kRowBlock32 rows, each block
+// holding its 27 slots one after another: a warp still reads one coalesced run,
+// and an FP32 phase streams one run of memory per array instead of 27 far
+// apart. Measured at 512^3: the FP32 phases 17% faster than slot-major, while
+// the same blocking made the FP64 phases 20% slower.
+// BLK false: slot-major whatever the type (the batched path's own FP32 copy).
+template <typename T, bool BLK = (sizeof(T) == 4)>
+__host__ __device__ __forceinline__ int64_t mat_index(int k, int64_t q, int64_t pitch) {
+  if constexpr (BLK)
+    return ((q / kRowBlock32) * kSlots + k) * kRowBlock32 + (q % kRowBlock32);
+  else
+    return (int64_t)k * pitch + q;
+}
+
+// Entries of an FP32 matrix array of a level with `pitch` (whole blocks).
+inline int64_t blocked32_entries(int64_t pitch) {
+  return (pitch + kRowBlock32 - 1) / kRowBlock32 * kRowBlock32 * kSlots;
+}
+
 // Parity colours in sweep order. The injected (f2c) points, parity colour 0
 // (all coordinates even), are swept last in the forward sweep: swept first they
 // would overwrite the prolonged coarse correction before any other row reads
@@ -142,7 +167,8 @@ struct Level {
   int64_t pitch = 0;         // slot stride (>= n+next+1, multiple of 256)
   double* val = nullptr;     // [27][pitch]
   int* col = nullptr;        // [27][pitch]
-  float* val32 = nullptr;    // FP32 copy for the mixed-precision V-cycle (built on first use)
+  float* val32 = nullptr;    // FP32 copy for the mixed-precision V-cycle (built on first use), blocked
+  int* col32 = nullptr;      // its columns in the same blocked layout (mat_index<float>)
   int* new2old = nullptr;    // [n] colour row -> natural row
   int* old2new = nullptr;    // [n]
   int* f2c = nullptr;        // [n of next level] coarse colour row -> fine colour row

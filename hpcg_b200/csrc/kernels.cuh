@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
           for (int r = 0; r < R; ++r) {
             const int64_t q = q0 + 32 * r;
             if (q < r1) {
-              const T a = val[k * pitch + q];
-              const T xv = __ldg(x + col[k * pitch + q]);
+              const T a = val[mat_index<T>(k, q, pitch)];
+              const T xv = __ldg(x + col[mat_index<T>(k, q, pitch)]);
               sum[r] -= a * xv;
               if (k == kDiagSlot) xd[r] = xv;
             }
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
       for (int r = 0; r < R; ++r) {
         const int64_t q = q0 + 32 * r;
         if (q < r1) {
-          const T d = val[kDiagSlot * pitch + q];
+          const T d = val[mat_index<T>(kDiagSlot, q, pitch)];
           if (!FIRST) sum[r] += xd[r] * d;
           const T out = sum[r] / d;
           x[q] = out;
@@ -150,8 +150,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
       if (mask & (1u << k)) {
         T a[R];
         int c[R];
-        load_vec<T, R>(val + k * pitch + q0, a);
-        load_vec<int, R>(col + k * pitch + q0, c);
+        load_vec<T, R>(val + mat_index<T>(k, q0, pitch), a);
+        load_vec<int, R>(col + mat_index<T>(k, q0, pitch), c);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const T xv = __ldg(x + c[r]);
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_gs_phase(const T* _
       }
     }
     T d[R], out[R];
-    load_vec<T, R>(val + kDiagSlot * pitch + q0, d);
+    load_vec<T, R>(val + mat_index<T>(kDiagSlot, q0, pitch), d);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (!FIRST) sum[r] += xd[r] * d[r];
@@ -237,12 +237,12 @@ __global__ void __launch_bounds__(gs_tile_rows<T>(CFG)) k_gs_tile(const T* __res
       const int k = i / VCH, ch = i - k * VCH;
       const int row = b0 + ch * (16 / (int)sizeof(T));
       if (((mask >> k) & 1u || (FIRST && k == kDiagSlot)) && row < lim)
-        cp_async16(sval + (buf * kSlots + k) * TILE + ch * (16 / sizeof(T)), val + k * pitch + row);
+        cp_async16(sval + (buf * kSlots + k) * TILE + ch * (16 / sizeof(T)), val + mat_index<T>(k, row, pitch));
     }
     for (int i = threadIdx.x; i < kSlots * CCH; i += TILE) {
       const int k = i / CCH, ch = i - k * CCH;
       const int row = b0 + ch * 4;
-      if ((mask >> k) & 1u && row < lim) cp_async16(scol + (buf * kSlots + k) * TILE + ch * 4, col + k * pitch + row);
+      if ((mask >> k) & 1u && row < lim) cp_async16(scol + (buf * kSlots + k) * TILE + ch * 4, col + mat_index<T>(k, row, pitch));
     }
   };
   double acc = 0.0;
@@ -288,6 +288,21 @@ __global__ void __launch_bounds__(gs_tile_rows<T>(CFG)) k_gs_tile(const T* __res
   }
 }
 
+// The FP32 V-cycle's matrix: values rounded to FP32 and the columns, moved from
+// the slot-major FP64 arrays into the blocked layout of mat_index<float>.
+__global__ void k_block32(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                          float* __restrict__ val32, int* __restrict__ col32) {
+  const int64_t total = (int64_t)kSlots * pitch;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int k = (int)(i / pitch);
+    const int64_t q = i - (int64_t)k * pitch;
+    const int64_t d = mat_index<float>(k, q, pitch);
+    val32[d] = (float)val[i];
+    col32[d] = col[i];
+  }
+}
+
 // Natural-order (level-scheduled) Gauss-Seidel: the rows of one wavefront
 // ix + 2 iy + 4 iz = const, which only read rows of other wavefronts.
 template <typename T>
@@ -301,12 +316,12 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
     T xd = (T)0;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
-      const T a = val[k * pitch + q];
-      const T xv = x[col[k * pitch + q]];
+      const T a = val[mat_index<T>(k, q, pitch)];
+      const T xv = x[col[mat_index<T>(k, q, pitch)]];
       sum -= a * xv;
       if (k == kDiagSlot) xd = xv;
     }
-    const T d = val[kDiagSlot * pitch + q];
+    const T d = val[mat_index<T>(kDiagSlot, q, pitch)];
     sum += xd * d;
     x[q] = sum / d;
   }
@@ -356,8 +371,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
         int cl[kSlots];
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-          a[k] = __ldcs(val + k * pitch + q);
-          cl[k] = __ldcs(col + k * pitch + q);
+          a[k] = __ldcs(val + mat_index<T>(k, q, pitch));
+          cl[k] = __ldcs(col + mat_index<T>(k, q, pitch));
         }
         T xv[kSlots];
 #pragma unroll
@@ -368,8 +383,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
       } else {
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-          const T xv = __ldg(x + col[k * pitch + q]);
-          sum += val[k * pitch + q] * xv;
+          const T xv = __ldg(x + col[mat_index<T>(k, q, pitch)]);
+          sum += val[mat_index<T>(k, q, pitch)] * xv;
           if (k == kDiagSlot) xq = xv;
         }
       }
@@ -388,8 +403,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
           T sum = (T)0, xq = (T)0;
 #pragma unroll
           for (int k = 0; k < kSlots; ++k) {
-            const T xv = __ldg(x + col[k * pitch + q]);
-            sum += val[k * pitch + q] * xv;
+            const T xv = __ldg(x + col[mat_index<T>(k, q, pitch)]);
+            sum += val[mat_index<T>(k, q, pitch)] * xv;
             if (k == kDiagSlot) xq = xv;
           }
           y[q] = sum;
@@ -404,8 +419,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
       for (int k = 0; k < kSlots; ++k) {
         T a[R];
         int c[R];
-        load_vec<T, R>(val + k * pitch + q0, a);
-        load_vec<int, R>(col + k * pitch + q0, c);
+        load_vec<T, R>(val + mat_index<T>(k, q0, pitch), a);
+        load_vec<int, R>(col + mat_index<T>(k, q0, pitch), c);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const T xv = __ldg(x + c[r]);
@@ -447,8 +462,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
       int cl[kSlots];
 #pragma unroll
       for (int k = 0; k < kSlots; ++k) {
-        a[k] = __ldcs(val + k * pitch + f);
-        cl[k] = __ldcs(col + k * pitch + f);
+        a[k] = __ldcs(val + mat_index<T>(k, f, pitch));
+        cl[k] = __ldcs(col + mat_index<T>(k, f, pitch));
       }
       T xv[kSlots];
 #pragma unroll
@@ -457,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
       for (int k = 0; k < kSlots; ++k) sum += a[k] * xv[k];
     } else {
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) sum += val[k * pitch + f] * __ldg(xf + col[k * pitch + f]);
+      for (int k = 0; k < kSlots; ++k) sum += val[mat_index<T>(k, f, pitch)] * __ldg(xf + col[mat_index<T>(k, f, pitch)]);
     }
     rc[tq[t]] = rf[f] - sum;
   }
@@ -688,7 +703,7 @@ __global__ void __launch_bounds__(kThreads) k_adjoint_values(ColourGrid g, const
     double* o = out + (int64_t)i * kSlots;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
-      const int c = col[k * pitch + q];
+      const int c = col[mat_index<double>(k, q, pitch)];
       o[k] = c == n ? 0.0 : -(l * x[c]);
     }
   }

@@ -194,7 +194,7 @@ int free_problem(hpcg_b200_problem* p) {
   if (p->ctx) cudaStreamSynchronize(p->ctx->stream);
   for (int l = 0; l < kMaxLevels; ++l) {
     Level& L = p->lev[l];
-    void* ptrs[] = {L.val, L.col, L.val32, L.new2old, L.old2new, L.f2c, L.tf, L.tq, L.r, L.x, L.r32, L.x32,
+    void* ptrs[] = {L.val, L.col, L.val32, L.col32, L.new2old, L.old2new, L.f2c, L.tf, L.tq, L.r, L.x, L.r32, L.x32,
                     L.wave_rows};
     for (void* q : ptrs) dev_free(q);
     delete[] L.wave_start;
@@ -481,6 +481,8 @@ int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal) {
   if (L.val32) {  // the FP32 copy is rebuilt on next use
     dev_free(L.val32);
     L.val32 = nullptr;
+    dev_free(L.col32);
+    L.col32 = nullptr;
   }
   HB_CK(cudaStreamSynchronize(c->stream));
   return HPCG_B200_OK;
@@ -515,6 +517,8 @@ int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27
   if (L.val32) {
     dev_free(L.val32);
     L.val32 = nullptr;
+    dev_free(L.col32);
+    L.col32 = nullptr;
   }
   return HPCG_B200_OK;
 }

@@ -16,13 +16,18 @@ namespace {
 
 constexpr int kPerSm = 8;  // resident 256-thread blocks per SM targeted by grid-stride kernels
 
+// The column array a kernel of value type T reads: the FP32 V-cycle has its own,
+// in its blocked layout.
+template <typename T>
+const int* cols_of(const Level& L) {
+  return sizeof(T) == 4 ? L.col32 : L.col;
+}
+
 inline int red_blocks(const Context* c, int64_t n) {
   int b = grid_for(c, n, kThreads, kPerSm);
   return b > kRedBlocksMax / 2 ? kRedBlocksMax / 2 : b;
 }
 
-// dot != nullptr: the phase also writes its r'z block partials there (FP64
-// full-slot phases only; the grid is capped at kDotStride blocks).
 // The tiled phase (configuration 9): one block per SM-resident slot, walking
 // tiles of rows; its dynamic shared memory is enabled on first launch.
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK, bool DOT>
@@ -43,9 +48,11 @@ void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   const int64_t tiles = ((int64_t)r1 - a0 + rows - 1) / rows;
   int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms * per_sm);
   if (DOT && g > kDotStride) g = kDotStride;
-  k<<<g, rows, smem, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, dot);
+  k<<<g, rows, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot);
 }
 
+// dot != nullptr: the phase also writes its r'z block partials there (FP64
+// full-slot phases only; the grid is capped at kDotStride blocks).
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1>
 void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                double* dot = nullptr) {
@@ -66,12 +73,12 @@ void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, in
       auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK, cfg_sched(CFG), cfg_rows(CFG), true>;
       int g = grid_of(c, k, units);
       if (g > kDotStride) g = kDotStride;
-      k<<<g, kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, dot);
+      k<<<g, kThreads, 0, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot);
       return;
     }
   }
   auto k = k_gs_phase<T, TR, FIRST, CFG, CMASK>;
-  k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rhs, x, r0, r1, mask, nullptr);
+  k<<<grid_of(c, k, units), kThreads, 0, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, nullptr);
 }
 
 // A configuration with R contiguous rows per thread needs the row range to start
@@ -147,7 +154,7 @@ int spmv_launch_o(Context* c, const Level& L, const T* val, const T* x, T* y, do
   auto k = k_spmv<T, DOT, CFG, ORDER>;
   const int r = ORDER == 1 ? 1 : cfg_rows(CFG);
   const int g = grid_of(c, k, ((int64_t)L.n + r - 1) / r);
-  k<<<g, kThreads, 0, c->stream>>>(L.g, val, L.col, L.pitch, x, y, L.n, partials);
+  k<<<g, kThreads, 0, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials);
   return g;
 }
 
@@ -175,7 +182,7 @@ int spmv_dispatch(Context* c, const Level& L, const T* val, const T* x, T* y, do
 template <typename T, int CFG>
 void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   auto k = k_restrict<T, CFG>;
-  k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, L.col, L.pitch, rf, xf, L.tf, L.tq, rc, nc);
+  k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tf, L.tq, rc, nc);
 }
 
 template <typename T>
@@ -669,9 +676,13 @@ int ensure_f32(hpcg_b200_problem* P) {
   for (int l = 0; l < P->nlev; ++l) {
     Level& L = P->lev[l];
     if (!L.val32) {
-      HB_TRY(dev_alloc((void**)&L.val32, sizeof(float) * kSlots * L.pitch, &P->bytes));
-      const int64_t cnt = (int64_t)kSlots * L.pitch;
-      k_convert<float, double><<<grid_for(c, cnt, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.val32, L.val, cnt);
+      const int64_t cnt = blocked32_entries(L.pitch);
+      HB_TRY(dev_alloc((void**)&L.val32, sizeof(float) * cnt, &P->bytes));
+      HB_TRY(dev_alloc((void**)&L.col32, sizeof(int) * cnt, &P->bytes));
+      HB_CK(cudaMemsetAsync(L.val32, 0, sizeof(float) * cnt, c->stream));
+      HB_CK(cudaMemsetAsync(L.col32, 0, sizeof(int) * cnt, c->stream));
+      k_block32<<<grid_for(c, (int64_t)kSlots * L.pitch, kThreads, kPerSm), kThreads, 0, c->stream>>>(
+          L.val, L.col, L.pitch, L.val32, L.col32);
       HB_CK(cudaGetLastError());
     }
     if (!L.r32) {
