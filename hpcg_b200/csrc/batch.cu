@@ -88,9 +88,9 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
     const int q = tl.start + threadIdx.x;
     if (q >= it.r1) continue;
     if (it.first)
-      gs_row<float, float, true, kPlain, false>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+      gs_row<float, float, true, kPlain, 0>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
     else
-      gs_row<float, float, false, kPlain, false>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
+      gs_row<float, float, false, kPlain, 0>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
   }
 }
 
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict_
     float sum = 0.0f;
 #pragma unroll
     for (int k = 0; k < kSlots; ++k)
-      sum += it.val[mat_index<float, false>(k, f, it.pitch)] * __ldg(it.xf + it.col[mat_index<float, false>(k, f, it.pitch)]);
+      sum += it.val[mat_index<float, 0>(k, f, it.pitch)] * __ldg(it.xf + it.col[mat_index<float, 0>(k, f, it.pitch)]);
     it.rc[it.tq[u]] = it.rf[f] - sum;
   }
 }

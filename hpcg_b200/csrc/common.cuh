@@ -42,19 +42,18 @@ constexpr int kRowBlock32 = 1024;
 // and an FP32 phase streams one run of memory per array instead of 27 far
 // apart. Measured at 512^3: the FP32 phases 17% faster than slot-major, while
 // the same blocking made the FP64 phases 20% slower.
-// BLK false: slot-major whatever the type (the batched path's own FP32 copy).
-template <typename T, bool BLK = (sizeof(T) == 4)>
+// B: rows per block, 0 for slot-major (the default for FP64; the batched path's
+// FP32 copy and the multi-system path's FP64 copy choose their own).
+template <typename T, int B = (sizeof(T) == 4 ? kRowBlock32 : 0)>
 __host__ __device__ __forceinline__ int64_t mat_index(int k, int64_t q, int64_t pitch) {
-  if constexpr (BLK)
-    return ((q / kRowBlock32) * kSlots + k) * kRowBlock32 + (q % kRowBlock32);
+  if constexpr (B > 0)
+    return ((q / B) * kSlots + k) * B + (q % B);
   else
     return (int64_t)k * pitch + q;
 }
 
-// Entries of an FP32 matrix array of a level with `pitch` (whole blocks).
-inline int64_t blocked32_entries(int64_t pitch) {
-  return (pitch + kRowBlock32 - 1) / kRowBlock32 * kRowBlock32 * kSlots;
-}
+// Entries of a matrix array of a level with `pitch` in blocks of `rows` rows.
+inline int64_t blocked_entries(int64_t pitch, int rows) { return (pitch + rows - 1) / rows * rows * kSlots; }
 
 // Parity colours in sweep order. The injected (f2c) points, parity colour 0
 // (all coordinates even), are swept last in the forward sweep: swept first they

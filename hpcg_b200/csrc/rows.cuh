@@ -12,8 +12,8 @@ enum LoadSchedule : int { kPlain = 0, kStaged = 1 };
 // (diagonal included, slot order), sum += x_i a_ii, x_i = sum / a_ii. FIRST: x
 // enters as zero; the masked-out slots (and the diagonal) multiply a zero.
 // Returns the new x_i.
-// BLK: the matrix layout (mat_index).
-template <typename T, typename TR, bool FIRST, int SCHED, bool BLK = (sizeof(T) == 4)>
+// B: the matrix layout (rows per block of mat_index; 0 slot-major).
+template <typename T, typename TR, bool FIRST, int SCHED, int B = (sizeof(T) == 4 ? kRowBlock32 : 0)>
 __device__ __forceinline__ T gs_row(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
                                     const TR* __restrict__ rhs, T* x, int q, uint32_t mask) {
   T sum = (T)rhs[q];
@@ -24,8 +24,8 @@ __device__ __forceinline__ T gs_row(const T* __restrict__ val, const int* __rest
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       if (mask & (1u << k)) {
-        a[k] = __ldcs(val + mat_index<T, BLK>(k, q, pitch));
-        cl[k] = __ldcs(col + mat_index<T, BLK>(k, q, pitch));
+        a[k] = __ldcs(val + mat_index<T, B>(k, q, pitch));
+        cl[k] = __ldcs(col + mat_index<T, B>(k, q, pitch));
       }
     }
     T xv[kSlots];
@@ -43,14 +43,14 @@ __device__ __forceinline__ T gs_row(const T* __restrict__ val, const int* __rest
 #pragma unroll
     for (int k = 0; k < kSlots; ++k) {
       if (mask & (1u << k)) {
-        const T a = val[mat_index<T, BLK>(k, q, pitch)];
-        const T xv = __ldg(x + col[mat_index<T, BLK>(k, q, pitch)]);
+        const T a = val[mat_index<T, B>(k, q, pitch)];
+        const T xv = __ldg(x + col[mat_index<T, B>(k, q, pitch)]);
         sum -= a * xv;
         if (k == kDiagSlot) xd = xv;
       }
     }
   }
-  const T d = val[mat_index<T, BLK>(kDiagSlot, q, pitch)];
+  const T d = val[mat_index<T, B>(kDiagSlot, q, pitch)];
   if (!FIRST) sum += xd * d;
   const T out = sum / d;
   x[q] = out;

@@ -676,7 +676,7 @@ int ensure_f32(hpcg_b200_problem* P) {
   for (int l = 0; l < P->nlev; ++l) {
     Level& L = P->lev[l];
     if (!L.val32) {
-      const int64_t cnt = blocked32_entries(L.pitch);
+      const int64_t cnt = blocked_entries(L.pitch, kRowBlock32);
       HB_TRY(dev_alloc((void**)&L.val32, sizeof(float) * cnt, &P->bytes));
       HB_TRY(dev_alloc((void**)&L.col32, sizeof(int) * cnt, &P->bytes));
       HB_CK(cudaMemsetAsync(L.val32, 0, sizeof(float) * cnt, c->stream));

@@ -70,3 +70,23 @@ def test_cg_multi_zero_rhs_and_device_vectors(prob):
     assert ni[0] == 0 and nr0[0] == 0.0          # 0/0 > tol is false: no iterations, as CG.cpp:100
     assert torch.all(x[0] == 0)
     assert nr[1] / nr0[1] <= 1e-8 and ni[1] > 0
+
+
+def test_mg_multi_follows_value_changes(binding):
+    """After set_diagonal the multi-system V-cycle is still bitwise the
+    single-system one (both read the problem's current matrix)."""
+    P = binding.Problem.generate(32, 16, 24)
+    try:
+        n = P.nrow
+        r = np.random.default_rng(5).standard_normal((4, n))
+        for diag in (None, np.full(n, 30.0)):
+            if diag is not None:
+                P.set_diagonal(diag)
+            z = np.zeros((4, n))
+            P.ComputeMG_multi(r, z)
+            for j in range(4):
+                zj = np.zeros(n)
+                P.ComputeMG(np.ascontiguousarray(r[j]), zj)
+                assert np.array_equal(z[j], zj), (diag is None, j)
+    finally:
+        P.free()
