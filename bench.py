@@ -393,7 +393,9 @@ def gpu_launches_per_set(iters, nlevels=4):
     mg = 15 * 2 + 2  # per non-coarsest level: pre and post symmetric sweeps (15 colour phases each),
     # residual-restriction, prolongation
     per_mg = mg * (nlevels - 1) + 15
-    per_iter = per_mg + 2 + 1 + 2 + 2  # r'z + finalize, p update (k > 1), SpMV + finalize, x/r update + finalize
+    # r'z finalize (its partials come out of the post-smoother), p update (k > 1),
+    # SpMV + finalize, x/r update + finalize
+    per_iter = per_mg + 1 + 1 + 2 + 2
     first_iter_adjust = -1  # k = 1 copies z to p instead of the update kernel
     loads_stores = 2 + 1    # b and x gathered in, x scattered out
     preamble = 3            # SpMV, r = b - Ax with r'r, finalize
