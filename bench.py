@@ -533,13 +533,17 @@ def b200_arm(args, rank, world, local_rank):
         batch = batched(dev)
 
     line = None
+    tuning = [P.level_config(l) for l in range(4)]
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow)
         achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
+        gs_cfg = tuning[0]["gs"]
+        kernel = (f"k_gs_bulk<double,double,false> (level 0, configuration {gs_cfg})" if gs_cfg == 10 else
+                  f"k_gs_phase<double,double,false> (level 0, configuration {gs_cfg})")
         tr = committed_traffic()
         traffic = None
-        if tr and tr.get("n") == n and gs_launch:
+        if tr and tr.get("n") == n and tr.get("config") == gs_cfg and gs_launch:
             traffic = tr.get("bytes_per_launch")
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -559,7 +563,7 @@ def b200_arm(args, rank, world, local_rank):
             "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": traffic, "kernel": "k_gs_phase<double,double,false> (level 0)",
+                         "traffic": traffic, "kernel": kernel,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)" if peak_kind == "measured"
                          else peak_kind, "launches": gs_launch, "avg_launch_ms": round(gs_ms / max(gs_launch, 1), 4),
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
@@ -590,7 +594,6 @@ def b200_arm(args, rank, world, local_rank):
                 line["cpu_baseline"] = cpu_baseline(args)
             except Exception as ex:  # reported, not fatal
                 line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
-    tuning = [P.level_config(l) for l in range(4)]
     if line:
         line["config"]["autotuned"] = tuning
     P.free()

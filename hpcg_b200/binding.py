@@ -41,7 +41,7 @@ EXPORTS = (
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
-    "hpcg_b200_mg_f32", "hpcg_b200_last_error",
+    "hpcg_b200_mg_f32", "hpcg_b200_wait_selftest", "hpcg_b200_last_error",
 )
 
 
@@ -117,6 +117,7 @@ def lib():
         l.hpcg_b200_shard_dot.argtypes = [vp, vp, vp, C.POINTER(d)]
         l.hpcg_b200_shard_cg.argtypes = [vp, vp, vp, i, d, i, C.POINTER(i), C.POINTER(d), C.POINTER(d), vp]
         l.hpcg_b200_mg_f32.argtypes = [vp, vp, vp]
+        l.hpcg_b200_wait_selftest.argtypes = [i, d]
         l.hpcg_b200_last_error.restype = C.c_char_p
         for name in EXPORTS:
             f = getattr(l, name)
@@ -327,10 +328,10 @@ class Problem:
         return n.value, pitch.value, starts
 
     def level_config(self, level):
-        """Autotuner choices of a level: dict(gs, gs_first, gs32, spmv, spmv_order, tuned)."""
-        out = np.zeros(6, np.int32)
+        """Autotuner choices of a level: dict(gs, gs_first, gs32, spmv, spmv_order, tuned, gs32_first)."""
+        out = np.zeros(7, np.int32)
         _check(lib().hpcg_b200_level_config(self._h, level, out.ctypes.data), "hpcg_b200_level_config")
-        keys = ("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned")
+        keys = ("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned", "gs32_first")
         return dict(zip(keys, (int(v) for v in out)))
 
     def export_level(self, level):
@@ -522,6 +523,12 @@ def profile_read(kind, device=0):
     _check(lib().hpcg_b200_profile_read(device, kind, C.byref(ms), C.byref(ln), C.byref(rows)),
            "hpcg_b200_profile_read")
     return ms.value, ln.value, rows.value
+
+
+def wait_selftest(seconds, device=0):
+    """Status of hpcg_b200_wait_selftest: a device-side wait on a barrier that
+    nothing completes, given up after `seconds` (ERR_TIMEOUT expected)."""
+    return lib().hpcg_b200_wait_selftest(device, float(seconds))
 
 
 def ComputeDotProduct(n, x, y):

@@ -14,6 +14,7 @@
 //   - every colour-order vector has `pitch` >= n+next+1 entries, entry n+next always 0.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,8 +32,10 @@ constexpr int kColours = 8;
 constexpr int kMaxLevels = 4;
 constexpr uint64_t kMagic = 0x48504347b2000001ull;  // "HPCG" + version
 
-// Rows per block of the FP32 V-cycle's matrix copy (see mat_index).
-constexpr int kRowBlock32 = 1024;
+// Rows per block of the FP32 V-cycle's matrix copy (see mat_index): one tile of
+// the bulk-copy Gauss-Seidel phases, so that a tile's values and columns are
+// two runs of memory (two copies).
+constexpr int kRowBlock32 = 128;
 
 // Position of slot k of row q in a level's matrix arrays (values and columns).
 // The FP64 arrays are slot-major: 27 runs of `pitch` entries, so a warp's 32
@@ -40,8 +43,9 @@ constexpr int kRowBlock32 = 1024;
 // and its own columns) is stored in blocks of kRowBlock32 rows, each block
 // holding its 27 slots one after another: a warp still reads one coalesced run,
 // and an FP32 phase streams one run of memory per array instead of 27 far
-// apart. Measured at 512^3: the FP32 phases 17% faster than slot-major, while
-// the same blocking made the FP64 phases 20% slower.
+// apart. Measured at 512^3: the FP32 phases 17% faster than slot-major (as fast
+// with 128-row as with 1024-row blocks), while the same blocking made the FP64
+// phases 20% slower.
 // B: rows per block, 0 for slot-major (the default for FP64; the batched path's
 // FP32 copy and the multi-system path's FP64 copy choose their own).
 template <typename T, int B = (sizeof(T) == 4 ? kRowBlock32 : 0)>
@@ -158,6 +162,16 @@ struct RankGeom {
   int ipx = 0, ipy = 0, ipz = 0;
 };
 
+// Tensor maps of a level's FP64 matrix arrays for the bulk-copy Gauss-Seidel
+// phases: 2-D (x = row over the pitch, y = slot), box kBulkRows x 27.
+struct BulkMaps {
+  CUtensorMap val;
+  CUtensorMap col;
+  const void* val_ptr = nullptr;  // the arrays they describe
+  const void* col_ptr = nullptr;
+  bool ok = false;                // encoded (false: the encoder is unavailable)
+};
+
 struct Level {
   ColourGrid g;
   int n = 0;                 // rows
@@ -180,6 +194,7 @@ struct Level {
   // kernel configuration of this level's row kernels, chosen by the autotuner
   int gs_sched = 1;          // kernel configuration of the Gauss-Seidel phases (FP64)
   int gs_sched32 = 1;        // kernel configuration of the Gauss-Seidel phases (FP32 V-cycle)
+  int gs_first32 = 1;        // ... of its first-sweep phases
   int gs_first = 1;          // kernel configuration of the first-sweep phases (FP64)
   int mv_sched = 1;          // kernel configuration of SpMV / restriction
   int mv_order = 0;          // SpMV row order: 0 storage, 1 natural, 2 slab (see k_spmv)
@@ -188,6 +203,7 @@ struct Level {
   int* wave_rows = nullptr;  // colour-order rows sorted by ix + 2 iy + 4 iz
   int nwaves = 0;
   int* wave_start = nullptr; // host array [nwaves+1]
+  mutable BulkMaps* maps = nullptr;  // host; built on the first bulk-copy phase
 };
 
 struct Context;
@@ -287,6 +303,9 @@ struct Context {
   double prof_ms[kProfKinds] = {};
   long prof_launches[kProfKinds] = {};
   int64_t prof_rows[kProfKinds] = {};                 // rows processed by the timed launches
+  // fault word of the kernels with bounded waits (pinned, mapped): nonzero once a
+  // wait gave up; read and cleared by stream_sync
+  unsigned* fault = nullptr;
 };
 
 // Event pair around one launch of `kind` (no-op unless profiling); prof_end after the launch.
@@ -301,6 +320,9 @@ Context* context_for(int device);
 Context* current_context();
 // Grows the staging buffers to at least n entries.
 int ensure_stage(Context* c, size_t n);
+// Synchronises c's stream; HPCG_B200_ERR_TIMEOUT if a kernel's bounded wait gave
+// up since the last call (the fault word is cleared).
+int stream_sync(Context* c);
 
 // Device allocation accounted against the optional budget HPCG_B200_DEVICE_BUDGET (bytes).
 int dev_alloc(void** ptr, size_t bytes, size_t* counter);

@@ -81,6 +81,8 @@ Context* context_for(int device) {
   if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(Scalars));
   if (e == cudaSuccess) e = cudaMemset(c->scal, 0, sizeof(Scalars));
   if (e == cudaSuccess) e = cudaMallocHost(&c->scal_host, sizeof(Scalars));
+  if (e == cudaSuccess) e = cudaHostAlloc(&c->fault, sizeof(unsigned), cudaHostAllocMapped);
+  if (e == cudaSuccess) *c->fault = 0;
   if (e != cudaSuccess) {
     set_error("context set-up", e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -112,6 +114,17 @@ int ensure_stage(Context* c, size_t n) {
   c->stage_cap = 0;
   for (int i = 0; i < 3; ++i) HB_CK(cudaMalloc(&c->stage[i], n * sizeof(double)));
   c->stage_cap = n;
+  return HPCG_B200_OK;
+}
+
+int stream_sync(Context* c) {
+  HB_CK(cudaStreamSynchronize(c->stream));
+  volatile unsigned* f = c->fault;
+  if (f && *f) {
+    *f = 0;
+    set_error_text("a device-side wait gave up (bounded mbarrier wait in a Gauss-Seidel phase)");
+    return HPCG_B200_ERR_TIMEOUT;
+  }
   return HPCG_B200_OK;
 }
 

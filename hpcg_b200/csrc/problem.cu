@@ -198,6 +198,7 @@ int free_problem(hpcg_b200_problem* p) {
                     L.wave_rows};
     for (void* q : ptrs) dev_free(q);
     delete[] L.wave_start;
+    delete L.maps;
   }
   void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
   for (void* q : vs) dev_free(q);

@@ -10,9 +10,10 @@ namespace hb {
 
 constexpr int kThreads = 256;
 
-// Sum of v over the block, valid in thread 0. Fixed shuffle tree: deterministic.
+// Sum of v over the block (any whole number of warps up to 1024 threads), valid
+// in thread 0. Fixed shuffle tree: deterministic.
 __device__ __forceinline__ double block_sum(double v) {
-  __shared__ double warp_part[kThreads / 32];
+  __shared__ double warp_part[32];  // up to 1024 threads
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) warp_part[w] = v;
@@ -27,7 +28,7 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 __device__ __forceinline__ double block_max(double v) {
-  __shared__ double warp_part[kThreads / 32];
+  __shared__ double warp_part[32];  // up to 1024 threads
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) warp_part[w] = v;

@@ -165,7 +165,7 @@ int store_partial(Comm* C, int i, int nparts, bool max = false) {
 
 int read_scal(Context* c) {
   HB_CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
 
@@ -508,7 +508,7 @@ int hpcg_b200_shard_dot(hpcg_b200_comm* comm, const double* const* x, const doub
   double* out = C->use_nccl ? C->red + 1 : C->red + C->size;
   HB_TRY(reduce(C, kFinStore, out));
   HB_CK(cudaMemcpyAsync(result, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
 

@@ -51,12 +51,110 @@ void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   k<<<g, rows, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot);
 }
 
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link to the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// 2-D map of one slot-major array: x = row (pitch entries, the row stride), y =
+// slot (27); box kBulkRows x 27.
+bool encode_slot_major(CUtensorMap* m, CUtensorMapDataType type, size_t esize, const void* base, int64_t pitch) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)kSlots};
+  const cuuint64_t strides[1] = {(cuuint64_t)pitch * esize};
+  const cuuint32_t box[2] = {(cuuint32_t)kBulkRows, (cuuint32_t)kSlots};
+  const cuuint32_t elem[2] = {1, 1};
+  return fn(m, type, 2, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The level's FP64 tensor maps (built on first use, rebuilt if the arrays moved);
+// nullptr if they cannot be encoded.
+const BulkMaps* bulk_maps(const Level& L) {
+  if (!L.maps) L.maps = new BulkMaps();
+  BulkMaps* m = L.maps;
+  if (m->val_ptr != L.val || m->col_ptr != L.col) {
+    m->ok = encode_slot_major(&m->val, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), L.val, L.pitch) &&
+            encode_slot_major(&m->col, CU_TENSOR_MAP_DATA_TYPE_INT32, sizeof(int), L.col, L.pitch);
+    m->val_ptr = L.val;
+    m->col_ptr = L.col;
+  }
+  return m->ok ? m : nullptr;
+}
+
+// The bulk-copy pipeline (configuration 10): one block per SM (its shared
+// memory allows no second), at most one per tile. false: not launched (FP64
+// tensor maps unavailable).
+template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
+bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
+                    double* dot) {
+  auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT>;
+  constexpr int smem = gs_bulk_smem<T>();
+  static CUtensorMap none;  // the FP32 kernels take no maps
+  const CUtensorMap* tv = &none;
+  const CUtensorMap* tc = &none;
+  if constexpr (bulk_tensor_tile<T>()) {
+    const BulkMaps* m = bulk_maps(L);
+    if (!m) return false;
+    tv = &m->val;
+    tc = &m->col;
+  }
+  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
+  if (!(attr_set >> c->device & 1)) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set |= 1ull << c->device;
+  }
+  const int a0 = r0 & ~(kBulkRows - 1);
+  const int64_t tiles = ((int64_t)r1 - a0 + kBulkRows - 1) / kBulkRows;
+  int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+  if (DOT && g > kDotStride) g = kDotStride;
+  k<<<g, gs_bulk_threads<T>(), smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault,
+                                                  *tv, *tc);
+  return true;
+}
+
 // dot != nullptr: the phase also writes its r'z block partials there (FP64
 // full-slot phases only; the grid is capped at kDotStride blocks).
 template <typename T, typename TR, bool FIRST, int CFG, int64_t CMASK = -1>
 void gs_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                double* dot = nullptr) {
-  if constexpr (cfg_tiled(CFG)) {
+  if constexpr (CFG == kBulkCfg) {
+    if (r1 <= r0) return;
+    bool done = false;
+    if constexpr (!FIRST && CMASK < 0) {
+      // the full-slot phases with the mask compiled in: the 27 gathers of a row
+      // are issued back to back instead of behind one test each
+      if (mask == kAllSlots) {
+        if constexpr (sizeof(T) == 8) {
+          if (dot) done = gs_bulk_launch<T, TR, false, kAllSlots, true>(c, L, val, rhs, x, r0, r1, mask, dot);
+        }
+        if (!dot) done = gs_bulk_launch<T, TR, false, kAllSlots, false>(c, L, val, rhs, x, r0, r1, mask, nullptr);
+      } else {
+        done = gs_bulk_launch<T, TR, FIRST, CMASK, false>(c, L, val, rhs, x, r0, r1, mask, nullptr);
+      }
+    } else {
+      done = gs_bulk_launch<T, TR, FIRST, CMASK, false>(c, L, val, rhs, x, r0, r1, mask, nullptr);
+    }
+    if (!done) gs_launch<T, TR, FIRST, 1, CMASK>(c, L, val, rhs, x, r0, r1, mask, dot);  // no tensor maps here
+    return;
+  } else if constexpr (cfg_tiled(CFG)) {
     if (r1 <= r0) return;
     if constexpr (!FIRST && CMASK < 0 && sizeof(T) == 8) {
       if (dot) {
@@ -101,7 +199,8 @@ void gs_dispatch(Context* c, const Level& L, int cfg, const T* val, const TR* rh
     case 6: gs_launch<T, TR, FIRST, 6>(c, L, val, rhs, x, r0, r1, mask, dot); break;
     case 7: gs_launch<T, TR, FIRST, 7>(c, L, val, rhs, x, r0, r1, mask, dot); break;
     case 8: gs_launch<T, TR, FIRST, 8>(c, L, val, rhs, x, r0, r1, mask, dot); break;
-    default: gs_launch<T, TR, FIRST, 9>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    case 9: gs_launch<T, TR, FIRST, 9>(c, L, val, rhs, x, r0, r1, mask, dot); break;
+    default: gs_launch<T, TR, FIRST, 10>(c, L, val, rhs, x, r0, r1, mask, dot); break;
   }
 }
 
@@ -137,7 +236,8 @@ void gs_first_dispatch(Context* c, const Level& L, int cfg, const T* val, const 
       case 5: gs_first_const<T, TR, 5>(c, L, val, rhs, x, r0, r1, s); return;
       case 7: gs_first_const<T, TR, 7>(c, L, val, rhs, x, r0, r1, s); return;
       case 8: gs_first_const<T, TR, 8>(c, L, val, rhs, x, r0, r1, s); return;
-      default: gs_first_const<T, TR, 9>(c, L, val, rhs, x, r0, r1, s); return;
+      case 9: gs_first_const<T, TR, 9>(c, L, val, rhs, x, r0, r1, s); return;
+      default: gs_first_const<T, TR, 10>(c, L, val, rhs, x, r0, r1, s); return;
     }
   }
   gs_dispatch<T, TR, true>(c, L, cfg, val, rhs, x, r0, r1, mask);
@@ -165,10 +265,55 @@ int spmv_launch(Context* c, const Level& L, const T* val, const T* x, T* y, doub
   return spmv_launch_o<T, DOT, CFG, 0>(c, L, val, x, y, partials);
 }
 
+// Slab-order tiles of the bulk SpMV: slab runs of whole tiles, colour blocks on
+// even rows (the tensor copy's row coordinate times 8 bytes on 16).
+inline bool bulk_slab_ok(const Level& L) {
+  if (!slab_ok(L, kBulkRows)) return false;
+  for (int s = 0; s < kColours; ++s)
+    if (L.g.start[s] % 2) return false;
+  return true;
+}
+
+template <typename T, bool DOT, int ORDER>
+int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials,
+                     const BulkMaps* m) {
+  auto k = k_spmv_bulk<T, DOT, ORDER>;
+  constexpr int smem = gs_bulk_smem<T>();
+  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
+  if (!(attr_set >> c->device & 1)) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set |= 1ull << c->device;
+  }
+  const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sms));
+  k<<<g, gs_bulk_threads<T>(), smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault,
+                                                  m->val, m->col);
+  return g;
+}
+
+// SpMV configuration 7 (FP64): slab order where the tiles fit it, storage order
+// otherwise (the natural order has no tile form). Returns the grid, or 0 if it
+// cannot run (no tensor maps): the caller falls back.
+template <typename T, bool DOT>
+int spmv_bulk(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
+  if constexpr (sizeof(T) != 8) {
+    return 0;
+  } else {
+    const BulkMaps* m = bulk_maps(L);
+    if (!m) return 0;
+    if (L.mv_order == 2 && bulk_slab_ok(L)) return spmv_bulk_launch<T, DOT, 2>(c, L, val, x, y, partials, m);
+    return spmv_bulk_launch<T, DOT, 0>(c, L, val, x, y, partials, m);
+  }
+}
+
 // Launches y = A x on level L; returns the grid (the number of partials written when DOT).
 template <typename T, bool DOT>
 int spmv_dispatch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials) {
   switch (L.mv_sched) {
+    case kBulkMvCfg: {
+      const int g = spmv_bulk<T, DOT>(c, L, val, x, y, partials);
+      return g > 0 ? g : spmv_launch<T, DOT, 1>(c, L, val, x, y, partials);
+    }
     case 0: return spmv_launch<T, DOT, 0>(c, L, val, x, y, partials);
     case 1: return spmv_launch<T, DOT, 1>(c, L, val, x, y, partials);
     case 2: return spmv_launch<T, DOT, 2>(c, L, val, x, y, partials);
@@ -205,7 +350,7 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
                                     : (first ? kProfGsFirst : kProfGsFull);
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
-  const int cfg = sizeof(T) == 4 ? L.gs_sched32 : first ? L.gs_first : L.gs_sched;
+  const int cfg = sizeof(T) == 4 ? (first ? L.gs_first32 : L.gs_sched32) : first ? L.gs_first : L.gs_sched;
   if (first)
     gs_first_dispatch<T, TR>(c, L, cfg, val, rhs, x, r0, r1, s, first_mask(L.g, s));
   else
@@ -325,7 +470,38 @@ bool rtz_fused(const hpcg_b200_problem* P) { return P->symgs_mode == HPCG_B200_S
 // registers per thread) of the Gauss-Seidel phase and of the SpMV on scratch
 // vectors (Ap as x, zprev as right-hand side on level 0; the coarse r/x pair
 // otherwise) and keeps the fastest. Every configuration computes the same bits,
-// so the choice only affects speed. HPCG_B200_CONFIG=0..3 forces one.
+// so the choice only affects speed. HPCG_B200_CONFIG=n forces configuration n
+// (clamped to each kernel's range).
+// Measurement knob HPCG_B200_LEVEL_CONFIG: the configurations of every level
+// given instead of tuned, "gs,gs_first,spmv,spmv_order,gs32,gs32_first" per
+// level, levels separated by ';' (a profiler run then uses the plain run's
+// choices: under a profiler the tuner's timings are not the real ones).
+// Fills v[6] for level l; false if the variable is unset or has no such level.
+bool level_config_override(int l, int v[6]) {
+  const char* s = std::getenv("HPCG_B200_LEVEL_CONFIG");
+  if (!s || !*s) return false;
+  for (int i = 0; i < l; ++i) {
+    s = std::strchr(s, ';');
+    if (!s) return false;
+    ++s;
+  }
+  for (int i = 0; i < 6; ++i) {
+    char* end = nullptr;
+    const long x = std::strtol(s, &end, 10);
+    if (end == s) return false;
+    v[i] = (int)x;
+    s = end;
+    if (i < 5) {
+      if (*s != ',') return false;
+      ++s;
+    }
+  }
+  const int lim[6] = {kGsConfigs, kGsConfigs, kConfigs, 3, kGsConfigs, kGsConfigs};
+  for (int i = 0; i < 6; ++i)
+    if (v[i] < 0 || v[i] >= lim[i]) return false;
+  return true;
+}
+
 int autotune(hpcg_b200_problem* P) {
   Context* c = P->ctx;
   const char* force = std::getenv("HPCG_B200_CONFIG");
@@ -333,6 +509,14 @@ int autotune(hpcg_b200_problem* P) {
     Level& L = P->lev[l];
     if (L.tuned) continue;
     L.tuned = true;
+    int ov[6];
+    if (level_config_override(l, ov)) {
+      L.gs_sched = ov[0];
+      L.gs_first = ov[1];
+      L.mv_sched = ov[2];
+      L.mv_order = ov[3];
+      continue;
+    }
     if (force && *force) {
       const int f = std::atoi(force);
       L.gs_sched = L.gs_first = f < 0 ? 0 : f >= kGsConfigs ? kGsConfigs - 1 : f;
@@ -378,6 +562,7 @@ int autotune(hpcg_b200_problem* P) {
                                             first_mask(L.g, 4));
         }));
         for (int v = 0; v < kOrders && sched < kConfigs; ++v) {
+          if (sched == kBulkMvCfg && v == 1) continue;  // the bulk SpMV has no natural order
           L.mv_sched = sched;
           L.mv_order = v;
           // the variant CG runs: fused with the p'Ap partials
@@ -411,7 +596,7 @@ int finalize(Context* c, int nparts, int op, double* out = nullptr) {
 
 int read_scalars(Context* c) {
   HB_CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
 
@@ -647,7 +832,7 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
   *normr0_out = normr0;
   if (c->prof) HB_TRY(prof_flush(c));
   if (times) {
-    HB_CK(cudaStreamSynchronize(c->stream));
+    HB_TRY(stream_sync(c));
     double t_mg = 0, t_dw = 0, t_spmv = 0, t_up = 0;
     for (size_t i = 0; i + 4 < ev.size(); i += 5) {
       float a, b2, d, e;
@@ -692,10 +877,16 @@ int ensure_f32(hpcg_b200_problem* P) {
       HB_CK(cudaMemsetAsync(L.x32, 0, sizeof(float) * L.pitch, c->stream));
       // FP32 phases load half the bytes per instruction: tune them on their own
       // (on the level's FP32 work vectors, which every V-cycle rewrites)
+      int ov[6];
+      if (level_config_override(l, ov)) {
+        L.gs_sched32 = ov[4];
+        L.gs_first32 = ov[5];
+        continue;
+      }
       const char* force = std::getenv("HPCG_B200_CONFIG");
       if (force && *force) {
         const int f = std::atoi(force);
-        L.gs_sched32 = f < 0 ? 0 : f >= kGsConfigs ? kGsConfigs - 1 : f;
+        L.gs_sched32 = L.gs_first32 = f < 0 ? 0 : f >= kGsConfigs ? kGsConfigs - 1 : f;
         continue;
       }
       const int r0 = L.g.start[1], r1 = L.g.start[2];
@@ -703,25 +894,41 @@ int ensure_f32(hpcg_b200_problem* P) {
       cudaEvent_t e0, e1;
       HB_CK(cudaEventCreate(&e0));
       HB_CK(cudaEventCreate(&e1));
-      float t[kGsConfigs];
-      for (int cfg = 0; cfg < kGsConfigs; ++cfg) t[cfg] = 1e30f;
+      float t[kGsConfigs], tf[kGsConfigs];
+      for (int cfg = 0; cfg < kGsConfigs; ++cfg) t[cfg] = tf[cfg] = 1e30f;
+      auto time_it = [&](float& best_ms, auto&& launch) -> int {
+        HB_CK(cudaEventRecord(e0, c->stream));
+        launch();
+        HB_CK(cudaEventRecord(e1, c->stream));
+        HB_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        HB_CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) best_ms = ms;
+        return HPCG_B200_OK;
+      };
       for (int rep = 0; rep < 4; ++rep) {  // round-robin over the configurations, as in autotune
         for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
-          HB_CK(cudaEventRecord(e0, c->stream));
-          gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
-          HB_CK(cudaEventRecord(e1, c->stream));
-          HB_CK(cudaEventSynchronize(e1));
-          float ms = 0.f;
-          HB_CK(cudaEventElapsedTime(&ms, e0, e1));
-          if (ms < t[cfg]) t[cfg] = ms;
+          HB_TRY(time_it(t[cfg], [&] {
+            gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
+          }));
+          // the first-sweep phase of a middle sweep position, as in autotune
+          HB_TRY(time_it(tf[cfg], [&] {
+            gs_first_dispatch<float, float>(c, L, cfg, L.val32, L.r32, L.x32, L.g.start[4], L.g.start[5], 4,
+                                            first_mask(L.g, 4));
+          }));
         }
       }
-      float best = 1e30f;
-      for (int cfg = 0; cfg < kGsConfigs; ++cfg)
+      float best = 1e30f, best_first = 1e30f;
+      for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
         if (t[cfg] < best) {
           best = t[cfg];
           L.gs_sched32 = cfg;
         }
+        if (tf[cfg] < best_first) {
+          best_first = tf[cfg];
+          L.gs_first32 = cfg;
+        }
+      }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       HB_CK(cudaGetLastError());
@@ -921,7 +1128,7 @@ int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst
   k_gather<double><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n);
   HB_CK(cudaGetLastError());
   if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * L.n, cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
 
@@ -1059,6 +1266,16 @@ int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, in
   return HPCG_B200_OK;
 }
 
+int hpcg_b200_wait_selftest(int device, double seconds) {
+  if (!(seconds > 0.0 && seconds <= 2.0)) return HPCG_B200_ERR_ARG;
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  Setter dev(device);
+  k_wait_selftest<<<1, 32, 0, c->stream>>>((unsigned long long)(seconds * 1e9), c->fault);
+  HB_CK(cudaGetLastError());
+  return stream_sync(c);
+}
+
 int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   if (!config || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
@@ -1069,6 +1286,7 @@ int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config) {
   config[3] = L.mv_sched;
   config[4] = L.mv_order;
   config[5] = L.tuned ? 1 : 0;
+  config[6] = L.gs_first32;
   return HPCG_B200_OK;
 }
 
@@ -1108,7 +1326,7 @@ int hpcg_b200_waxpby(int n, double alpha, const double* x, double beta, const do
   k_waxpby<false><<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, alpha, dx, beta, dy, dw, nullptr);
   HB_CK(cudaGetLastError());
   if (!wdev) HB_CK(cudaMemcpyAsync(w, dw, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
 

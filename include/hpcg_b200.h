@@ -273,11 +273,19 @@ int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64
 int hpcg_b200_export_level(const hpcg_b200_problem* p, int level, int* new2old, int* cols, double* vals,
                            int* f2c);
 
-/* The autotuner's choices for one level (6 ints): kernel configuration of the
+/* The autotuner's choices for one level (7 ints): kernel configuration of the
  * Gauss-Seidel phases, of the first-sweep phases, of the FP32 phases, of the
- * SpMV/restriction, the SpMV row order (0 storage, 1 natural, 2 slab), and
- * whether the level has been tuned yet (tuning happens on first use). */
+ * SpMV/restriction, the SpMV row order (0 storage, 1 natural, 2 slab), whether
+ * the level has been tuned yet (tuning happens on first use), and the
+ * configuration of the FP32 first-sweep phases. */
 int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config);
+
+/* Check of the device-side bounded wait used by the bulk-copy Gauss-Seidel
+ * phases (configuration 10): one thread waits `seconds` (0 < seconds <= 2) on
+ * an mbarrier that nothing completes, gives up, records the fault and returns.
+ * Returns HPCG_B200_ERR_TIMEOUT (the expected outcome) with the device context
+ * still usable. No reference counterpart: test support for the wait path. */
+int hpcg_b200_wait_selftest(int device, double seconds);
 
 /* The row order the library uses for an (nx, ny, nz) grid, computed on the host
  * (no GPU needed): new2old[q] = natural row of colour-order row q, and

@@ -164,6 +164,51 @@ def test_spmv_every_row_order_bitwise(oracle, binding, monkeypatch, order):
         D.free()
 
 
+@pytest.mark.parametrize("dims,order", [((32, 16, 24), 2), ((32, 24, 48), 0), ((32, 24, 48), 2)])
+def test_bulk_spmv_and_phases_vs_oracle(oracle, binding, monkeypatch, dims, order):
+    """SpMV configuration 7 (tiles streamed by tensor copies; slab order where the
+    slab runs split into 128-row tiles, 32 x 16 x 24, else storage order) and
+    the bulk Gauss-Seidel phases on every level, set through
+    HPCG_B200_LEVEL_CONFIG: SpMV bitwise the reference's, CG (fused p'Ap and
+    r'z partials) as the oracle's on the colour order."""
+    cfg = ";".join(["10,10,7,%d,10,10" % order] * 4)
+    monkeypatch.setenv("HPCG_B200_LEVEL_CONFIG", cfg)
+    P = oracle.generate(*dims)
+    D = binding.Problem.optimize(levels_of(P))
+    try:
+        x = np.random.default_rng(order).standard_normal(P.levels[0].n)
+        y = np.zeros_like(x)
+        D.ComputeSPMV(x, y)  # first use: the configurations are set here
+        for l in range(4):
+            c = D.level_config(l)
+            assert (c["gs"], c["gs_first"], c["spmv"], c["spmv_order"]) == (10, 10, 7, order)
+        assert np.array_equal(y, oracle.spmv(P.levels[0], x))
+        perms = perms_of(binding, P)
+        PL = oracle.permute(P.levels, perms)
+        for k in (1, 10, 30):
+            xs = np.zeros(P.levels[0].n)
+            ni, nr, nr0 = D.CG(P.b, xs, k, 0.0, True)
+            xo, nio, nro, nr0o, _ = oracle.cg(PL, P.b[perms[0]], np.zeros(P.levels[0].n), k, 0.0,
+                                              skip=skip_of(binding, P))
+            assert ni == nio == k
+            hist_close([nr / nr0], [nro / nr0o])
+    finally:
+        D.free()
+
+
+def test_level_config_override_rejects_bad_values(binding, monkeypatch):
+    """A malformed or out-of-range HPCG_B200_LEVEL_CONFIG is ignored (the level is tuned)."""
+    monkeypatch.setenv("HPCG_B200_LEVEL_CONFIG", "10,5,99,2,10,5")
+    D = binding.Problem.generate(16)
+    try:
+        x = np.zeros(16 ** 3)
+        D.ComputeSPMV(x, x.copy())
+        c = D.level_config(0)
+        assert c["tuned"] == 1 and c["spmv"] < 8
+    finally:
+        D.free()
+
+
 def test_spmv_matches_reference_golden(oracle, case16):
     P, D, _, _ = case16
     g = np.load(os.path.join(GOLD, "golden_16.npz"))
@@ -220,11 +265,11 @@ def test_mg_colour_bitwise(oracle, binding, case32):
     assert np.max(np.abs(z - ref)) <= 1e-14 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("cfg", [str(c) for c in range(10)])
+@pytest.mark.parametrize("cfg", [str(c) for c in range(11)])
 def test_mg_colour_every_config_bitwise(oracle, binding, monkeypatch, cfg):
     """Every kernel configuration of the phases (load schedules, registers, 2 or 4
     contiguous rows with vector loads, 2 or 4 interleaved rows, shared-memory
-    tiles filled by asynchronous copies) computes the same
+    tiles filled by asynchronous copies, the bulk-copy pipeline) computes the same
     V-cycle bits; the coarsest level (3 x 2 x 5) has colour blocks of odd sizes
     starting off multiples of 4."""
     monkeypatch.setenv("HPCG_B200_CONFIG", cfg)
@@ -447,10 +492,11 @@ def test_symmetry_departure(binding, case32):
     assert abs(xtMy - ytMx) / ((xn * 52 * yn + yn * 52 * xn) * eps) <= 1.0
 
 
-@pytest.mark.parametrize("cfg", [None, "1", "6", "7", "8", "9"])
+@pytest.mark.parametrize("cfg", [None, "1", "6", "7", "8", "9", "10"])
 def test_fp32_vcycle_bitwise(oracle, binding, monkeypatch, cfg):
     """The FP32 V-cycle (autotuned, or one kernel configuration forced: rows per
-    thread 1, 4 contiguous, 2 and 4 interleaved, shared-memory tiles) is bitwise the oracle's FP32
+    thread 1, 4 contiguous, 2 and 4 interleaved, shared-memory tiles, bulk-copy
+    pipeline) is bitwise the oracle's FP32
     V-cycle on the colour order with the last colour not repeated at the turn of
     each sweep."""
     if cfg is not None:
@@ -573,3 +619,57 @@ def test_graph_loop_equals_stream_loop(case32):
         assert ng == ne, (max_iter, tol, prec)
         assert np.array_equal(xg, xe)
         assert times[0] > 0.0
+
+
+@pytest.mark.parametrize("cfg", ["9", "10"])
+def test_cg_forced_config_vs_oracle(oracle, binding, monkeypatch, cfg):
+    """CG with the phases forced to a configuration that runs its own kernel
+    (shared-memory tiles, bulk-copy pipeline), r'z from the post-smoother's fused
+    partials: history and x as the oracle's CG on the colour order; the graph
+    loop equals the stream loop."""
+    monkeypatch.setenv("HPCG_B200_CONFIG", cfg)
+    P = oracle.generate(32)
+    D = binding.Problem.optimize(levels_of(P))
+    try:
+        perms = perms_of(binding, P)
+        PL = oracle.permute(P.levels, perms)
+        b = P.b[perms[0]]
+        for k in (1, 10, 50):
+            x = np.zeros(32 ** 3)
+            ni, nr, nr0 = D.CG(P.b, x, k, 0.0, True)
+            assert D.level_config(0)["gs"] == int(cfg)
+            xo, nio, nro, nr0o, _ = oracle.cg(PL, b, np.zeros(32 ** 3), k, 0.0, skip=skip_of(binding, P))
+            assert ni == nio == k
+            hist_close([nr / nr0], [nro / nr0o])
+            xn = np.empty_like(xo)
+            xn[perms[0]] = xo
+            assert np.max(np.abs(x - xn)) <= 1e-10 * max(np.max(np.abs(xn)), 1.0)
+        xg = np.zeros(32 ** 3)
+        ng = D.CG(P.b, xg, 20, 0.0, True)
+        xe = np.zeros(32 ** 3)
+        ne = D.CG(P.b, xe, 20, 0.0, True, times=np.zeros(10))
+        assert ng == ne and np.array_equal(xg, xe)
+    finally:
+        D.free()
+
+
+def test_bounded_wait_gives_up_and_context_survives(oracle, binding, case16):
+    """The device-side wait of the bulk-copy phases ends by itself: waiting on an
+    mbarrier that nothing completes returns HPCG_B200_ERR_TIMEOUT after the
+    limit, and the same context then runs the V-cycle bit for bit."""
+    import time
+    t0 = time.perf_counter()
+    st = binding.wait_selftest(0.25)
+    dt = time.perf_counter() - t0
+    assert st == binding.ERR_TIMEOUT
+    assert 0.2 <= dt < 30.0
+    assert "gave up" in binding.last_error()
+    P, D, perms, PL = case16
+    r = np.random.default_rng(11).standard_normal(16 ** 3)
+    z = np.zeros_like(r)
+    D.ComputeMG(r, z)
+    exp = np.empty_like(z)
+    exp[perms[0]] = oracle.mg(PL, r[perms[0]], skip=skip_of(binding, P))
+    assert np.array_equal(z, exp)
+    with pytest.raises(binding.HpcgError):
+        binding._check(binding.lib().hpcg_b200_wait_selftest(0, 5.0), "wait_selftest")

@@ -168,6 +168,36 @@ def test_cg_colour_vs_permuted_reference(run_colour_ref):
         assert abs(nr / nr0 - s) <= 1e-10 * max(s, 1e-9), (it, nr / nr0, s)
 
 
+def test_bulk_config_ranks_vs_permuted_reference(oracle, binding, monkeypatch):
+    """The bulk-copy pipeline (configuration 10) on ranks with halos (3 x 1 x 2,
+    odd coarse blocks): colour MG as the reference run on the colour-permuted
+    ranks, and the CG history as before."""
+    monkeypatch.setenv("HPCG_B200_CONFIG", "10")
+    R = Run(oracle, binding, DECOMPS[2])
+    try:
+        n2o = R.perms()[0]
+        perms = R.perms()
+        for r in range(R.size):
+            R.ref.permute(r, perms)
+        rs = rand_vectors(R, 12)
+        zs = [np.zeros(R.n) for _ in rs]
+        R.comm.ComputeMG(rs, zs)
+        assert R.P[0].level_config(0)["gs"] == 10
+        ref = R.ref.mg([r[n2o] for r in rs])
+        for a, bc in zip(zs, ref):
+            b = np.empty_like(bc)
+            b[n2o] = bc
+            assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b))
+        bs = [p.get_rhs() for p in R.P]
+        xs = [np.zeros(R.n) for _ in bs]
+        ni, nr, nr0 = R.comm.CG(bs, xs, 10, 0.0)
+        xr, ni_r, nr_r, nr0_r = R.ref.cg(10, 0.0)
+        s_ = nr_r / nr0_r
+        assert ni == ni_r == 10 and abs(nr / nr0 - s_) <= 1e-10 * max(s_, 1e-9)
+    finally:
+        R.close()
+
+
 def test_cg_converges_and_tolerance_stop(run):
     bs = [p.get_rhs() for p in run.P]
     xs = [np.zeros(run.n) for _ in bs]
