@@ -323,6 +323,9 @@ int ensure_stage(Context* c, size_t n);
 // Synchronises c's stream; HPCG_B200_ERR_TIMEOUT if a kernel's bounded wait gave
 // up since the last call (the fault word is cleared).
 int stream_sync(Context* c);
+// The level's FP64 tensor maps for the bulk-copy kernels (built on first use,
+// rebuilt if the arrays moved); nullptr if they cannot be encoded.
+const BulkMaps* bulk_maps(const Level& L);
 
 // Device allocation accounted against the optional budget HPCG_B200_DEVICE_BUDGET (bytes).
 int dev_alloc(void** ptr, size_t bytes, size_t* counter);

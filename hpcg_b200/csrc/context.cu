@@ -3,6 +3,7 @@
 #include <cstdlib>
 #include <mutex>
 
+#include "bulk.cuh"
 #include "common.cuh"
 
 namespace hb {
@@ -115,6 +116,54 @@ int ensure_stage(Context* c, size_t n) {
   for (int i = 0; i < 3; ++i) HB_CK(cudaMalloc(&c->stage[i], n * sizeof(double)));
   c->stage_cap = n;
   return HPCG_B200_OK;
+}
+
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link to the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// 2-D map of one slot-major array: x = row (pitch entries, the row stride), y =
+// slot (27); box kBulkRows x 27.
+static bool encode_slot_major(CUtensorMap* m, CUtensorMapDataType type, size_t esize, const void* base, int64_t pitch) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)kSlots};
+  const cuuint64_t strides[1] = {(cuuint64_t)pitch * esize};
+  const cuuint32_t box[2] = {(cuuint32_t)kBulkRows, (cuuint32_t)kSlots};
+  const cuuint32_t elem[2] = {1, 1};
+  return fn(m, type, 2, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The level's FP64 tensor maps (built on first use, rebuilt if the arrays moved);
+// nullptr if they cannot be encoded.
+const BulkMaps* bulk_maps(const Level& L) {
+  if (!L.maps) L.maps = new BulkMaps();
+  BulkMaps* m = L.maps;
+  if (m->val_ptr != L.val || m->col_ptr != L.col) {
+    m->ok = encode_slot_major(&m->val, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), L.val, L.pitch) &&
+            encode_slot_major(&m->col, CU_TENSOR_MAP_DATA_TYPE_INT32, sizeof(int), L.col, L.pitch);
+    m->val_ptr = L.val;
+    m->col_ptr = L.col;
+  }
+  return m->ok ? m : nullptr;
 }
 
 int stream_sync(Context* c) {

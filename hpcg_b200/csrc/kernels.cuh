@@ -6,6 +6,7 @@
 // differ (fixed-shape tree instead of a serial loop, deterministic run to run).
 #pragma once
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
 #include "rows.cuh"
@@ -293,138 +294,6 @@ __global__ void __launch_bounds__(gs_tile_rows<T>(CFG)) k_gs_tile(const T* __res
   }
 }
 
-// ---- bulk-copy pipelined Gauss-Seidel phase (configuration 10) --------------
-// A persistent block per SM walks tiles of kBulkRows rows of the phase. A
-// producer warp streams each tile's matrix (all 27 slots' values and columns)
-// into shared-memory stages with two asynchronous copies by the SM's copy unit:
-// no thread holds the stream in registers, and the stream does not wait on the
-// row arithmetic. A stage's "full" mbarrier completes when all its bytes have
-// landed (transaction count). Groups of kBulkRows consumer threads take the
-// block's tiles in turn (tile i to group i mod G), one row per thread: they
-// gather x from global memory through the columns on chip, write the row and
-// arrive on the stage's "empty" mbarrier, after which the producer refills it.
-// Each group owns a ring of kBulkRing stages (the group's k-th tile uses stage
-// k mod kBulkRing of its ring), so a stage's fills are consumed in order by one
-// group and no wait on a barrier can start more than one phase early (an
-// mbarrier parity wait cannot tell phase n from phase n - 2). The arithmetic is
-// gs_row's in slot order: the same bits as every other configuration. The
-// first sweep copies all slots too (it reads about half), so the autotuner
-// usually keeps another configuration for it.
-// Every wait gives up after kBulkWaitNs of global time: the thread then sets
-// the context's fault word (host-mapped; stream_sync turns it into
-// HPCG_B200_ERR_TIMEOUT) and stops; before its block exits the producer waits,
-// bounded again, for the copies it issued.
-// Tiles start on multiples of kBulkRows (r0 rounded down); rows outside
-// [r0, r1) are copied and not computed. The last tile ends at r1 rounded up to
-// kBulkRows, which is within the pitch (a multiple of 256 above n).
-constexpr int kBulkRows = 128;                             // rows per tile = threads per consumer group
-constexpr int kBulkRing = 2;                               // stages per consumer group
-constexpr unsigned long long kBulkWaitNs = 1000000000ull;  // 1 s per wait
-// consumer groups: FP64 stages (41.5 KB) allow two groups' rings in shared memory, FP32 ones (27 KB) three
-template <typename T>
-__host__ __device__ constexpr int gs_bulk_groups() {
-  return sizeof(T) == 8 ? 2 : 3;
-}
-template <typename T>
-__host__ __device__ constexpr int gs_bulk_threads() {
-  return 32 + gs_bulk_groups<T>() * kBulkRows;  // producer warp + consumers
-}
-template <typename T>
-__host__ __device__ constexpr int gs_bulk_stages() {
-  return gs_bulk_groups<T>() * kBulkRing;
-}
-// How a tile reaches shared memory. FP32 (blocked copy with kRowBlock32 ==
-// kBulkRows): a tile is one block of the layout, its values one run of memory
-// and its columns another, two bulk copies. FP64 (slot-major): one 2-D tensor
-// copy per array (box kBulkRows rows x 27 slots of a map with the pitch as row
-// stride). Either way two requests per tile: the SM's copy unit takes a roughly
-// fixed time per request, so 2 x 27 per-slot copies of 0.5-1 KB capped the
-// phases near 4 TB/s.
-template <typename T>
-__host__ __device__ constexpr bool bulk_whole_tile() {
-  return sizeof(T) == 4 && kRowBlock32 == kBulkRows;
-}
-template <typename T>
-__host__ __device__ constexpr bool bulk_tensor_tile() {
-  return sizeof(T) == 8;
-}
-template <typename T>
-__host__ __device__ constexpr int gs_bulk_stage_bytes() {
-  return kSlots * kBulkRows * (int)(sizeof(T) + sizeof(int));
-}
-// stages + barriers + slack to align the stages to 128 bytes (tensor copies)
-template <typename T>
-__host__ __device__ constexpr int gs_bulk_smem() {
-  return gs_bulk_stages<T>() * gs_bulk_stage_bytes<T>() + 2 * gs_bulk_stages<T>() * (int)sizeof(uint64_t) + 128;
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-// makes the initialised barriers visible to the other threads and to the bulk-copy unit
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// true once the barrier's phase of the given parity has completed; false after limit_ns
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
-                                          unsigned long long limit_ns = kBulkWaitNs) {
-  if (mbar_test(bar, parity)) return true;
-  const unsigned long long t0 = global_ns();
-  while (!mbar_test(bar, parity))
-    if (global_ns() - t0 > limit_ns) return false;
-  return true;
-}
-// global -> shared bulk copy completing on `bar`, streamed with an evict-first L2 policy
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar, uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
-      : "memory");
-}
-// global -> shared 2-D tensor tile (box of the map at column x, row y) completing on `bar`
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar,
-                                            uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
-      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_addr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar)), "l"(policy)
-      : "memory");
-}
-__device__ __forceinline__ uint64_t evict_first_policy() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ void record_fault(unsigned* fault, unsigned code) {
-  *(volatile unsigned*)fault = code;
-  __threadfence_system();
-}
-
 // Check of the bounded wait itself: thread 0 waits on a barrier that nothing
 // arrives on; after limit_ns it records fault code 4 and the kernel returns.
 __global__ void k_wait_selftest(unsigned long long limit_ns, unsigned* fault) {
@@ -437,99 +306,9 @@ __global__ void k_wait_selftest(unsigned long long limit_ns, unsigned* fault) {
   if (threadIdx.x == 0 && !mbar_wait(&bar, 0, limit_ns)) record_fault(fault, 4);
 }
 
-// The producer/consumer pipeline of the bulk-copy kernels, run by the whole
-// block: the block's tiles are blockIdx.x, + gridDim.x, ... below ntiles; tile
-// `tile` holds rows first_row(tile) .. + kBulkRows. Each consumer thread calls
-// row(q0, sv, sc, t) for row t of every tile of its group, with the tile's
-// values sv[k * kBulkRows + t] and columns sc[k * kBulkRows + t] on chip.
-template <typename T, typename FirstRow, typename RowFn>
-__device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
-                                           int ntiles, FirstRow first_row, RowFn row, unsigned* fault,
-                                           const CUtensorMap& tm_val, const CUtensorMap& tm_col) {
-  constexpr int G = gs_bulk_groups<T>();
-  constexpr int S = gs_bulk_stages<T>();
-  constexpr int SB = gs_bulk_stage_bytes<T>();
-  constexpr int VB = kSlots * kBulkRows * (int)sizeof(T);  // value bytes of a stage (columns follow)
-  static_assert(bulk_whole_tile<T>() || bulk_tensor_tile<T>(), "a tile must arrive in two copies");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * SB);
-  uint64_t* empty = full + S;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kBulkRows);
-    }
-    mbar_init_fence();
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5;
-  if (warp == 0) {
-    // the producer warp: lane 0 waits for a free stage and posts the byte
-    // count, then lanes 0 and 1 issue the tile's two copies
-    const int lane = threadIdx.x;
-    const uint64_t policy = evict_first_policy();
-    int last[S];  // last fill issued into each stage (-1: none)
-#pragma unroll
-    for (int s = 0; s < S; ++s) last[s] = -1;
-    int i = 0;  // block-local tile number: group i % G, its (i / G)-th tile
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-      const int kg = i / G;
-      const int s = (i % G) * kBulkRing + kg % kBulkRing, use = kg / kBulkRing;
-      int ok = 1;
-      if (lane == 0) {
-        if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) {
-          record_fault(fault, 1);
-          ok = 0;
-        } else {
-          mbar_expect_tx(&full[s], SB);
-        }
-      }
-      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
-      const int64_t q0 = first_row(tile);
-      T* sv = reinterpret_cast<T*>(smem + s * SB);
-      int* sc = reinterpret_cast<int*>(smem + s * SB + VB);
-      if constexpr (bulk_whole_tile<T>()) {
-        // the tile is one block of the layout: all slots' values in one run, all columns in another
-        if (lane == 0) bulk_g2s(sv, val + mat_index<T>(0, q0, pitch), VB, &full[s], policy);
-        if (lane == 1) bulk_g2s(sc, col + mat_index<T>(0, q0, pitch), kSlots * kBulkRows * sizeof(int), &full[s], policy);
-      } else {
-        // rows q0 .. q0 + kBulkRows of all 27 slots, [slot][row] in shared memory
-        if (lane == 0) tma_load_2d(sv, &tm_val, (int)q0, 0, &full[s], policy);
-        if (lane == 1) tma_load_2d(sc, &tm_col, (int)q0, 0, &full[s], policy);
-      }
-#pragma unroll
-      for (int u = 0; u < S; ++u)
-        if (u == s) last[u] = use;
-    }
-    // no copy may still be landing when the block exits: the last fill of
-    // every stage has completed (consumed or not)
-    if (lane == 0) {
-#pragma unroll
-      for (int s = 0; s < S; ++s)
-        if (last[s] >= 0 && !mbar_wait(&full[s], last[s] & 1)) record_fault(fault, 2);
-    }
-    __syncwarp();
-  } else {
-    const int g = (warp - 1) / (kBulkRows / 32);   // consumer group
-    const int t = (threadIdx.x - 32) % kBulkRows;  // row of the tile
-    int kg = 0;                                    // the group's tile count
-    for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles; tile += G * gridDim.x, ++kg) {
-      const int s = g * kBulkRing + kg % kBulkRing, use = kg / kBulkRing;
-      if (!mbar_wait(&full[s], use & 1)) {
-        record_fault(fault, 3);
-        break;
-      }
-      row(first_row(tile), reinterpret_cast<const T*>(smem + s * SB),
-          reinterpret_cast<const int*>(smem + s * SB + VB), t);
-      mbar_arrive(&empty[s]);
-    }
-  }
-}
-
 // Gauss-Seidel colour phase over rows [r0, r1) through the pipeline (configuration 10).
 template <typename T, typename TR, bool FIRST, int64_t CMASK = -1, bool DOT = false>
-__global__ void __launch_bounds__(gs_bulk_threads<T>(), 1) k_gs_bulk(const T* __restrict__ val,
+__global__ void __launch_bounds__(GsShape<T>::threads, 1) k_gs_bulk(const T* __restrict__ val,
                                                                      const int* __restrict__ col, int64_t pitch,
                                                                      const TR* __restrict__ rhs, T* x, int r0,
                                                                      int r1, uint32_t mask_arg,
@@ -540,7 +319,7 @@ __global__ void __launch_bounds__(gs_bulk_threads<T>(), 1) k_gs_bulk(const T* __
   const int a0 = r0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T>(
+  bulk_tiles<T, GsShape<T>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t) {
         const int64_t q = q0 + t;
@@ -729,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
 // tiles and colour blocks that start on an even row (checked on the host).
 // Partials: one per block.
 template <typename T, bool DOT, int ORDER>
-__global__ void __launch_bounds__(gs_bulk_threads<T>(), 1) k_spmv_bulk(ColourGrid g, const T* __restrict__ val,
+__global__ void __launch_bounds__(SpmvShape<T>::threads, 1) k_spmv_bulk(ColourGrid g, const T* __restrict__ val,
                                                                        const int* __restrict__ col, int64_t pitch,
                                                                        const T* __restrict__ x, T* __restrict__ y,
                                                                        int n, double* __restrict__ partials,
@@ -739,7 +518,7 @@ __global__ void __launch_bounds__(gs_bulk_threads<T>(), 1) k_spmv_bulk(ColourGri
   static_assert(ORDER == 0 || ORDER == 2, "storage or slab order");
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T>(
+  bulk_tiles<T, SpmvShape<T>>(
       val, col, pitch, ntiles,
       [&](int tile) {
         return ORDER == 2 ? slab_row(g, (int64_t)tile * kBulkRows) : (int64_t)tile * kBulkRows;

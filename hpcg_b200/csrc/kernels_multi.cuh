@@ -7,6 +7,7 @@
 // V-cycle is bitwise the one hpcg_b200_mg computes.
 #pragma once
 
+#include "bulk.cuh"
 #include "reduce.cuh"
 
 namespace hb {
@@ -119,6 +120,110 @@ __global__ void __launch_bounds__(kThreads) k_spmv_m(const double* __restrict__ 
       for (int j = 0; j < S; ++j) acc[j] += xq[j] * sum[j];
     }
   }
+  if (DOT) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const double s = block_sum(off == (j / S) * S ? acc[j % S] : 0.0);
+      if (threadIdx.x == 0) partials[j * gridDim.x + blockIdx.x] = s;
+    }
+  }
+}
+
+// Pipeline shapes of the multi-system kernels: LANES threads per row, at most
+// 1024 threads a block (four lanes: one group with a ring of four stages).
+template <int LANES>
+using MultiShape = BulkShape<double, LANES == 4 ? 1 : 2, LANES == 4 ? 4 : 2, LANES>;
+
+// k_gs_phase_m through the bulk-copy pipeline (bulk.cuh): the tile's values and
+// columns arrive on chip by two tensor copies, the lanes of a row gather their
+// S-entry runs of x as in k_gs_phase_m, in the same order: the same bits. The
+// full-slot phases (FIRST false) take all 27 slots.
+template <int K, int LANES, bool FIRST>
+__global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
+    k_gs_phase_m_bulk(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                      const double* __restrict__ rhs, double* x, int r0, int r1, uint32_t mask_arg, unsigned* fault,
+                      const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col) {
+  constexpr int S = K / LANES;
+  const uint32_t mask = FIRST ? mask_arg : kAllSlots;
+  const int a0 = r0 & ~(kBulkRows - 1);
+  const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
+  bulk_tiles<double, MultiShape<LANES>>(
+      val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
+      [&](int64_t q0, const double* sv, const int* sc, int t) {
+        const int row = t / LANES;
+        const int off = (t % LANES) * S;
+        const int64_t q = q0 + row;
+        if (q < r0 || q >= r1) return;
+        double sum[S], xd[S];
+        load_k<S>(rhs + q * K + off, sum);
+#pragma unroll
+        for (int j = 0; j < S; ++j) xd[j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          if (mask & (1u << k)) {
+            const double a = sv[k * kBulkRows + row];
+            double xv[S];
+            load_k<S>(x + (int64_t)sc[k * kBulkRows + row] * K + off, xv);
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+              sum[j] -= a * xv[j];
+              if (k == kDiagSlot) xd[j] = xv[j];
+            }
+          }
+        }
+        const double d = sv[kDiagSlot * kBulkRows + row];
+        double out[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+          if (!FIRST) sum[j] += xd[j] * d;
+          out[j] = sum[j] / d;
+        }
+        store_k<S>(x + q * K + off, out);
+      },
+      fault, tm_val, tm_col);
+}
+
+// k_spmv_m through the bulk-copy pipeline, rows in storage order; DOT: partials
+// of x_j'y_j at partials[j*gridDim.x + block].
+template <int K, int LANES, bool DOT>
+__global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
+    k_spmv_m_bulk(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                  const double* __restrict__ x, double* __restrict__ y, int n, double* __restrict__ partials,
+                  unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
+                  const __grid_constant__ CUtensorMap tm_col) {
+  constexpr int S = K / LANES;
+  const int off = (int)(threadIdx.x % LANES) * S;  // the producer warp (32 threads) keeps the lanes aligned
+  double acc[S];
+#pragma unroll
+  for (int j = 0; j < S; ++j) acc[j] = 0.0;
+  const int ntiles = (n + kBulkRows - 1) / kBulkRows;
+  bulk_tiles<double, MultiShape<LANES>>(
+      val, col, pitch, ntiles, [&](int tile) { return (int64_t)tile * kBulkRows; },
+      [&](int64_t q0, const double* sv, const int* sc, int t) {
+        const int row = t / LANES;
+        const int64_t q = q0 + row;
+        if (q >= n) return;
+        double sum[S], xq[S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) sum[j] = xq[j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          const double a = sv[k * kBulkRows + row];
+          double xv[S];
+          load_k<S>(x + (int64_t)sc[k * kBulkRows + row] * K + off, xv);
+#pragma unroll
+          for (int j = 0; j < S; ++j) {
+            sum[j] += a * xv[j];
+            if (k == kDiagSlot) xq[j] = xv[j];
+          }
+        }
+        store_k<S>(y + q * K + off, sum);
+        if (DOT) {
+#pragma unroll
+          for (int j = 0; j < S; ++j) acc[j] += xq[j] * sum[j];
+        }
+      },
+      fault, tm_val, tm_col);
   if (DOT) {
 #pragma unroll
     for (int j = 0; j < K; ++j) {

@@ -3,6 +3,7 @@
 // kernels_multi.cuh; each matrix row is read once per sweep for all K.
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "kernels_multi.cuh"
@@ -15,6 +16,7 @@ void release_accounted(size_t bytes);
 struct MultiState {
   int K = 0;
   int lanes = 1;  // threads per row of the matrix kernels (K/lanes systems each), tuned on creation
+  int bulk = 0;   // 0: register-pipelined kernels; 1: bulk-copy full phases and SpMV; 2: first sweep too
   double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
   double* lr[kMaxLevels] = {nullptr};  // coarse right-hand sides (levels > 0)
   double* lx[kMaxLevels] = {nullptr};  // coarse solutions (levels > 0)
@@ -49,19 +51,45 @@ int alloc_z(MultiState* m, double** p, size_t count, cudaStream_t st) {
   return HPCG_B200_OK;
 }
 
-template <int K, int LANES>
+template <int K, int LANES, int BULK>
 int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x);
+template <int K, int LANES, int BULK, bool DOT>
+int spmv_m(Context* c, const Level& L, const double* x, double* y, double* partials);
 
-// The matrix work of one CG iteration with LANES threads per row: a V-cycle and
-// the SpMV with its p'Ap partials.
-template <int K, int LANES>
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+// Calls f(IC<LANES>, IC<BULK>) for the state's configuration.
+template <int K, typename F>
+int dispatch_m(const MultiState* m, F&& f) {
+  if (m->lanes == 4) {
+    if constexpr (K >= 8) {
+      if (m->bulk == 1) return f(IC<4>{}, IC<1>{});
+      if (m->bulk == 2) return f(IC<4>{}, IC<2>{});
+      return f(IC<4>{}, IC<0>{});
+    }
+  } else if (m->lanes == 2) {
+    if constexpr (K >= 4) {
+      if (m->bulk == 1) return f(IC<2>{}, IC<1>{});
+      if (m->bulk == 2) return f(IC<2>{}, IC<2>{});
+      return f(IC<2>{}, IC<0>{});
+    }
+  }
+  if (m->bulk == 1) return f(IC<1>{}, IC<1>{});
+  if (m->bulk == 2) return f(IC<1>{}, IC<2>{});
+  return f(IC<1>{}, IC<0>{});
+}
+
+// The matrix work of one CG iteration in one configuration: a V-cycle and the
+// SpMV with its p'Ap partials.
+template <int K, int LANES, int BULK>
 int time_iteration(hpcg_b200_problem* P, MultiState* m, cudaEvent_t e0, cudaEvent_t e1, float* best) {
   Context* c = P->ctx;
   const Level& L = P->lev[0];
   HB_CK(cudaEventRecord(e0, c->stream));
-  HB_TRY((mg_m<K, LANES>(P, m, 0, m->r, m->z)));
-  k_spmv_m<K, LANES, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, L.n, m->partials);
-  HB_CK(cudaGetLastError());
+  HB_TRY((mg_m<K, LANES, BULK>(P, m, 0, m->r, m->z)));
+  const int g = spmv_m<K, LANES, BULK, true>(c, L, m->p, m->Ap, m->partials);
+  if (g < 0) return -g;
   HB_CK(cudaEventRecord(e1, c->stream));
   HB_CK(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -70,41 +98,58 @@ int time_iteration(hpcg_b200_problem* P, MultiState* m, cudaEvent_t e0, cudaEven
   return HPCG_B200_OK;
 }
 
-// Threads per row of the matrix kernels: the fastest V-cycle + SpMV (round-robin
-// repetitions), or HPCG_B200_MULTI_LANES. Same V-cycle bits either way.
+// Threads per row and kernel form of the matrix kernels: the fastest V-cycle +
+// SpMV (round-robin repetitions over lanes 1, 2, 4 x register-pipelined, bulk
+// full phases, bulk everywhere), or HPCG_B200_MULTI_LANES / HPCG_B200_MULTI_BULK.
+// Same V-cycle bits either way.
+template <int K>
 int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
-  const int K = m->K;
   const char* force = std::getenv("HPCG_B200_MULTI_LANES");
-  if (force && *force) {
-    const int f = std::atoi(force);
+  const char* force_bulk = std::getenv("HPCG_B200_MULTI_BULK");
+  const bool have_maps = bulk_maps(P->lev[0]) != nullptr;
+  if ((force && *force) || (force_bulk && *force_bulk)) {
+    const int f = force && *force ? std::atoi(force) : 1;
     m->lanes = f >= 4 && K >= 8 ? 4 : f >= 2 && K >= 4 ? 2 : 1;
+    const int b = force_bulk && *force_bulk ? std::atoi(force_bulk) : 0;
+    m->bulk = have_maps ? (b < 0 ? 0 : b > 2 ? 2 : b) : 0;
     return HPCG_B200_OK;
   }
   Context* c = P->ctx;
   cudaEvent_t e0, e1;
   HB_CK(cudaEventCreate(&e0));
   HB_CK(cudaEventCreate(&e1));
-  float t_[3] = {1e30f, 1e30f, 1e30f};  // lanes 1, 2, 4
+  float t_[3][3];  // [lanes 1, 2, 4][bulk 0, 1, 2]
+  for (auto& row : t_)
+    for (float& v : row) v = 1e30f;
+  const int nbulk = have_maps ? 3 : 1;
   int st = HPCG_B200_OK;
   for (int rep = 0; rep < 3 && st == HPCG_B200_OK; ++rep) {
-    if (K == 2) st = time_iteration<2, 1>(P, m, e0, e1, &t_[0]);
-    if (K == 4) {
-      st = time_iteration<4, 1>(P, m, e0, e1, &t_[0]);
-      if (!st) st = time_iteration<4, 2>(P, m, e0, e1, &t_[1]);
-    }
-    if (K == 8) {
-      st = time_iteration<8, 1>(P, m, e0, e1, &t_[0]);
-      if (!st) st = time_iteration<8, 2>(P, m, e0, e1, &t_[1]);
-      if (!st) st = time_iteration<8, 4>(P, m, e0, e1, &t_[2]);
+    for (int li = 0; li < 3 && st == HPCG_B200_OK; ++li) {
+      const int lanes = 1 << li;
+      if ((lanes == 2 && K < 4) || (lanes == 4 && K < 8)) continue;
+      for (int b = 0; b < nbulk && st == HPCG_B200_OK; ++b) {
+        MultiState probe;
+        probe.lanes = lanes;
+        probe.bulk = b;
+        float* slot = &t_[li][b];
+        st = dispatch_m<K>(&probe, [&](auto l, auto bk) {
+          return time_iteration<K, decltype(l)::value, decltype(bk)::value>(P, m, e0, e1, slot);
+        });
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   HB_TRY(st);
-  int best = 0;
-  for (int i = 1; i < 3; ++i)
-    if (t_[i] < t_[best]) best = i;
-  m->lanes = 1 << best;
+  int bl = 0, bb = 0;
+  for (int li = 0; li < 3; ++li)
+    for (int b = 0; b < 3; ++b)
+      if (t_[li][b] < t_[bl][bb]) {
+        bl = li;
+        bb = b;
+      }
+  m->lanes = 1 << bl;
+  m->bulk = bb;
   // the timed work wrote z, Ap and the coarse vectors: every solve loads its own
   // b and x and every V-cycle starts from zero, but leave the state as created
   HB_CK(cudaMemsetAsync(m->z, 0, sizeof(double) * (size_t)P->lev[0].pitch * K, c->stream));
@@ -118,7 +163,8 @@ int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
 
 // The state for K systems (re-created when K changes). Vectors are zeroed, so
 // the zero row n of every level (padded stencil slots) reads 0 for all K.
-int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
+template <int K>
+int ensure_state(hpcg_b200_problem* P, MultiState** out) {
   MultiState*& m = P->multi;
   if (m && m->K == K) {
     *out = m;
@@ -139,14 +185,42 @@ int ensure_state(hpcg_b200_problem* P, int K, MultiState** out) {
   HB_TRY(dev_alloc((void**)&m->s, sizeof(MScalars), &m->bytes));
   HB_CK(cudaMemsetAsync(m->s, 0, sizeof(MScalars), st));
   HB_CK(cudaMallocHost(&m->s_host, sizeof(MScalars)));
-  HB_TRY(tune_lanes(P, m));
+  HB_TRY(tune_lanes<K>(P, m));
   *out = m;
   return HPCG_B200_OK;
 }
 
-template <int K, int LANES>
+// Enables a bulk kernel's shared memory on c's device (once per kernel and device).
+template <typename Kern>
+void bulk_attr(Kern k, int smem, int device, uint64_t* done) {
+  if (!(*done >> device & 1)) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    *done |= 1ull << device;
+  }
+}
+
+template <int K, int LANES, int BULK>
 void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, int r0, int r1, bool first,
                     uint32_t mask) {
+  const BulkMaps* bm = BULK == 2 || (BULK == 1 && !first) ? bulk_maps(L) : nullptr;
+  if (bm) {
+    using Sh = MultiShape<LANES>;
+    const int64_t tiles = ((int64_t)r1 - (r0 & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
+    const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+    static uint64_t done[2] = {0, 0};
+    if (first) {
+      auto k = k_gs_phase_m_bulk<K, LANES, true>;
+      bulk_attr(k, Sh::smem, c->device, &done[0]);
+      k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
+                                                  bm->col);
+    } else {
+      auto k = k_gs_phase_m_bulk<K, LANES, false>;
+      bulk_attr(k, Sh::smem, c->device, &done[1]);
+      k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
+                                                  bm->col);
+    }
+    return;
+  }
   const int64_t work = (int64_t)(r1 - r0) * LANES;
   if (first) {
     auto k = k_gs_phase_m<K, LANES, true>;
@@ -157,42 +231,74 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
   }
 }
 
-template <int K, int LANES>
+// y = A x for K systems; returns the number of blocks (DOT: partial sets written)
+// or a negative status.
+template <int K, int LANES, int BULK, bool DOT>
+int spmv_m(Context* c, const Level& L, const double* x, double* y, double* partials) {
+  const BulkMaps* bm = BULK ? bulk_maps(L) : nullptr;
+  if (bm) {
+    using Sh = MultiShape<LANES>;
+    auto k = k_spmv_m_bulk<K, LANES, DOT>;
+    static uint64_t done = 0;
+    bulk_attr(k, Sh::smem, c->device, &done);
+    const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
+    const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+    k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, x, y, L.n, partials, c->fault, bm->val,
+                                                bm->col);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error("k_spmv_m_bulk", e);
+      return -status_of(e);
+    }
+    return g;
+  }
+  auto k = k_spmv_m<K, LANES, DOT>;
+  const int g = DOT ? kParts : grid_of(c, k, (int64_t)L.n * LANES);
+  k<<<g, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, x, y, L.n, partials);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("k_spmv_m", e);
+    return -status_of(e);
+  }
+  return g;
+}
+
+template <int K, int LANES, int BULK>
 int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool first) {
   int last = -1;
   for (int s = 0; s < kColours; ++s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
     last = s;
-    launch_phase_m<K, LANES>(c, L, rhs, x, r0, r1, first, first ? first_mask(L.g, s) : kAllSlots);
+    launch_phase_m<K, LANES, BULK>(c, L, rhs, x, r0, r1, first, first ? first_mask(L.g, s) : kAllSlots);
   }
   // backward sweep, without repeating the last colour (as the single-system path)
   for (int s = last - 1; s >= 0; --s) {
     const int r0 = L.g.start[s], r1 = L.g.start[s + 1];
     if (r1 <= r0) continue;
-    launch_phase_m<K, LANES>(c, L, rhs, x, r0, r1, false, kAllSlots);
+    launch_phase_m<K, LANES, BULK>(c, L, rhs, x, r0, r1, false, kAllSlots);
   }
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
 }
 
 // ComputeMG_ref.cpp:39-63 for K systems on level l (colour order, interleaved).
-template <int K, int LANES>
+template <int K, int LANES, int BULK>
 int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x) {
   const Level& L = P->lev[l];
   Context* c = P->ctx;
-  HB_TRY((gs_colour_m<K, LANES>(c, L, r, x, true)));
+  HB_TRY((gs_colour_m<K, LANES, BULK>(c, L, r, x, true)));
   if (l + 1 < P->nlev) {
     const Level& C = P->lev[l + 1];
     auto kr = k_restrict_m<K, LANES>;
     kr<<<grid_of(c, kr, (int64_t)C.n * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x, L.tf, L.tq,
                                                                           m->lr[l + 1], C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY((mg_m<K, LANES>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1])));
+    HB_TRY((mg_m<K, LANES, BULK>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1])));
     auto kp = k_prolong_m<K>;
     kp<<<grid_of(c, kp, C.n), kThreads, 0, c->stream>>>(L.tf, L.tq, m->lx[l + 1], x, C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY((gs_colour_m<K, LANES>(c, L, r, x, false)));
+    HB_TRY((gs_colour_m<K, LANES, BULK>(c, L, r, x, false)));
   }
   return HPCG_B200_OK;
 }
@@ -242,13 +348,12 @@ int store_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, do
   k<<<grid_of(c, k, L.n), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n, nrhs);
   HB_CK(cudaGetLastError());
   if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
-  return HPCG_B200_OK;
+  return stream_sync(c);
 }
 
 template <int K>
-int finalize_m(Context* c, MultiState* m, int op, int iter, double tol) {
-  k_finalize_m<K><<<1, kThreads, 0, c->stream>>>(m->partials, kParts, op, m->s, iter, tol);
+int finalize_m(Context* c, MultiState* m, int op, int iter, double tol, int nparts = kParts) {
+  k_finalize_m<K><<<1, kThreads, 0, c->stream>>>(m->partials, nparts, op, m->s, iter, tol);
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
 }
@@ -256,24 +361,24 @@ int finalize_m(Context* c, MultiState* m, int op, int iter, double tol) {
 // CG.cpp:59-143 for K systems in lockstep; a system stops updating once its
 // scaled residual is at or below the tolerance; the loop ends when none is left
 // or after max_iter iterations.
-template <int K, int LANES>
+template <int K, int LANES, int BULK>
 int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any_iters) {
   const Level& L = P->lev[0];
   Context* c = P->ctx;
   const int n = L.n;
-  auto ks = k_spmv_m<K, LANES, false>;
-  ks<<<grid_of(c, ks, (int64_t)n * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->x, m->Ap, n, nullptr);
+  int g = spmv_m<K, LANES, BULK, false>(c, L, m->x, m->Ap, nullptr);
+  if (g < 0) return -g;
   k_resid_m<K><<<kParts, kThreads, 0, c->stream>>>(m->b, m->Ap, m->r, n, m->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize_m<K>(c, m, kMNorm0, 0, tol));
   HB_CK(cudaMemcpyAsync(m->s_host, m->s, sizeof(MScalars), cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   int k = 1;
   for (; k <= max_iter; ++k) {
     bool any = false;
     for (int j = 0; j < K; ++j) any = any || m->s_host->active[j];
     if (!any) break;
-    HB_TRY((mg_m<K, LANES>(P, m, 0, m->r, m->z)));
+    HB_TRY((mg_m<K, LANES, BULK>(P, m, 0, m->r, m->z)));
     k_dot_m<K><<<kParts, kThreads, 0, c->stream>>>(m->r, m->z, n, m->partials);
     HB_CK(cudaGetLastError());
     if (k == 1) {
@@ -284,14 +389,14 @@ int cg_m(hpcg_b200_problem* P, MultiState* m, int max_iter, double tol, int* any
       k_update_p_m<K><<<kParts, kThreads, 0, c->stream>>>(m->z, m->p, n, m->s);
       HB_CK(cudaGetLastError());
     }
-    k_spmv_m<K, LANES, true><<<kParts, kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, m->p, m->Ap, n, m->partials);
-    HB_CK(cudaGetLastError());
-    HB_TRY(finalize_m<K>(c, m, kMPap, k, tol));
+    g = spmv_m<K, LANES, BULK, true>(c, L, m->p, m->Ap, m->partials);
+    if (g < 0) return -g;
+    HB_TRY(finalize_m<K>(c, m, kMPap, k, tol, g));
     k_update_xr_m<K><<<kParts, kThreads, 0, c->stream>>>(m->x, m->p, m->r, m->Ap, n, m->s, m->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize_m<K>(c, m, kMNormr, k, tol));
     HB_CK(cudaMemcpyAsync(m->s_host, m->s, sizeof(MScalars), cudaMemcpyDeviceToHost, c->stream));
-    HB_CK(cudaStreamSynchronize(c->stream));
+    HB_TRY(stream_sync(c));
   }
   *any_iters = k - 1;
   return HPCG_B200_OK;
@@ -301,17 +406,13 @@ template <int K>
 int run_cg_multi(hpcg_b200_problem* P, int nrhs, const double* b, double* x, int max_iter, double tol, int* niters,
                  double* normr, double* normr0) {
   MultiState* m = nullptr;
-  HB_TRY(ensure_state(P, K, &m));
+  HB_TRY(ensure_state<K>(P, &m));
   HB_TRY(load_m<K>(P, m, nrhs, b, m->b));
   HB_TRY(load_m<K>(P, m, nrhs, x, m->x));
   int done = 0;
-  if (m->lanes == 4) {
-    if constexpr (K >= 8) HB_TRY((cg_m<K, 4>(P, m, max_iter, tol, &done)));
-  } else if (m->lanes == 2) {
-    if constexpr (K >= 4) HB_TRY((cg_m<K, 2>(P, m, max_iter, tol, &done)));
-  } else {
-    HB_TRY((cg_m<K, 1>(P, m, max_iter, tol, &done)));
-  }
+  HB_TRY(dispatch_m<K>(m, [&](auto l, auto bk) {
+    return cg_m<K, decltype(l)::value, decltype(bk)::value>(P, m, max_iter, tol, &done);
+  }));
   HB_TRY(store_m<K>(P, m, nrhs, m->x, x));
   for (int j = 0; j < nrhs; ++j) {
     niters[j] = m->s_host->niters[j];
@@ -324,15 +425,11 @@ int run_cg_multi(hpcg_b200_problem* P, int nrhs, const double* b, double* x, int
 template <int K>
 int run_mg_multi(hpcg_b200_problem* P, int nrhs, const double* r, double* x) {
   MultiState* m = nullptr;
-  HB_TRY(ensure_state(P, K, &m));
+  HB_TRY(ensure_state<K>(P, &m));
   HB_TRY(load_m<K>(P, m, nrhs, r, m->r));
-  if (m->lanes == 4) {
-    if constexpr (K >= 8) HB_TRY((mg_m<K, 4>(P, m, 0, m->r, m->z)));
-  } else if (m->lanes == 2) {
-    if constexpr (K >= 4) HB_TRY((mg_m<K, 2>(P, m, 0, m->r, m->z)));
-  } else {
-    HB_TRY((mg_m<K, 1>(P, m, 0, m->r, m->z)));
-  }
+  HB_TRY(dispatch_m<K>(m, [&](auto l, auto bk) {
+    return mg_m<K, decltype(l)::value, decltype(bk)::value>(P, m, 0, m->r, m->z);
+  }));
   return store_m<K>(P, m, nrhs, m->z, x);
 }
 

@@ -51,54 +51,6 @@ void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   k<<<g, rows, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot);
 }
 
-// cuTensorMapEncodeTiled, looked up once through the runtime (no link to the driver library).
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(f);
-    else
-      cudaGetLastError();
-  }
-  return fn;
-}
-
-// 2-D map of one slot-major array: x = row (pitch entries, the row stride), y =
-// slot (27); box kBulkRows x 27.
-bool encode_slot_major(CUtensorMap* m, CUtensorMapDataType type, size_t esize, const void* base, int64_t pitch) {
-  EncodeTiledFn fn = encode_tiled();
-  if (!fn) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)kSlots};
-  const cuuint64_t strides[1] = {(cuuint64_t)pitch * esize};
-  const cuuint32_t box[2] = {(cuuint32_t)kBulkRows, (cuuint32_t)kSlots};
-  const cuuint32_t elem[2] = {1, 1};
-  return fn(m, type, 2, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-// The level's FP64 tensor maps (built on first use, rebuilt if the arrays moved);
-// nullptr if they cannot be encoded.
-const BulkMaps* bulk_maps(const Level& L) {
-  if (!L.maps) L.maps = new BulkMaps();
-  BulkMaps* m = L.maps;
-  if (m->val_ptr != L.val || m->col_ptr != L.col) {
-    m->ok = encode_slot_major(&m->val, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), L.val, L.pitch) &&
-            encode_slot_major(&m->col, CU_TENSOR_MAP_DATA_TYPE_INT32, sizeof(int), L.col, L.pitch);
-    m->val_ptr = L.val;
-    m->col_ptr = L.col;
-  }
-  return m->ok ? m : nullptr;
-}
-
 // The bulk-copy pipeline (configuration 10): one block per SM (its shared
 // memory allows no second), at most one per tile. false: not launched (FP64
 // tensor maps unavailable).
@@ -106,7 +58,7 @@ template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
 bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                     double* dot) {
   auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT>;
-  constexpr int smem = gs_bulk_smem<T>();
+  constexpr int smem = GsShape<T>::smem;
   static CUtensorMap none;  // the FP32 kernels take no maps
   const CUtensorMap* tv = &none;
   const CUtensorMap* tc = &none;
@@ -125,7 +77,7 @@ bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   const int64_t tiles = ((int64_t)r1 - a0 + kBulkRows - 1) / kBulkRows;
   int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
   if (DOT && g > kDotStride) g = kDotStride;
-  k<<<g, gs_bulk_threads<T>(), smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault,
+  k<<<g, GsShape<T>::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault,
                                                   *tv, *tc);
   return true;
 }
@@ -278,7 +230,7 @@ template <typename T, bool DOT, int ORDER>
 int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials,
                      const BulkMaps* m) {
   auto k = k_spmv_bulk<T, DOT, ORDER>;
-  constexpr int smem = gs_bulk_smem<T>();
+  constexpr int smem = SpmvShape<T>::smem;
   static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
   if (!(attr_set >> c->device & 1)) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -286,7 +238,7 @@ int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y,
   }
   const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sms));
-  k<<<g, gs_bulk_threads<T>(), smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault,
+  k<<<g, SpmvShape<T>::threads, smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault,
                                                   m->val, m->col);
   return g;
 }

@@ -90,3 +90,35 @@ def test_mg_multi_follows_value_changes(binding):
                 assert np.array_equal(z[j], zj), (diag is None, j)
     finally:
         P.free()
+
+
+@pytest.mark.parametrize("lanes,bulk", [(1, 1), (2, 1), (4, 1), (2, 2), (4, 2), (2, 0)])
+def test_every_multi_form_is_single_mg_bitwise(binding, monkeypatch, lanes, bulk):
+    """Every (lanes, kernel form) of the eight-system path: register-pipelined,
+    bulk-copy full phases and SpMV, bulk-copy first sweep too. Each system's
+    V-cycle is bitwise the single-system one and the lockstep CG follows the
+    single-system CG, on a grid whose coarse colour blocks start off tile
+    boundaries (24 x 16 x 40)."""
+    monkeypatch.setenv("HPCG_B200_MULTI_LANES", str(lanes))
+    monkeypatch.setenv("HPCG_B200_MULTI_BULK", str(bulk))
+    P = binding.Problem.generate(24, 16, 40)
+    try:
+        n = P.nrow
+        r = np.random.default_rng(10 * lanes + bulk).standard_normal((8, n))
+        z = np.zeros((8, n))
+        P.ComputeMG_multi(r, z)
+        for j in range(8):
+            zj = np.zeros(n)
+            P.ComputeMG(np.ascontiguousarray(r[j]), zj)
+            assert np.array_equal(z[j], zj), j
+        b = np.random.default_rng(5).uniform(-1.0, 1.0, (8, n))
+        x = np.zeros((8, n))
+        ni, nr, nr0 = P.CG_multi(b, x, 12, 0.0)
+        for j in (0, 5):
+            xs = np.zeros(n)
+            ni_s, nr_s, nr0_s = P.CG(np.ascontiguousarray(b[j]), xs, 12, 0.0, True)
+            s = nr_s / nr0_s
+            assert ni[j] == ni_s == 12
+            assert abs(nr[j] / nr0[j] - s) <= 1e-10 * max(s, 1e-9), (j, nr[j] / nr0[j], s)
+    finally:
+        P.free()
