@@ -187,6 +187,7 @@ struct Level {
   int* f2c = nullptr;        // [n of next level] coarse colour row -> fine colour row
   int* tf = nullptr;         // transfer pairs (fine row, coarse row) sorted by fine row:
   int* tq = nullptr;         //   tf[t] = f2c[tq[t]], tf increasing
+  int tf_run = -1;           // f0 if tf[t] = f0 + t for every t (one run of fine rows), else -1
   double* r = nullptr;       // coarse right-hand side (levels > 0), [pitch]
   double* x = nullptr;       // coarse solution (levels > 0), [pitch]
   float* r32 = nullptr;      // FP32 V-cycle vectors, [pitch]

@@ -581,6 +581,31 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
   }
 }
 
+// The restriction through the bulk-copy pipeline (with SpMV configuration 7),
+// when the injected rows are one run f0 .. f0 + nc of fine rows (tf[t] = f0 + t,
+// checked on the host): the run is tiled like a phase. Same sums as k_restrict.
+template <typename T>
+__global__ void __launch_bounds__(SpmvShape<T>::threads, 1)
+    k_restrict_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const T* __restrict__ rf,
+                    const T* __restrict__ xf, const int* __restrict__ tq, T* __restrict__ rc, int f0, int nc,
+                    unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
+                    const __grid_constant__ CUtensorMap tm_col) {
+  const int r1 = f0 + nc;
+  const int a0 = f0 & ~(kBulkRows - 1);
+  const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
+  bulk_tiles<T, SpmvShape<T>>(
+      val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
+      [&](int64_t q0, const T* sv, const int* sc, int t) {
+        const int64_t f = q0 + t;
+        if (f < f0 || f >= r1) return;
+        T sum = (T)0;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * __ldg(xf + sc[k * kBulkRows + t]);
+        rc[tq[f - f0]] = rf[f] - sum;
+      },
+      fault, tm_val, tm_col);
+}
+
 // ComputeProlongation_ref.cpp:49 over the same sorted pairs
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_prolong(const int* __restrict__ tf, const int* __restrict__ tq,

@@ -185,6 +185,11 @@ int build_transfer(hpcg_b200_problem* p, int l) {
   HB_TRY(alloc_n(p, &L.tq, nc));
   HB_CK(cudaMemcpy(L.tf, tf.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
   HB_CK(cudaMemcpy(L.tq, tq.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+  // the injected rows as one run of storage (the colour-0 block of the parity
+  // colouring): the bulk-copy restriction tiles it like a phase
+  bool run = nc > 0;
+  for (int u = 0; u < nc && run; ++u) run = tf[u] == tf[0] + u;
+  L.tf_run = run ? tf[0] : -1;
   return HPCG_B200_OK;
 }
 

@@ -282,8 +282,37 @@ void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, cons
   k<<<grid_of(c, k, nc), kThreads, 0, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tf, L.tq, rc, nc);
 }
 
+// The restriction on the bulk-copy pipeline (SpMV configuration 7, injected rows
+// in one run); false if it cannot run here.
+template <typename T>
+bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
+  if (L.tf_run < 0 || nc <= 0) return false;
+  static CUtensorMap none;  // the FP32 copy takes no maps
+  const CUtensorMap* tv = &none;
+  const CUtensorMap* tc = &none;
+  if constexpr (bulk_tensor_tile<T>()) {
+    const BulkMaps* m = bulk_maps(L);
+    if (!m) return false;
+    tv = &m->val;
+    tc = &m->col;
+  }
+  auto k = k_restrict_bulk<T>;
+  constexpr int smem = SpmvShape<T>::smem;
+  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
+  if (!(attr_set >> c->device & 1)) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set |= 1ull << c->device;
+  }
+  const int64_t tiles = ((int64_t)L.tf_run + nc - (L.tf_run & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
+  const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+  k<<<g, SpmvShape<T>::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tq, rc, L.tf_run, nc,
+                                                   c->fault, *tv, *tc);
+  return true;
+}
+
 template <typename T>
 void restrict_dispatch(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
+  if (L.mv_sched == kBulkMvCfg && restrict_bulk<T>(c, L, val, rf, xf, rc, nc)) return;
   switch (L.mv_sched) {  // scalar configurations only: the transfer pairs need not be contiguous
     case 0: case 4: restrict_launch<T, 0>(c, L, val, rf, xf, rc, nc); break;
     case 2: restrict_launch<T, 2>(c, L, val, rf, xf, rc, nc); break;
