@@ -10,9 +10,11 @@
 // problem is still above its tolerance and the iteration limit is not reached;
 // problems that have converged skip their tiles. No kernel waits on another.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
+#include "bulk.cuh"
 #include "reduce.cuh"
 #include "rows.cuh"
 
@@ -92,6 +94,55 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
     else
       gs_row<float, float, false, kPlain, 0>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
   }
+}
+
+// The batched colour phase through the bulk-copy pipeline (bulk.cuh): every
+// tile is one 128-row block of its problem's blocked FP32 copy (val32, col32 of
+// the single-problem path), so it arrives by two copies; the tiles of problems
+// that have converged are skipped on both sides. Same arithmetic as k_b_gs.
+__global__ void __launch_bounds__(GsShape<float>::threads, 1)
+    k_b_gs_bulk(const BGs* __restrict__ items, const BTile* __restrict__ tiles, int ntiles,
+                const BScal* __restrict__ sc, unsigned* fault) {
+  bulk_tiles_src<float, GsShape<float>>(
+      ntiles,
+      [&](int t) {
+        const BTile tl = tiles[t];
+        const BGs& it = items[tl.item];
+        return TileSrc<float>{tl.start, it.val + mat_index<float>(0, tl.start, it.pitch),
+                              it.col + mat_index<float>(0, tl.start, it.pitch)};
+      },
+      [&](int t) { return !sc[items[tiles[t].item].prob].active; },
+      [&](int t, int64_t q0, const float* sv, const int* scol, int row) {
+        const BGs& it = items[tiles[t].item];
+        const int64_t q = q0 + row;
+        if (q < it.r0 || q >= it.r1) return;
+        const uint32_t mask = it.mask;
+        float sum = it.rhs[q];
+        float xd = 0.0f;
+        if (mask == kAllSlots) {  // full-slot phases: the 27 gathers without a test each
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            const float a = sv[k * kBulkRows + row];
+            const float xv = __ldg(it.x + scol[k * kBulkRows + row]);
+            sum -= a * xv;
+            if (k == kDiagSlot) xd = xv;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            if (mask & (1u << k)) {
+              const float a = sv[k * kBulkRows + row];
+              const float xv = __ldg(it.x + scol[k * kBulkRows + row]);
+              sum -= a * xv;
+              if (k == kDiagSlot) xd = xv;
+            }
+          }
+        }
+        const float d = sv[kDiagSlot * kBulkRows + row];
+        if (!it.first) sum += xd * d;
+        it.x[q] = sum / d;
+      },
+      fault, nullptr, nullptr);
 }
 
 // rc = (rf - A xf) at the injected rows (ComputeMG_ref.cpp:49-51, sorted pairs)
@@ -332,6 +383,8 @@ struct Step {
   int item_off;  // first item of the step (tiles index the whole item array)
   int tile_off;  // first tile of the step
   int ntiles;
+  int btile_off = 0;  // GS phases: the step's 128-row tiles for k_b_gs_bulk
+  int bntiles = 0;
 };
 
 }  // namespace
@@ -347,6 +400,9 @@ struct hpcg_b200_batch {
   hb::BGs* gs_items;
   hb::BRes* res_items;
   hb::BTile* tiles;
+  hb::BGs* gs_bitems;  // the GS items on the blocked FP32 copies (bulk-copy phases)
+  hb::BTile* btiles;   // their 128-row tiles
+  bool bulk;           // GS phases on k_b_gs_bulk (chosen by timing at creation)
   std::vector<hb::Step> steps;
   hb::BVec* vec;
   hb::BTile* vtiles;  // row tiles of every problem's level 0
@@ -385,14 +441,21 @@ void tiles_of(std::vector<BTile>& tiles, int item, int r0, int r1) {
   for (int s = r0; s < r1; s += kTile) tiles.push_back({item, s});
 }
 
+// 128-row tiles of the bulk-copy phase: blocks of the blocked FP32 copy that
+// hold rows of [r0, r1)
+void bulk_tiles_of(std::vector<BTile>& tiles, int item, int r0, int r1) {
+  for (int s = r0 & ~(kBulkRows - 1); s < r1; s += kBulkRows) tiles.push_back({item, s});
+}
+
 // The V-cycle of every problem as one step sequence (ComputeMG_ref.cpp:39-63
 // with the colour sweeps of the single-problem path): level l pre-smooth
 // (forward from x = 0, backward without the last colour), restriction,
 // recursion, prolongation, post-smooth; the coarsest level one symmetric sweep.
 void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<BRes>& res,
-                  std::vector<BTile>& tiles) {
+                  std::vector<BTile>& tiles, std::vector<BGs>& gsb, std::vector<BTile>& btiles) {
   auto phase = [&](int s, bool first) {
     Step st{0, (int)gs.size(), (int)tiles.size(), 0};
+    st.btile_off = (int)btiles.size();
     for (int p = 0; p < B->m; ++p) {
       const Level& L = B->probs[p]->lev[l];
       const int item = (int)gs.size();
@@ -409,8 +472,14 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       it.prob = p;
       gs.push_back(it);
       tiles_of(tiles, item, it.r0, it.r1);
+      BGs bit = it;  // the same phase on the blocked copies (item index = gs index)
+      bit.val = L.val32;
+      bit.col = L.col32;
+      gsb.push_back(bit);
+      bulk_tiles_of(btiles, item, it.r0, it.r1);
     }
     st.ntiles = (int)tiles.size() - st.tile_off;
+    st.bntiles = (int)btiles.size() - st.btile_off;
     B->steps.push_back(st);
   };
   auto sweep = [&](bool first) {
@@ -449,7 +518,7 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
   sweep(true);
   if (l + 1 < 4) {
     transfer(1);
-    build_vcycle(B, l + 1, gs, res, tiles);
+    build_vcycle(B, l + 1, gs, res, tiles, gsb, btiles);
     transfer(2);
     sweep(false);
   }
@@ -464,7 +533,17 @@ int launch_step(hpcg_b200_batch* B, const Step& s) {
   Context* c = B->ctx;
   const int g = grid_tiles(c, s.ntiles);
   // tiles hold indices into the whole item array, so the items go in unshifted
-  if (s.kind == 0)
+  if (s.kind == 0 && B->bulk) {
+    using Sh = GsShape<float>;
+    static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
+    if (!(attr_set >> c->device & 1)) {
+      cudaFuncSetAttribute(k_b_gs_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::smem);
+      attr_set |= 1ull << c->device;
+    }
+    const int gb = s.bntiles < c->sms ? (s.bntiles < 1 ? 1 : s.bntiles) : c->sms;
+    k_b_gs_bulk<<<gb, Sh::threads, Sh::smem, c->stream>>>(B->gs_bitems, B->btiles + s.btile_off, s.bntiles, B->sc,
+                                                          c->fault);
+  } else if (s.kind == 0)
     k_b_gs<<<g, kThreads, 0, c->stream>>>(B->gs_items, B->tiles + s.tile_off, s.ntiles, B->sc);
   else if (s.kind == 1)
     k_b_restrict<<<g, kThreads, 0, c->stream>>>(B->res_items, B->tiles + s.tile_off, s.ntiles, B->sc);
@@ -561,12 +640,56 @@ int build_graph(hpcg_b200_batch* B) {
   return st;
 }
 
+// GS phases on the bulk-copy kernel or on k_b_gs: the faster V-cycle (all
+// problems active, three rounds each way, round-robin), or HPCG_B200_BATCH_BULK.
+// Every V-cycle starts its sweeps from the right-hand side alone, so the work
+// vectors it leaves behind are rewritten by the next solve.
+int choose_bulk(hpcg_b200_batch* B) {
+  const char* force = std::getenv("HPCG_B200_BATCH_BULK");
+  if (force && *force) {
+    B->bulk = std::atoi(force) != 0;
+    return HPCG_B200_OK;
+  }
+  Context* c = B->ctx;
+  std::vector<BScal> on(B->m);
+  for (BScal& x : on) {
+    std::memset(&x, 0, sizeof(x));
+    x.active = 1;
+  }
+  HB_CK(cudaMemcpy(B->sc, on.data(), sizeof(BScal) * B->m, cudaMemcpyHostToDevice));
+  cudaEvent_t e0, e1;
+  HB_CK(cudaEventCreate(&e0));
+  HB_CK(cudaEventCreate(&e1));
+  float best[2] = {1e30f, 1e30f};
+  int st = HPCG_B200_OK;
+  for (int rep = 0; rep < 3 && st == HPCG_B200_OK; ++rep) {
+    for (int b = 0; b < 2 && st == HPCG_B200_OK; ++b) {
+      B->bulk = b != 0;
+      if (cudaEventRecord(e0, c->stream) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+      for (const Step& s : B->steps)
+        if (st == HPCG_B200_OK) st = launch_step(B, s);
+      if (st == HPCG_B200_OK && cudaEventRecord(e1, c->stream) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+      if (st == HPCG_B200_OK) st = stream_sync(c);
+      float ms = 0.f;
+      if (st == HPCG_B200_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+      if (st == HPCG_B200_OK && ms < best[b]) best[b] = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  HB_TRY(st);
+  B->bulk = best[1] < best[0];
+  HB_CK(cudaMemset(B->sc, 0, sizeof(BScal) * B->m));
+  return HPCG_B200_OK;
+}
+
 void destroy(hpcg_b200_batch* B) {
   if (!B) return;
   cudaSetDevice(B->device);
   if (B->ctx) cudaStreamSynchronize(B->ctx->stream);
   if (B->graph) cudaGraphExecDestroy(B->graph);
-  void* v[] = {B->gs_items, B->res_items, B->tiles, B->vec, B->vtiles, B->vrange, B->partials, B->sc, B->ctl};
+  void* v[] = {B->gs_items, B->res_items, B->tiles, B->gs_bitems, B->btiles, B->vec, B->vtiles, B->vrange,
+               B->partials, B->sc, B->ctl};
   for (void* q : v) cudaFree(q);
   for (float* q : B->val32) cudaFree(q);
   if (B->sc_host) cudaFreeHost(B->sc_host);
@@ -599,6 +722,7 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
   B->ctx = c;
   B->m = count;
   B->gs_items = nullptr; B->res_items = nullptr; B->tiles = nullptr; B->vec = nullptr; B->vtiles = nullptr;
+  B->gs_bitems = nullptr; B->btiles = nullptr; B->bulk = false;
   B->vrange = nullptr; B->partials = nullptr; B->sc = nullptr; B->sc_host = nullptr; B->ctl = nullptr;
   B->bytes = 0;
   B->graph = nullptr;
@@ -626,10 +750,10 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
     }
   }
   if (st == HPCG_B200_OK) {
-    std::vector<BGs> gs;
+    std::vector<BGs> gs, gsb;
     std::vector<BRes> res;
-    std::vector<BTile> tiles;
-    build_vcycle(B, 0, gs, res, tiles);
+    std::vector<BTile> tiles, btiles;
+    build_vcycle(B, 0, gs, res, tiles, gsb, btiles);
     std::vector<BVec> vec(count);
     std::vector<BTile> vt;
     std::vector<int> range(count + 1, 0);
@@ -645,6 +769,8 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
     st = alloc_copy(B, (void**)&B->gs_items, gs.data(), sizeof(BGs) * gs.size());
     if (!st && !res.empty()) st = alloc_copy(B, (void**)&B->res_items, res.data(), sizeof(BRes) * res.size());
     if (!st) st = alloc_copy(B, (void**)&B->tiles, tiles.data(), sizeof(BTile) * tiles.size());
+    if (!st) st = alloc_copy(B, (void**)&B->gs_bitems, gsb.data(), sizeof(BGs) * gsb.size());
+    if (!st) st = alloc_copy(B, (void**)&B->btiles, btiles.data(), sizeof(BTile) * btiles.size());
     if (!st) st = alloc_copy(B, (void**)&B->vec, vec.data(), sizeof(BVec) * vec.size());
     if (!st) st = alloc_copy(B, (void**)&B->vtiles, vt.data(), sizeof(BTile) * vt.size());
     if (!st) st = alloc_copy(B, (void**)&B->vrange, range.data(), sizeof(int) * range.size());
@@ -653,6 +779,7 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
     if (!st) st = dev_alloc((void**)&B->ctl, sizeof(BCtl), &B->bytes);
     if (!st && cudaMallocHost(&B->sc_host, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_NOMEM;
     if (!st && cudaMemset(B->sc, 0, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+    if (!st) st = choose_bulk(B);
   }
   if (st != HPCG_B200_OK) {
     destroy(B);
@@ -691,7 +818,7 @@ int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* B, const double* const* b, double*
   if (!B->graph) HB_TRY(build_graph(B));
   HB_CK(cudaGraphLaunch(B->graph, c->stream));
   HB_CK(cudaMemcpyAsync(B->sc_host, B->sc, sizeof(BScal) * B->m, cudaMemcpyDeviceToHost, c->stream));
-  HB_CK(cudaStreamSynchronize(c->stream));
+  HB_TRY(stream_sync(c));
   for (int p = 0; p < B->m; ++p) {
     niters[p] = B->sc_host[p].niters;
     normr[p] = std::sqrt(B->sc_host[p].normr2);

@@ -144,16 +144,27 @@ __device__ __forceinline__ void record_fault(unsigned* fault, unsigned code) {
   __threadfence_system();
 }
 
+// Where a tile comes from: its first row and, when the tile is one block of
+// the layout (whole-tile copies), the addresses of its value and column blocks.
+template <typename T>
+struct TileSrc {
+  int64_t q0;
+  const T* vals;
+  const int* cols;
+};
+
 // The producer/consumer pipeline of the bulk-copy kernels, run by the whole
-// block: the block's tiles are blockIdx.x, + gridDim.x, ... below ntiles; tile
-// `tile` holds rows first_row(tile) .. + kBulkRows. Each consumer thread calls
-// row(q0, sv, sc, t) for every tile of its group, t its index in the group
-// (row t / LANES of the tile, lane t % LANES), with the tile's values
-// sv[k * kBulkRows + row] and columns sc[k * kBulkRows + row] on chip.
-template <typename T, typename Shape, typename FirstRow, typename RowFn>
-__device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
-                                           int ntiles, FirstRow first_row, RowFn row, unsigned* fault,
-                                           const CUtensorMap& tm_val, const CUtensorMap& tm_col) {
+// block. The block's tiles are blockIdx.x, + gridDim.x, ... below ntiles, less
+// those for which skip(tile) holds (every thread of the block must get the same
+// answer); the i-th tile kept goes to consumer group i mod G. src(tile) gives
+// the tile's TileSrc; the tensor maps (FP64 tiles only) are kernel parameters.
+// Each consumer thread calls row(tile, q0, sv, sc, t) for
+// every tile of its group, t its index in the group (row t / LANES of the tile,
+// lane t % LANES), with the tile's values sv[k * kBulkRows + row] and columns
+// sc[k * kBulkRows + row] on chip.
+template <typename T, typename Shape, typename Src, typename Skip, typename RowFn>
+__device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, RowFn row, unsigned* fault,
+                                               const CUtensorMap* tm_val, const CUtensorMap* tm_col) {
   constexpr int G = Shape::groups;
   constexpr int RING = Shape::ring;
   constexpr int S = Shape::stages;
@@ -181,8 +192,9 @@ __device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int*
     int last[S];  // last fill issued into each stage (-1: none)
 #pragma unroll
     for (int s = 0; s < S; ++s) last[s] = -1;
-    int i = 0;  // block-local tile number: group i % G, its (i / G)-th tile
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+    int i = 0;  // tiles kept so far: tile i goes to group i % G, as its (i / G)-th
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      if (skip(tile)) continue;
       const int kg = i / G;
       const int s = (i % G) * RING + kg % RING, use = kg / RING;
       int ok = 1;
@@ -195,21 +207,22 @@ __device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int*
         }
       }
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
-      const int64_t q0 = first_row(tile);
+      const TileSrc<T> ts = src(tile);
       T* sv = reinterpret_cast<T*>(smem + s * SB);
       int* sc = reinterpret_cast<int*>(smem + s * SB + VB);
       if constexpr (bulk_whole_tile<T>()) {
         // the tile is one block of the layout: all slots' values in one run, all columns in another
-        if (lane == 0) bulk_g2s(sv, val + mat_index<T>(0, q0, pitch), VB, &full[s], policy);
-        if (lane == 1) bulk_g2s(sc, col + mat_index<T>(0, q0, pitch), kSlots * kBulkRows * sizeof(int), &full[s], policy);
+        if (lane == 0) bulk_g2s(sv, ts.vals, VB, &full[s], policy);
+        if (lane == 1) bulk_g2s(sc, ts.cols, kSlots * kBulkRows * sizeof(int), &full[s], policy);
       } else {
         // rows q0 .. q0 + kBulkRows of all 27 slots, [slot][row] in shared memory
-        if (lane == 0) tma_load_2d(sv, &tm_val, (int)q0, 0, &full[s], policy);
-        if (lane == 1) tma_load_2d(sc, &tm_col, (int)q0, 0, &full[s], policy);
+        if (lane == 0) tma_load_2d(sv, tm_val, (int)ts.q0, 0, &full[s], policy);
+        if (lane == 1) tma_load_2d(sc, tm_col, (int)ts.q0, 0, &full[s], policy);
       }
 #pragma unroll
       for (int u = 0; u < S; ++u)
         if (u == s) last[u] = use;
+      ++i;
     }
     // no copy may still be landing when the block exits: the last fill of
     // every stage has completed (consumed or not)
@@ -222,18 +235,39 @@ __device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int*
   } else {
     const int g = (warp - 1) / (Shape::group_threads / 32);   // consumer group
     const int t = (threadIdx.x - 32) % Shape::group_threads;  // index in the group
-    int kg = 0;                                    // the group's tile count
-    for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles; tile += G * gridDim.x, ++kg) {
-      const int s = g * RING + kg % RING, use = kg / RING;
-      if (!mbar_wait(&full[s], use & 1)) {
-        record_fault(fault, 3);
-        break;
+    int i = 0;                                                // tiles kept so far
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      if (skip(tile)) continue;
+      if (i % G == g) {
+        const int kg = i / G;
+        const int s = g * RING + kg % RING, use = kg / RING;
+        if (!mbar_wait(&full[s], use & 1)) {
+          record_fault(fault, 3);
+          break;
+        }
+        row(tile, src(tile).q0, reinterpret_cast<const T*>(smem + s * SB),
+            reinterpret_cast<const int*>(smem + s * SB + VB), t);
+        mbar_arrive(&empty[s]);
       }
-      row(first_row(tile), reinterpret_cast<const T*>(smem + s * SB),
-          reinterpret_cast<const int*>(smem + s * SB + VB), t);
-      mbar_arrive(&empty[s]);
+      ++i;
     }
   }
+}
+
+// The common case: one matrix (val, col, pitch), tile `tile` starting at row
+// first_row(tile), no tile skipped; row(q0, sv, sc, t).
+template <typename T, typename Shape, typename FirstRow, typename RowFn>
+__device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                                           int ntiles, FirstRow first_row, RowFn row, unsigned* fault,
+                                           const CUtensorMap& tm_val, const CUtensorMap& tm_col) {
+  bulk_tiles_src<T, Shape>(
+      ntiles,
+      [&](int tile) {
+        const int64_t q0 = first_row(tile);
+        return TileSrc<T>{q0, val + mat_index<T>(0, q0, pitch), col + mat_index<T>(0, q0, pitch)};
+      },
+      [](int) { return false; },
+      [&](int, int64_t q0, const T* sv, const int* sc, int t) { row(q0, sv, sc, t); }, fault, &tm_val, &tm_col);
 }
 
 }  // namespace hb

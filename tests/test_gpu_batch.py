@@ -55,3 +55,29 @@ def test_batch_device_vectors_and_errors(binding, batch):
     with pytest.raises(binding.HpcgError) as e:
         binding.Batch([(24, 24, 24)])
     assert e.value.status == binding.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("bulk", ["0", "1"])
+def test_batch_both_phase_kernels_follow_single_solves(binding, monkeypatch, bulk):
+    """The batched colour phases on the 256-row register kernel and on the
+    bulk-copy kernel (128-row blocks of each problem's blocked FP32 copy, the
+    tiles of converged problems skipped): each follows its one-at-a-time solve,
+    including a problem that converges early (zero right-hand side)."""
+    monkeypatch.setenv("HPCG_B200_BATCH_BULK", bulk)
+    B = binding.Batch([(16, 32, 48), (32, 16, 16), (16, 16, 16)])
+    try:
+        bs = [p.get_rhs() for p in B.problems]
+        bs[2] = np.zeros_like(bs[2])
+        xs = [np.zeros(p.nrow) for p in B.problems]
+        ni, nr, nr0 = B.CG_mixed(bs, xs, 8, 0.0)
+        assert ni[2] == 0 and nr0[2] == 0.0
+        for i in (0, 1):
+            p = B.problems[i]
+            x1 = np.zeros(p.nrow)
+            n1, r1, r01 = p.CG_mixed(bs[i], x1, 8, 0.0)
+            assert ni[i] == n1 == 8
+            s = r1 / r01
+            assert abs(nr[i] / nr0[i] - s) <= 1e-10 * max(s, 1e-9), (i, nr[i] / nr0[i], s)
+            assert np.max(np.abs(xs[i] - x1)) <= 1e-9 * max(np.max(np.abs(x1)), 1.0)
+    finally:
+        B.free()
