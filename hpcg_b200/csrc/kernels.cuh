@@ -768,13 +768,59 @@ __global__ void __launch_bounds__(kThreads) k_update_p(int n, const double* __re
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = z[i] + beta * p[i];
 }
 
-// Iteration 1: p = z (CG.cpp:109); later iterations: p = z + beta p (CG.cpp:115).
-__global__ void __launch_bounds__(kThreads) k_update_p_iter(int n, const double* __restrict__ z, double* p,
-                                                            const Scalars* __restrict__ s) {
-  const bool first = s->iter == 0;
-  const double beta = s->beta;
+// p = z + beta p with the previous iteration's x update folded in: x = x +
+// alpha p (CG.cpp:121, alpha still the previous iteration's) reads the p that
+// this kernel reads anyway, so the x/r update that follows the SpMV need not
+// read p again. The same operations on the same values as k_update_p after
+// k_update_xr. first (iteration 1): p = z (CG.cpp:109), x untouched.
+__device__ __forceinline__ void update_px(int n, const double* __restrict__ z, double* p, double* x,
+                                          const Scalars* __restrict__ s, bool first) {
+  const double beta = s->beta, alpha = s->alpha;
   const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = first ? z[i] : z[i] + beta * p[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    if (first) {
+      p[i] = z[i];
+    } else {
+      const double pi = p[i];
+      x[i] = x[i] + alpha * pi;
+      p[i] = z[i] + beta * pi;
+    }
+  }
+}
+__global__ void __launch_bounds__(kThreads) k_update_px(int n, const double* __restrict__ z, double* p, double* x,
+                                                        const Scalars* __restrict__ s) {
+  update_px(n, z, p, x, s, false);
+}
+// iteration-aware form for the graph's loop body (s->iter: iterations completed)
+__global__ void __launch_bounds__(kThreads) k_update_px_iter(int n, const double* __restrict__ z, double* p,
+                                                             double* x, const Scalars* __restrict__ s) {
+  update_px(n, z, p, x, s, s->iter == 0);
+}
+
+// r = r + (-alpha) Ap (CG.cpp:122) and partials of r'r (CG.cpp:123); x waits
+// for the next k_update_px (or k_update_x after the loop).
+__global__ void __launch_bounds__(kThreads) k_update_r(int n, double* r, const double* __restrict__ Ap,
+                                                       const Scalars* __restrict__ s, double* __restrict__ partials) {
+  const double malpha = -s->alpha;
+  const int stride = gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double ri = r[i] + malpha * Ap[i];
+    r[i] = ri;
+    acc += ri * ri;
+  }
+  const double sum = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+}
+
+// The last iteration's x = x + alpha p (CG.cpp:121), after the loop; with
+// iter_gate, only if the graph's loop completed an iteration (s->iter > 0).
+__global__ void __launch_bounds__(kThreads) k_update_x(int n, double* x, const double* __restrict__ p,
+                                                       const Scalars* __restrict__ s, int iter_gate) {
+  if (iter_gate && s->iter == 0) return;
+  const double alpha = s->alpha;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = x[i] + alpha * p[i];
 }
 
 // The loop condition of CG.cpp:100, k <= max_iter && normr/normr0 > tolerance,

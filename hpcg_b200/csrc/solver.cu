@@ -624,12 +624,12 @@ int cg_iteration_body(hpcg_b200_problem* P, bool prec) {
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, nb, kFinRtzIter));
   }
-  k_update_p_iter<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);
+  k_update_px_iter<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, P->x, c->scal);  // with x of the last iteration
   HB_CK(cudaGetLastError());
   const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize(c, gs, kFinPap));
-  k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);
+  k_update_r<<<nb, kThreads, 0, c->stream>>>(n, P->r, P->Ap, c->scal, c->partials);
   HB_CK(cudaGetLastError());
   return finalize(c, nb, kFinNormr);
 }
@@ -725,6 +725,9 @@ int run_cg_graph(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int*
   cudaGraphExec_t& ex = P->cg_graph[prec ? 1 : 0];
   if (!ex) HB_TRY(build_cg_graph(P, prec, &ex));
   HB_CK(cudaGraphLaunch(ex, c->stream));
+  // the last iteration's x update (CG.cpp:121), if the loop ran one
+  k_update_x<<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, P->x, P->p, c->scal, 1);
+  HB_CK(cudaGetLastError());
   HB_TRY(read_scalars(c));
   *niters = c->scal_host->iter;
   *normr_out = std::sqrt(c->scal_host->normr2);
@@ -790,7 +793,7 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
       HB_CK(cudaMemcpyAsync(P->p, P->z, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :109
     } else {
       HB_TRY(finalize(c, rz_parts, kFinRtz));
-      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, c->scal);  // :115
+      k_update_px<<<gv, kThreads, 0, c->stream>>>(n, P->z, P->p, P->x, c->scal);  // :115, and :121 of k - 1
       HB_CK(cudaGetLastError());
     }
     HB_TRY(mark());
@@ -801,13 +804,17 @@ int run_cg(hpcg_b200_problem* P, int max_iter, double tol, bool prec, int* niter
     HB_TRY(prof_end(c, kProfSpmv, ev0, n));
     HB_TRY(finalize(c, gs, kFinPap));                                       // :118-120
     HB_TRY(mark());
-    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials);  // :121-123
+    k_update_r<<<nb, kThreads, 0, c->stream>>>(n, P->r, P->Ap, c->scal, c->partials);  // :122-123 (x: next :115)
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, nb, kFinNormr));
     HB_TRY(mark());
     HB_TRY(read_scalars(c));
     normr = std::sqrt(c->scal_host->normr2);
     *niters = k;
+  }
+  if (*niters > 0) {  // the last iteration's x update (CG.cpp:121)
+    k_update_x<<<gv, kThreads, 0, c->stream>>>(n, P->x, P->p, c->scal, 0);
+    HB_CK(cudaGetLastError());
   }
   *normr_out = normr;
   *normr0_out = normr0;

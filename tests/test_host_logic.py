@@ -131,7 +131,8 @@ def test_gpu_launch_count_model():
     import bench
     # 16 launches per symmetric sweep would double count; the model is 15 per sweep.
     # Per iteration besides the V-cycle: r'z finalize (partials from the
-    # post-smoother), p update, SpMV + finalize, x/r update + finalize = 6, which
-    # makes the 117 launches per iteration of the 512^3 launch list.
-    assert bench.gpu_launches_per_set(1) == (32 * 3 + 15) + 6 - 1 + 3 + 3
+    # post-smoother), p update (with the previous x update), SpMV + finalize,
+    # r update + finalize = 6, which makes the 117 launches per iteration of the
+    # 512^3 launch list; one x update after the loop.
+    assert bench.gpu_launches_per_set(1) == (32 * 3 + 15) + 6 - 1 + 3 + 3 + 1
     assert bench.gpu_launches_per_set(2) - bench.gpu_launches_per_set(1) == 117
