@@ -225,6 +225,8 @@ struct hpcg_b200_problem {
   hb::MultiState* multi;  // work vectors of the multi-system path (created on first use)
   cudaGraphExec_t cg_graph[2];  // instantiated CG loop, [unpreconditioned, preconditioned]
   bool cg_graph_failed;         // capture was refused once: stay with stream launches
+  cudaGraphExec_t coarse_graph[2];  // the V-cycle below level 0 as one graph, [FP64, FP32]
+  bool coarse_graph_failed;         // its capture was refused once: stream launches
   hb::RankGeom* geom;  // position in a run over several ranks (nullptr: one rank)
   size_t bytes;  // device bytes held
 };

@@ -23,6 +23,13 @@ int alloc_n(hpcg_b200_problem* p, T** ptr, int64_t count) {
   return dev_alloc((void**)ptr, sizeof(T) * (size_t)count, &p->bytes);
 }
 
+// Releases the captured coarse V-cycle (0: FP64, 1: FP32); the next stream-run
+// V-cycle captures it again.
+void drop_coarse_graph(hpcg_b200_problem* p, int which) {
+  if (p->coarse_graph[which]) cudaGraphExecDestroy(p->coarse_graph[which]);
+  p->coarse_graph[which] = nullptr;
+}
+
 hpcg_b200_problem* new_problem(int device, Context* c) {
   hpcg_b200_problem* p = new hpcg_b200_problem;
   std::memset(p, 0, sizeof(*p));
@@ -209,8 +216,10 @@ int free_problem(hpcg_b200_problem* p) {
   for (void* q : vs) dev_free(q);
   free_multi(p);
   free_plans(p);
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < 2; ++i) {
     if (p->cg_graph[i]) cudaGraphExecDestroy(p->cg_graph[i]);
+    if (p->coarse_graph[i]) cudaGraphExecDestroy(p->coarse_graph[i]);
+  }
   release_accounted(p->bytes);
   p->magic = 0;
   delete p;
@@ -489,6 +498,7 @@ int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal) {
     L.val32 = nullptr;
     dev_free(L.col32);
     L.col32 = nullptr;
+    drop_coarse_graph(p, 1);  // it holds the old copy's addresses
   }
   HB_CK(cudaStreamSynchronize(c->stream));
   return HPCG_B200_OK;
@@ -525,6 +535,7 @@ int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27
     L.val32 = nullptr;
     dev_free(L.col32);
     L.col32 = nullptr;
+    drop_coarse_graph(p, 1);  // it holds the old copy's addresses
   }
   return HPCG_B200_OK;
 }
@@ -538,6 +549,7 @@ int hpcg_b200_set_symgs_mode(hpcg_b200_problem* p, int mode) {
     for (int i = 0; i < 2; ++i) {
       if (p->cg_graph[i]) cudaGraphExecDestroy(p->cg_graph[i]);
       p->cg_graph[i] = nullptr;
+      drop_coarse_graph(p, i);
     }
   }
   p->symgs_mode = mode;

@@ -421,6 +421,8 @@ int symgs_level(hpcg_b200_problem* p, int l, const double* rhs, double* x, bool 
   return gs_colour<double, double>(c, L, L.val, rhs, x, x_is_zero, l == 0, dot);
 }
 
+int coarse_vcycle(hpcg_b200_problem* p, bool f32);
+
 // ComputeMG_ref.cpp:39-63 on colour-order device vectors of level l. rtz (level
 // 0, colour mode): the post-smoother also leaves the block partials of r'x in
 // rtz[0 .. kColours * kDotStride), zeroed here first.
@@ -435,7 +437,7 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x, double* rt
     restrict_dispatch<double>(c, L, L.val, r, x, C.r, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY(prof_end(c, l == 0 ? kProfRestrict : -1, ev0, C.n));
-    HB_TRY(mg_level(p, l + 1, C.r, C.x));
+    HB_TRY(l == 0 ? coarse_vcycle(p, false) : mg_level(p, l + 1, C.r, C.x));
     k_prolong<double><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x, x, C.n);
     HB_CK(cudaGetLastError());
     if (rtz) HB_CK(cudaMemsetAsync(rtz, 0, sizeof(double) * kColours * kDotStride, c->stream));
@@ -601,6 +603,44 @@ double now_s() {
 bool graph_enabled() {
   const char* e = std::getenv("HPCG_B200_GRAPH");
   return !(e && e[0] == '0');
+}
+
+int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x);
+
+// The V-cycle below level 0 (levels 1 .. nlev-1 between the level-0 restriction
+// and prolongation, on the fixed coarse vectors r, x of level 1) for the loops
+// that launch kernel by kernel: captured once as a CUDA graph and launched as
+// one unit, so that its small coarse-level kernels (about 80 of the 117
+// launches of a CG iteration) cost one launch instead of one each. Inside a
+// capture (the CG loop's own graph) and in the natural-order mode the kernels
+// are launched directly; the same kernels either way, so the same bits.
+int coarse_vcycle(hpcg_b200_problem* p, bool f32) {
+  Context* c = p->ctx;
+  auto direct = [&]() -> int {
+    return f32 ? mg32_level(p, 1, p->lev[1].r32, p->lev[1].x32) : mg_level(p, 1, p->lev[1].r, p->lev[1].x);
+  };
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HB_CK(cudaStreamIsCapturing(c->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone || p->coarse_graph_failed || !graph_enabled() ||
+      p->symgs_mode != HPCG_B200_SYMGS_COLOUR)
+    return direct();
+  cudaGraphExec_t& ex = p->coarse_graph[f32 ? 1 : 0];
+  if (!ex) {
+    HB_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = direct();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (st == HPCG_B200_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (st != HPCG_B200_OK || e != cudaSuccess) {  // refused: stream launches from now on
+      cudaGetLastError();
+      ex = nullptr;
+      p->coarse_graph_failed = true;
+      return direct();
+    }
+  }
+  HB_CK(cudaGraphLaunch(ex, c->stream));
+  return HPCG_B200_OK;
 }
 
 // One CG iteration (CG.cpp:101-125) with the iteration-aware kernels: the body
@@ -934,7 +974,7 @@ int mg32_level(hpcg_b200_problem* p, int l, const float* r, float* x) {
     Level& C = p->lev[l + 1];
     restrict_dispatch<float>(c, L, L.val32, r, x, C.r32, C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY(mg32_level(p, l + 1, C.r32, C.x32));
+    HB_TRY(l == 0 ? coarse_vcycle(p, true) : mg32_level(p, l + 1, C.r32, C.x32));
     k_prolong<float><<<grid_for(c, C.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.tf, L.tq, C.x32, x, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY((gs_colour<float, float>(c, L, L.val32, r, x, false, l == 0)));

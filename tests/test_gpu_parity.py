@@ -673,3 +673,35 @@ def test_bounded_wait_gives_up_and_context_survives(oracle, binding, case16):
     assert np.array_equal(z, exp)
     with pytest.raises(binding.HpcgError):
         binding._check(binding.lib().hpcg_b200_wait_selftest(0, 5.0), "wait_selftest")
+
+
+def test_stream_vcycle_follows_coarse_value_changes(oracle, binding):
+    """The loops that launch kernel by kernel run the V-cycle below level 0 as
+    one captured graph. After set_values on a coarse level (which rebuilds that
+    level's FP32 copy at a new address), the FP64 and FP32 V-cycles equal those
+    of a problem built with the new values from the start."""
+    P = oracle.generate(32)
+    lv = levels_of(P)
+    lv2 = [dict(d) for d in lv]
+    lv2[1]["vals"] = lv[1]["vals"] * 1.5
+    D1 = binding.Problem.optimize(lv)
+    D2 = binding.Problem.optimize(lv2)
+    try:
+        n = P.levels[0].n
+        r = np.random.default_rng(17).standard_normal(n)
+        z = np.zeros(n)
+        D1.ComputeMG(r, z)
+        D1.ComputeMG_f32(r, z)  # both coarse graphs captured on the old values
+        e = D2.export_level(1)
+        m = e["n"]
+        v27 = np.zeros((m, 27))
+        v27[e["new2old"]] = e["vals"][:, :m].T
+        D1.set_values(1, v27)
+        for f in (lambda D, x: D.ComputeMG(r, x), lambda D, x: D.ComputeMG_f32(r, x)):
+            a, b = np.zeros(n), np.zeros(n)
+            f(D1, a)
+            f(D2, b)
+            assert np.array_equal(a, b)
+    finally:
+        D1.free()
+        D2.free()
