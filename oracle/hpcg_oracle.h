@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY. Nothing in the product library links or calls this
  * code; only the test-suite, the smoke check and the CPU-baseline leg of the
- * benchmark load it, and only as the checker.
+ * benchmark load it, and only to compare results against.
  *
  * It restates, in plain C99 with strict IEEE-754 double arithmetic (built with
  * -ffp-contract=off, no fast-math), the reference routines of HPCG 3.1:

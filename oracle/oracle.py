@@ -1,9 +1,9 @@
-"""ctypes front end to the CPU checkers. TEST INFRASTRUCTURE ONLY.
+"""ctypes front end to the CPU references the tests compare against. TEST INFRASTRUCTURE ONLY.
 
 Only the test-suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this module, and only to check or time against it.
 
-Two checkers live here:
+Two CPU references live here:
 
 * ``liboracle.so`` -- the C restatement of the HPCG 3.1 reference path
   (``hpcg_oracle.c``; each routine cites the reference file:line it follows).
