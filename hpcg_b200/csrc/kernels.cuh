@@ -798,15 +798,18 @@ __global__ void __launch_bounds__(kThreads) k_update_px_iter(int n, const double
 }
 
 // r = r + (-alpha) Ap (CG.cpp:122) and partials of r'r (CG.cpp:123); x waits
-// for the next k_update_px (or k_update_x after the loop).
+// for the next k_update_px (or k_update_x after the loop). r32 (the mixed
+// form): also r narrowed to FP32 for the next V-cycle.
 __global__ void __launch_bounds__(kThreads) k_update_r(int n, double* r, const double* __restrict__ Ap,
-                                                       const Scalars* __restrict__ s, double* __restrict__ partials) {
+                                                       const Scalars* __restrict__ s, double* __restrict__ partials,
+                                                       float* __restrict__ r32 = nullptr) {
   const double malpha = -s->alpha;
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const double ri = r[i] + malpha * Ap[i];
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   const double sum = block_sum(acc);
@@ -842,10 +845,9 @@ __global__ void k_cg_setup(Scalars* s, int max_iter, double tol) {
 }
 
 // x = x + alpha p; r = r + (-alpha) Ap (CG.cpp:121-122); partials of r'r (CG.cpp:123).
-// r32 (the mixed form): also r narrowed to FP32 for the next V-cycle.
 __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const double* __restrict__ p, double* r,
                                                         const double* __restrict__ Ap, const Scalars* __restrict__ s,
-                                                        double* __restrict__ partials, float* __restrict__ r32 = nullptr) {
+                                                        double* __restrict__ partials) {
   const double alpha = s->alpha, malpha = -s->alpha;
   const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
@@ -853,7 +855,6 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const 
     x[i] = x[i] + alpha * p[i];
     const double ri = r[i] + malpha * Ap[i];
     r[i] = ri;
-    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   const double sum = block_sum(acc);

@@ -1019,19 +1019,23 @@ int run_cg_mixed(hpcg_b200_problem* P, int max_iter, double tol, int* niters, do
       k_widen_dot<true><<<nb, kThreads, 0, c->stream>>>(n, L.x32, P->r, zc, zp, c->partials);
       HB_CK(cudaGetLastError());
       HB_TRY(finalize(c, nb, kFinFlex));
-      k_update_p<<<gv, kThreads, 0, c->stream>>>(n, zc, P->p, c->scal);
+      k_update_px<<<gv, kThreads, 0, c->stream>>>(n, zc, P->p, P->x, c->scal);  // with x of iteration k - 1
       HB_CK(cudaGetLastError());
     }
     std::swap(zc, zp);
     const int gs = spmv_dispatch<double, true>(c, L, L.val, P->p, P->Ap, c->partials);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, gs, kFinPap));
-    k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, P->x, P->p, P->r, P->Ap, c->scal, c->partials, L.r32);
+    k_update_r<<<nb, kThreads, 0, c->stream>>>(n, P->r, P->Ap, c->scal, c->partials, L.r32);
     HB_CK(cudaGetLastError());
     HB_TRY(finalize(c, nb, kFinNormr));
     HB_TRY(read_scalars(c));
     normr = std::sqrt(c->scal_host->normr2);
     *niters = k;
+  }
+  if (*niters > 0) {  // the last iteration's x update
+    k_update_x<<<gv, kThreads, 0, c->stream>>>(n, P->x, P->p, c->scal, 0);
+    HB_CK(cudaGetLastError());
   }
   *normr_out = normr;
   *normr0_out = normr0;
