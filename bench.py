@@ -291,6 +291,7 @@ def multi_rhs(dev, n=256, k=8, tol=1e-9, max_iter=2000):
         x.zero_()
         (ni, nr, nr0), t_multi = timed(lib_stream, lambda: P.CG_multi(b, x, max_iter, tol))
         xs = torch.zeros(nrow, dtype=torch.float64, device=f"cuda:{dev}")
+        P.CG(b[0].contiguous(), xs, 1, tol, True)  # untimed: the single-system tuning and CG graph
         iters_single, t_single = [], 0.0
         for j in range(k):
             xs.zero_()
