@@ -26,6 +26,11 @@ struct MultiState {
   MScalars* s = nullptr;
   MScalars* s_host = nullptr;
   size_t bytes = 0;
+  // the V-cycle below level 0 as one captured graph (see coarse_m)
+  cudaGraphExec_t coarse = nullptr;
+  int coarse_key = -1;         // lanes * 4 + bulk of the captured kernels
+  bool coarse_failed = false;  // a capture was refused: stream launches from then on
+  bool tuning = false;         // while the forms are being timed, no graph
 };
 
 namespace {
@@ -41,6 +46,7 @@ void free_state(MultiState* m) {
     cudaFree(m->lx[l]);
   }
   if (m->s_host) cudaFreeHost(m->s_host);
+  if (m->coarse) cudaGraphExecDestroy(m->coarse);
   release_accounted(m->bytes);
   delete m;
 }
@@ -118,6 +124,7 @@ int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
   cudaEvent_t e0, e1;
   HB_CK(cudaEventCreate(&e0));
   HB_CK(cudaEventCreate(&e1));
+  m->tuning = true;
   float t_[3][3];  // [lanes 1, 2, 4][bulk 0, 1, 2]
   for (auto& row : t_)
     for (float& v : row) v = 1e30f;
@@ -140,6 +147,7 @@ int tune_lanes(hpcg_b200_problem* P, MultiState* m) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  m->tuning = false;
   HB_TRY(st);
   int bl = 0, bb = 0;
   for (int li = 0; li < 3; ++li)
@@ -282,6 +290,9 @@ int gs_colour_m(Context* c, const Level& L, const double* rhs, double* x, bool f
   return HPCG_B200_OK;
 }
 
+template <int K, int LANES, int BULK>
+int coarse_m(hpcg_b200_problem* P, MultiState* m);
+
 // ComputeMG_ref.cpp:39-63 for K systems on level l (colour order, interleaved).
 template <int K, int LANES, int BULK>
 int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x) {
@@ -294,12 +305,50 @@ int mg_m(hpcg_b200_problem* P, MultiState* m, int l, const double* r, double* x)
     kr<<<grid_of(c, kr, (int64_t)C.n * LANES), kThreads, 0, c->stream>>>(L.val, L.col, L.pitch, r, x, L.tf, L.tq,
                                                                           m->lr[l + 1], C.n);
     HB_CK(cudaGetLastError());
-    HB_TRY((mg_m<K, LANES, BULK>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1])));
+    if (l == 0) {
+      HB_TRY((coarse_m<K, LANES, BULK>(P, m)));
+    } else {
+      HB_TRY((mg_m<K, LANES, BULK>(P, m, l + 1, m->lr[l + 1], m->lx[l + 1])));
+    }
     auto kp = k_prolong_m<K>;
     kp<<<grid_of(c, kp, C.n), kThreads, 0, c->stream>>>(L.tf, L.tq, m->lx[l + 1], x, C.n);
     HB_CK(cudaGetLastError());
     HB_TRY((gs_colour_m<K, LANES, BULK>(c, L, r, x, false)));
   }
+  return HPCG_B200_OK;
+}
+
+// The levels below 0 of a K-system V-cycle as one captured CUDA graph (its
+// small coarse kernels cost one launch), recaptured when the lanes or the
+// kernel form change; launched directly while the forms are being timed, inside
+// another capture, or with HPCG_B200_GRAPH=0. The same kernels either way.
+template <int K, int LANES, int BULK>
+int coarse_m(hpcg_b200_problem* P, MultiState* m) {
+  Context* c = P->ctx;
+  auto direct = [&]() -> int { return mg_m<K, LANES, BULK>(P, m, 1, m->lr[1], m->lx[1]); };
+  const char* ge = std::getenv("HPCG_B200_GRAPH");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HB_CK(cudaStreamIsCapturing(c->stream, &cs));
+  if (m->tuning || m->coarse_failed || (ge && ge[0] == '0') || cs != cudaStreamCaptureStatusNone) return direct();
+  const int key = LANES * 4 + BULK;
+  if (!m->coarse || m->coarse_key != key) {
+    if (m->coarse) cudaGraphExecDestroy(m->coarse);
+    m->coarse = nullptr;
+    HB_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = direct();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (st == HPCG_B200_OK && e == cudaSuccess) e = cudaGraphInstantiate(&m->coarse, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (st != HPCG_B200_OK || e != cudaSuccess) {
+      cudaGetLastError();
+      m->coarse = nullptr;
+      m->coarse_failed = true;
+      return direct();
+    }
+    m->coarse_key = key;
+  }
+  HB_CK(cudaGraphLaunch(m->coarse, c->stream));
   return HPCG_B200_OK;
 }
 
