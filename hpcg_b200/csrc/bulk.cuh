@@ -139,6 +139,14 @@ __device__ __forceinline__ uint64_t evict_first_policy() {
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the kernel before it on the stream finishes;
+// griddep_wait() returns once that kernel has completed and its writes are
+// visible (at once for a kernel launched without the attribute), and
+// griddep_launch_dependents() lets the next such kernel start.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 __device__ __forceinline__ void record_fault(unsigned* fault, unsigned code) {
   *(volatile unsigned*)fault = code;
   __threadfence_system();
@@ -183,6 +191,13 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
     mbar_init_fence();
   }
   __syncthreads();
+  // Under a programmatic dependent launch the producer streams the first tiles
+  // while the previous kernel finishes: it reads only the matrix, and every
+  // kernel that writes a matrix array is followed by a stream synchronisation.
+  // (The batched kernel's skip predicate reads convergence flags; it is
+  // launched without the attribute, so the wait is already over.) The
+  // consumers read and write the vectors: they wait for that kernel first.
+  if (threadIdx.x == 0) griddep_launch_dependents();
   const int warp = threadIdx.x >> 5;
   if (warp == 0) {
     // the producer warp: lane 0 waits for a free stage and posts the byte
@@ -233,6 +248,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
     }
     __syncwarp();
   } else {
+    griddep_wait();
     const int g = (warp - 1) / (Shape::group_threads / 32);   // consumer group
     const int t = (threadIdx.x - 32) % Shape::group_threads;  // index in the group
     int i = 0;                                                // tiles kept so far

@@ -77,8 +77,24 @@ bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   const int64_t tiles = ((int64_t)r1 - a0 + kBulkRows - 1) / kBulkRows;
   int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
   if (DOT && g > kDotStride) g = kDotStride;
-  k<<<g, GsShape<T>::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault,
-                                                  *tv, *tc);
+  // programmatic dependent launch: the phase's producer streams its first
+  // matrix tiles while the previous kernel finishes (HPCG_B200_PDL=0: off)
+  static const bool pdl = [] {
+    const char* e = std::getenv("HPCG_B200_PDL");
+    return !(e && e[0] == '0');
+  }();
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(g);
+  cfg.blockDim = dim3(GsShape<T>::threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault, *tv, *tc);
   return true;
 }
 
@@ -897,6 +913,9 @@ int ensure_f32(hpcg_b200_problem* P) {
       k_block32<<<grid_for(c, (int64_t)kSlots * L.pitch, kThreads, kPerSm), kThreads, 0, c->stream>>>(
           L.val, L.col, L.pitch, L.val32, L.col32);
       HB_CK(cudaGetLastError());
+      // a Gauss-Seidel phase launched next may read the copy before this
+      // kernel is done (its producer does not wait): finish it here
+      HB_TRY(stream_sync(c));
     }
     if (!L.r32) {
       HB_TRY(dev_alloc((void**)&L.r32, sizeof(float) * L.pitch, &P->bytes));
