@@ -379,7 +379,8 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
     fi_ms, fi_l, fi_rows = B.profile_read(B.PROF_GS32_FIRST, dev)
     B.profile(False, dev)
     peak, _ = measured_peak_hbm()
-    full_gbs = metrics.gs_phase_bytes(fu_rows, n, vb=4) / (fu_ms * 1e-3) / 1e9 if fu_ms else None
+    packed = P.level_packed(0) > 0 and P.level_config(0)["gs32"] == 10
+    full_gbs = metrics.gs_phase_bytes(fu_rows, n, vb=4, packed=packed) / (fu_ms * 1e-3) / 1e9 if fu_ms else None
     first_gbs = metrics.first_sweep_bytes(fi_rows, vb=4) / (fi_ms * 1e-3) / 1e9 if fi_ms else None
     return {"fp64": {"iters": it64, "seconds": round(t64, 3), "scaled_residual": nr64 / nr064},
             "fp32_vcycle": {"iters": it32, "seconds": round(t32, 3), "scaled_residual": nr32 / nr032,
@@ -392,7 +393,9 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
                 "full_frac": round(full_gbs / peak, 4) if full_gbs else None,
                 "first_ms_per_iter": round(fi_ms / profile_iters, 3),
                 "first_gbs": round(first_gbs, 1) if first_gbs else None,
-                "bytes_per_row": {"full": 252, "first_sweep": 130}}}
+                "bytes_per_row": {"full": round(metrics.gs_phase_bytes(1, 8, vb=4, packed=packed), 3),
+                                  "first_sweep": 130},
+                "packed_columns": packed}}
 
 
 def gpu_launches_per_set(iters, nlevels=4):
@@ -549,14 +552,19 @@ def b200_arm(args, rank, world, local_rank):
     tuning = [P.level_config(l) for l in range(4)]
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
-        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow)
-        achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
         gs_cfg = tuning[0]["gs"]
-        kernel = (f"k_gs_bulk<double,double,false> (level 0, configuration {gs_cfg})" if gs_cfg == 10 else
+        packed0 = P.level_packed(0) > 0
+        gs_packed = packed0 and gs_cfg == 10
+        mv_packed = packed0 and tuning[0]["spmv"] == 7
+        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow, packed=gs_packed)
+        achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
+        kernel = (f"k_gs_bulk<double,double,false> (level 0, configuration {gs_cfg}"
+                  f"{', packed columns' if gs_packed else ''})" if gs_cfg == 10 else
                   f"k_gs_phase<double,double,false> (level 0, configuration {gs_cfg})")
         tr = committed_traffic()
         traffic = None
-        if tr and tr.get("n") == n and tr.get("config") == gs_cfg and gs_launch:
+        if (tr and tr.get("n") == n and tr.get("config") == gs_cfg and bool(tr.get("packed", False)) == gs_packed
+                and gs_launch):
             traffic = tr.get("bytes_per_launch")
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -572,6 +580,10 @@ def b200_arm(args, rank, world, local_rank):
                            "note": "same sets, profiler off: the CG loop as one CUDA graph, the library's "
                                    "default path (e2e runs it)"},
             "hbm_gbs_compulsory": round(hbm_gbs, 1),
+            "compulsory_model_note": "the model counts 4-byte column indices; levels with packed columns "
+                                     "(packed_index_bytes) stream 54.9 B of index per row instead of 108 in the "
+                                     "bulk-copy kernels, so this fraction can exceed 1",
+            "packed_index_bytes": [P.level_packed(l) for l in range(4)],
             "hbm_frac_compulsory": round(hbm_gbs / peak, 4),
             "bytes_per_iter_compulsory": bytes_iter,
             "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
@@ -582,7 +594,8 @@ def b200_arm(args, rank, world, local_rank):
                          else peak_kind, "launches": gs_launch, "avg_launch_ms": round(gs_ms / max(gs_launch, 1), 4),
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
             "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
-                     "gbs": round((sp_rows * (27 * 12 + 8 + 8)) / (sp_ms * 1e-3) / 1e9, 1) if sp_ms else None},
+                     "gbs": round(metrics.spmv_bytes(sp_rows, packed=mv_packed) / (sp_ms * 1e-3) / 1e9, 1)
+                     if sp_ms else None, "packed_columns": mv_packed},
             "first_sweep_gbs": round(metrics.first_sweep_bytes(gf_rows) / (gf_ms * 1e-3) / 1e9, 1) if gf_ms else None,
             "kernel_ms_per_iter": {
                 "gs_full_l0": round(gs_ms / (args.iters * args.steps), 3),

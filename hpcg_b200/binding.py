@@ -41,7 +41,7 @@ EXPORTS = (
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
-    "hpcg_b200_mg_f32", "hpcg_b200_wait_selftest", "hpcg_b200_last_error",
+    "hpcg_b200_mg_f32", "hpcg_b200_wait_selftest", "hpcg_b200_level_packed", "hpcg_b200_last_error",
 )
 
 
@@ -89,6 +89,7 @@ def lib():
         l.hpcg_b200_cg.argtypes = [vp, vp, vp, i, d, i, C.POINTER(i), C.POINTER(d), C.POINTER(d), vp]
         l.hpcg_b200_cg_mixed.argtypes = [vp, vp, vp, i, d, C.POINTER(i), C.POINTER(d), C.POINTER(d)]
         l.hpcg_b200_level_info.argtypes = [vp, i, C.POINTER(i), C.POINTER(C.c_int64), vp]
+        l.hpcg_b200_level_packed.argtypes = [vp, i, C.POINTER(C.c_int64)]
         l.hpcg_b200_export_level.argtypes = [vp, i, vp, vp, vp, vp]
         l.hpcg_b200_colour_permutation.argtypes = [i, i, i, vp, vp]
         l.hpcg_b200_stream.argtypes = [i]
@@ -326,6 +327,12 @@ class Problem:
         _check(lib().hpcg_b200_level_info(self._h, level, C.byref(n), C.byref(pitch), starts.ctypes.data),
                "hpcg_b200_level_info")
         return n.value, pitch.value, starts
+
+    def level_packed(self, level):
+        """Bytes of the level's packed column index (0: 32-bit columns only)."""
+        b = C.c_int64(0)
+        _check(lib().hpcg_b200_level_packed(self._h, level, C.byref(b)), "hpcg_b200_level_packed")
+        return b.value
 
     def level_config(self, level):
         """Autotuner choices of a level: dict(gs, gs_first, gs32, spmv, spmv_order, tuned, gs32_first)."""

@@ -52,19 +52,39 @@ template <typename T>
 __host__ __device__ constexpr bool bulk_tensor_tile() {
   return sizeof(T) == 8;
 }
+// Packed columns: a level's column indices as one record per kBulkRows-row
+// tile of its storage (tile j: rows kBulkRows j ..): kSlots 32-bit bases and a
+// word of padding (the offsets start on 16 bytes), then kSlots x kBulkRows
+// 16-bit offsets, slot-major. Slot k of row t of the tile is column
+// base[k] + offset, or the level's zero sink where the offset is kPackSink.
+// A tile whose columns of one slot (sink aside) span more than kPackMaxSpan
+// does not pack; the level then keeps only its 32-bit columns. 55 bytes a row
+// instead of 108; one bulk copy per tile, as the blocked FP32 columns.
+constexpr int kPackBaseWords = 28;
+constexpr int kPackRec = kPackBaseWords * 4 + kSlots * kBulkRows * 2;  // 7024 bytes
+constexpr unsigned kPackSink = 0xFFFFu;
+constexpr int kPackMaxSpan = 0xFFFE;
+static_assert(kPackRec % 16 == 0, "a record is one bulk copy");
+
 // Shape of a pipeline: G consumer groups of kBulkRows x LANES threads, each
-// with a ring of RING stages of one tile. FP64 stages are 41.5 KB and FP32 ones
-// 27 KB; all stages of a block share at most 227 KB of shared memory (one block
-// per SM).
-template <typename T, int G, int RING, int LANES = 1>
+// with a ring of RING stages of one tile. A stage holds the tile's values and
+// its columns (32-bit, or the packed record when PACKED), rounded up to 128
+// bytes (tensor copies land on 128-byte boundaries): FP64 stages are 41.5 KB
+// (33.9 KB packed) and FP32 ones 27 KB (20.4 KB packed); all stages of a block
+// share at most 227 KB of shared memory (one block per SM).
+template <typename T, int G, int RING, int LANES = 1, bool PACKED = false>
 struct BulkShape {
   static constexpr int groups = G;
   static constexpr int ring = RING;
   static constexpr int lanes = LANES;
+  static constexpr bool packed = PACKED;
   static constexpr int group_threads = kBulkRows * LANES;
   static constexpr int stages = groups * ring;
   static constexpr int threads = 32 + groups * group_threads;  // producer warp + consumers
-  static constexpr int stage_bytes = kSlots * kBulkRows * (int)(sizeof(T) + sizeof(int));
+  static constexpr int value_bytes = kSlots * kBulkRows * (int)sizeof(T);
+  static constexpr int col_bytes = PACKED ? kPackRec : kSlots * kBulkRows * (int)sizeof(int);
+  static constexpr int tx_bytes = value_bytes + col_bytes;  // bytes landing in a stage per fill
+  static constexpr int stage_bytes = (tx_bytes + 127) / 128 * 128;
   // stages + barriers + slack to align the stages to 128 bytes (tensor copies)
   static constexpr int smem = stages * stage_bytes + 2 * stages * (int)sizeof(uint64_t) + 128;
   static_assert(smem <= 227 * 1024, "shared memory of one block");
@@ -72,10 +92,21 @@ struct BulkShape {
 };
 // The shapes in use (measured at 512^3: two groups of two stages beat four
 // groups of one for the Gauss-Seidel phases by 8% and tied for the SpMV).
-template <typename T>
-using GsShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2>;
-template <typename T>
-using SpmvShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2>;
+template <typename T, bool PACKED = false>
+using GsShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2, 1, PACKED>;
+template <typename T, bool PACKED = false>
+using SpmvShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2, 1, PACKED>;
+
+// Column of slot k of row t of a tile in a stage (sc: the stage's column area).
+template <bool PACKED>
+__device__ __forceinline__ int stage_col(const int* sc, int k, int t, int sink) {
+  if constexpr (PACKED) {
+    const unsigned o = reinterpret_cast<const unsigned short*>(sc + kPackBaseWords)[k * kBulkRows + t];
+    return o == kPackSink ? sink : sc[k] + (int)o;
+  } else {
+    return sc[k * kBulkRows + t];
+  }
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -153,12 +184,14 @@ __device__ __forceinline__ void record_fault(unsigned* fault, unsigned code) {
 }
 
 // Where a tile comes from: its first row and, when the tile is one block of
-// the layout (whole-tile copies), the addresses of its value and column blocks.
+// the layout (whole-tile copies), the addresses of its value and column blocks;
+// with packed columns, the address of its record.
 template <typename T>
 struct TileSrc {
   int64_t q0;
   const T* vals;
   const int* cols;
+  const unsigned char* rec;
 };
 
 // The producer/consumer pipeline of the bulk-copy kernels, run by the whole
@@ -169,7 +202,8 @@ struct TileSrc {
 // Each consumer thread calls row(tile, q0, sv, sc, t) for
 // every tile of its group, t its index in the group (row t / LANES of the tile,
 // lane t % LANES), with the tile's values sv[k * kBulkRows + row] and columns
-// sc[k * kBulkRows + row] on chip.
+// on chip: sc[k * kBulkRows + row], or the packed record at sc
+// (stage_col<Shape::packed> reads either).
 template <typename T, typename Shape, typename Src, typename Skip, typename RowFn>
 __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, RowFn row, unsigned* fault,
                                                const CUtensorMap* tm_val, const CUtensorMap* tm_col) {
@@ -177,7 +211,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
   constexpr int RING = Shape::ring;
   constexpr int S = Shape::stages;
   constexpr int SB = Shape::stage_bytes;
-  constexpr int VB = kSlots * kBulkRows * (int)sizeof(T);  // value bytes of a stage (columns follow)
+  constexpr int VB = Shape::value_bytes;  // value bytes of a stage (columns follow)
   static_assert(bulk_whole_tile<T>() || bulk_tensor_tile<T>(), "a tile must arrive in two copies");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -218,7 +252,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
           record_fault(fault, 1);
           ok = 0;
         } else {
-          mbar_expect_tx(&full[s], SB);
+          mbar_expect_tx(&full[s], Shape::tx_bytes);
         }
       }
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
@@ -228,10 +262,15 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
       if constexpr (bulk_whole_tile<T>()) {
         // the tile is one block of the layout: all slots' values in one run, all columns in another
         if (lane == 0) bulk_g2s(sv, ts.vals, VB, &full[s], policy);
-        if (lane == 1) bulk_g2s(sc, ts.cols, kSlots * kBulkRows * sizeof(int), &full[s], policy);
       } else {
         // rows q0 .. q0 + kBulkRows of all 27 slots, [slot][row] in shared memory
         if (lane == 0) tma_load_2d(sv, tm_val, (int)ts.q0, 0, &full[s], policy);
+      }
+      if constexpr (Shape::packed) {
+        if (lane == 1) bulk_g2s(sc, ts.rec, kPackRec, &full[s], policy);
+      } else if constexpr (bulk_whole_tile<T>()) {
+        if (lane == 1) bulk_g2s(sc, ts.cols, kSlots * kBulkRows * sizeof(int), &full[s], policy);
+      } else {
         if (lane == 1) tma_load_2d(sc, tm_col, (int)ts.q0, 0, &full[s], policy);
       }
 #pragma unroll
@@ -270,17 +309,20 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
   }
 }
 
-// The common case: one matrix (val, col, pitch), tile `tile` starting at row
-// first_row(tile), no tile skipped; row(q0, sv, sc, t).
+// The common case: one matrix (val, col or the packed records colp, pitch),
+// tile `tile` starting at row first_row(tile) (a multiple of kBulkRows with
+// packed columns or whole-tile copies), no tile skipped; row(q0, sv, sc, t).
 template <typename T, typename Shape, typename FirstRow, typename RowFn>
 __device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
                                            int ntiles, FirstRow first_row, RowFn row, unsigned* fault,
-                                           const CUtensorMap& tm_val, const CUtensorMap& tm_col) {
+                                           const CUtensorMap& tm_val, const CUtensorMap& tm_col,
+                                           const unsigned char* colp = nullptr) {
   bulk_tiles_src<T, Shape>(
       ntiles,
       [&](int tile) {
         const int64_t q0 = first_row(tile);
-        return TileSrc<T>{q0, val + mat_index<T>(0, q0, pitch), col + mat_index<T>(0, q0, pitch)};
+        return TileSrc<T>{q0, val + mat_index<T>(0, q0, pitch), col + mat_index<T>(0, q0, pitch),
+                          Shape::packed ? colp + (q0 / kBulkRows) * kPackRec : nullptr};
       },
       [](int) { return false; },
       [&](int, int64_t q0, const T* sv, const int* sc, int t) { row(q0, sv, sc, t); }, fault, &tm_val, &tm_col);

@@ -205,6 +205,9 @@ struct Level {
   int nwaves = 0;
   int* wave_start = nullptr; // host array [nwaves+1]
   mutable BulkMaps* maps = nullptr;  // host; built on the first bulk-copy phase
+  // the columns packed for the bulk-copy kernels (one record per 128-row tile:
+  // 27 bases and 16-bit offsets), nullptr if they do not pack
+  unsigned char* colp = nullptr;
 };
 
 struct Context;

@@ -306,20 +306,19 @@ __global__ void k_wait_selftest(unsigned long long limit_ns, unsigned* fault) {
   if (threadIdx.x == 0 && !mbar_wait(&bar, 0, limit_ns)) record_fault(fault, 4);
 }
 
-// Gauss-Seidel colour phase over rows [r0, r1) through the pipeline (configuration 10).
-template <typename T, typename TR, bool FIRST, int64_t CMASK = -1, bool DOT = false>
-__global__ void __launch_bounds__(GsShape<T>::threads, 1) k_gs_bulk(const T* __restrict__ val,
-                                                                     const int* __restrict__ col, int64_t pitch,
-                                                                     const TR* __restrict__ rhs, T* x, int r0,
-                                                                     int r1, uint32_t mask_arg,
-                                                                     double* __restrict__ dot, unsigned* fault,
-                                                                     const __grid_constant__ CUtensorMap tm_val,
-                                                                     const __grid_constant__ CUtensorMap tm_col) {
+// Gauss-Seidel colour phase over rows [r0, r1) through the pipeline
+// (configuration 10); PACK: the level's packed columns (colp, sink).
+template <typename T, typename TR, bool FIRST, int64_t CMASK = -1, bool DOT = false, bool PACK = false>
+__global__ void __launch_bounds__(GsShape<T, PACK>::threads, 1)
+    k_gs_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const TR* __restrict__ rhs,
+              T* x, int r0, int r1, uint32_t mask_arg, double* __restrict__ dot, unsigned* fault,
+              const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
+              const unsigned char* __restrict__ colp, int sink) {
   const uint32_t mask = CMASK >= 0 ? (uint32_t)CMASK : mask_arg;
   const int a0 = r0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, GsShape<T>>(
+  bulk_tiles<T, GsShape<T, PACK>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t) {
         const int64_t q = q0 + t;
@@ -330,7 +329,7 @@ __global__ void __launch_bounds__(GsShape<T>::threads, 1) k_gs_bulk(const T* __r
         for (int k = 0; k < kSlots; ++k) {
           if (mask & (1u << k)) {
             const T a = sv[k * kBulkRows + t];
-            const T xv = __ldg(x + sc[k * kBulkRows + t]);
+            const T xv = __ldg(x + stage_col<PACK>(sc, k, t, sink));
             sum -= a * xv;
             if (k == kDiagSlot) xd = xv;
           }
@@ -341,7 +340,7 @@ __global__ void __launch_bounds__(GsShape<T>::threads, 1) k_gs_bulk(const T* __r
         x[q] = out;
         if (DOT) acc += (double)rhs[q] * (double)out;
       },
-      fault, tm_val, tm_col);
+      fault, tm_val, tm_col, colp);
   if (DOT) {
     const double s = block_sum(acc);
     if (threadIdx.x == 0) dot[blockIdx.x] = s;
@@ -507,18 +506,16 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
 // colours, then the next z pair), which needs slab runs that split into whole
 // tiles and colour blocks that start on an even row (checked on the host).
 // Partials: one per block.
-template <typename T, bool DOT, int ORDER>
-__global__ void __launch_bounds__(SpmvShape<T>::threads, 1) k_spmv_bulk(ColourGrid g, const T* __restrict__ val,
-                                                                       const int* __restrict__ col, int64_t pitch,
-                                                                       const T* __restrict__ x, T* __restrict__ y,
-                                                                       int n, double* __restrict__ partials,
-                                                                       unsigned* fault,
-                                                                       const __grid_constant__ CUtensorMap tm_val,
-                                                                       const __grid_constant__ CUtensorMap tm_col) {
+template <typename T, bool DOT, int ORDER, bool PACK = false>
+__global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
+    k_spmv_bulk(ColourGrid g, const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
+                const T* __restrict__ x, T* __restrict__ y, int n, double* __restrict__ partials, unsigned* fault,
+                const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
+                const unsigned char* __restrict__ colp, int sink) {
   static_assert(ORDER == 0 || ORDER == 2, "storage or slab order");
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, SpmvShape<T>>(
+  bulk_tiles<T, SpmvShape<T, PACK>>(
       val, col, pitch, ntiles,
       [&](int tile) {
         return ORDER == 2 ? slab_row(g, (int64_t)tile * kBulkRows) : (int64_t)tile * kBulkRows;
@@ -530,14 +527,14 @@ __global__ void __launch_bounds__(SpmvShape<T>::threads, 1) k_spmv_bulk(ColourGr
         T xq = (T)0;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-          const T xv = __ldg(x + sc[k * kBulkRows + t]);
+          const T xv = __ldg(x + stage_col<PACK>(sc, k, t, sink));
           sum += sv[k * kBulkRows + t] * xv;
           if (k == kDiagSlot) xq = xv;
         }
         y[q] = sum;
         if (DOT) acc += (double)xq * (double)sum;
       },
-      fault, tm_val, tm_col);
+      fault, tm_val, tm_col, colp);
   if (DOT) {
     const double s = block_sum(acc);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
@@ -584,26 +581,26 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
 // The restriction through the bulk-copy pipeline (with SpMV configuration 7),
 // when the injected rows are one run f0 .. f0 + nc of fine rows (tf[t] = f0 + t,
 // checked on the host): the run is tiled like a phase. Same sums as k_restrict.
-template <typename T>
-__global__ void __launch_bounds__(SpmvShape<T>::threads, 1)
+template <typename T, bool PACK = false>
+__global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
     k_restrict_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const T* __restrict__ rf,
                     const T* __restrict__ xf, const int* __restrict__ tq, T* __restrict__ rc, int f0, int nc,
                     unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
-                    const __grid_constant__ CUtensorMap tm_col) {
+                    const __grid_constant__ CUtensorMap tm_col, const unsigned char* __restrict__ colp, int sink) {
   const int r1 = f0 + nc;
   const int a0 = f0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<T, SpmvShape<T>>(
+  bulk_tiles<T, SpmvShape<T, PACK>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t) {
         const int64_t f = q0 + t;
         if (f < f0 || f >= r1) return;
         T sum = (T)0;
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * __ldg(xf + sc[k * kBulkRows + t]);
+        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * __ldg(xf + stage_col<PACK>(sc, k, t, sink));
         rc[tq[f - f0]] = rf[f] - sum;
       },
-      fault, tm_val, tm_col);
+      fault, tm_val, tm_col, colp);
 }
 
 // ComputeProlongation_ref.cpp:49 over the same sorted pairs

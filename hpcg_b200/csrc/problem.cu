@@ -2,11 +2,13 @@
 // structures (OptimizeProblem) or generated on the device, plus release,
 // accounting and inspection.
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <functional>
 #include <thread>
 #include <vector>
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "shard.cuh"
 
@@ -200,6 +202,88 @@ int build_transfer(hpcg_b200_problem* p, int l) {
   return HPCG_B200_OK;
 }
 
+// The packed columns of a level (kPackRec records, one per kBulkRows-row tile
+// of the storage): block b builds tiles b, b + gridDim.x, ..., thread t row t
+// of the tile. Rows at or beyond n are stored as the sink (they are never
+// computed). Sets *bad if the columns of a slot of a tile span more than
+// kPackMaxSpan.
+__global__ void __launch_bounds__(kBulkRows) k_pack_cols(const int* __restrict__ col, int64_t pitch, int n,
+                                                         int sink, int64_t ntiles, unsigned char* __restrict__ colp,
+                                                         int* bad) {
+  constexpr int W = kBulkRows / 32;
+  __shared__ int wlo[W], whi[W];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t q = tile * kBulkRows + t;
+    int* base = reinterpret_cast<int*>(colp + tile * kPackRec);
+    unsigned short* off = reinterpret_cast<unsigned short*>(base + kPackBaseWords);
+    if (t < kPackBaseWords - kSlots) base[kSlots + t] = 0;
+    for (int k = 0; k < kSlots; ++k) {
+      const int c = q < n ? col[mat_index<double>(k, q, pitch)] : sink;
+      const bool real = c != sink;
+      int lo = real ? c : INT_MAX, hi = real ? c : INT_MIN;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      }
+      if (lane == 0) {
+        wlo[w] = lo;
+        whi[w] = hi;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        lo = min(lo, wlo[i]);
+        hi = max(hi, whi[i]);
+      }
+      __syncthreads();
+      const int b = lo == INT_MAX ? 0 : lo;
+      if (t == 0) {
+        base[k] = b;
+        if (lo != INT_MAX && (int64_t)hi - lo > kPackMaxSpan) *bad = 1;
+      }
+      off[k * kBulkRows + t] = real ? (unsigned short)(c - b) : (unsigned short)kPackSink;
+    }
+  }
+}
+
+// The packed columns of level l for the bulk-copy kernels (k_pack_cols). The
+// level keeps only its 32-bit columns if a tile does not pack, or with
+// HPCG_B200_PACKED=0.
+int build_packed(hpcg_b200_problem* p, int l) {
+  Level& L = p->lev[l];
+  const char* e = std::getenv("HPCG_B200_PACKED");
+  if ((e && e[0] == '0') || L.n <= 0) return HPCG_B200_OK;
+  Context* c = p->ctx;
+  const int64_t ntiles = L.pitch / kBulkRows;
+  const size_t bytes = (size_t)ntiles * kPackRec;
+  HB_TRY(dev_alloc((void**)&L.colp, bytes, &p->bytes));
+  int* bad = nullptr;
+  HB_CK(cudaMalloc(&bad, sizeof(int)));
+  int h = 0;
+  cudaError_t err = cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
+  if (err == cudaSuccess) {
+    const int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms * 16);
+    k_pack_cols<<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, L.colp, bad);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
+  cudaFree(bad);
+  if (err != cudaSuccess) {
+    set_error("pack columns", err);
+    return status_of(err);
+  }
+  if (h) {  // a tile does not pack: give the memory back
+    dev_free(L.colp);
+    L.colp = nullptr;
+    p->bytes -= bytes;
+    release_accounted(bytes);
+  }
+  return HPCG_B200_OK;
+}
+
 int free_problem(hpcg_b200_problem* p) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   cudaSetDevice(p->device);
@@ -207,7 +291,7 @@ int free_problem(hpcg_b200_problem* p) {
   for (int l = 0; l < kMaxLevels; ++l) {
     Level& L = p->lev[l];
     void* ptrs[] = {L.val, L.col, L.val32, L.col32, L.new2old, L.old2new, L.f2c, L.tf, L.tq, L.r, L.x, L.r32, L.x32,
-                    L.wave_rows};
+                    L.wave_rows, L.colp};
     for (void* q : ptrs) dev_free(q);
     delete[] L.wave_start;
     delete L.maps;
@@ -286,6 +370,7 @@ int generate_impl(int nx, int ny, int nz, int nlevels, int device, const RankGeo
   }
   for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
   for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) status = upload_plan(p, l, sends[l]);
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) status = build_packed(p, l);
   if (status != HPCG_B200_OK) {
     free_problem(p);
     return status;
@@ -391,6 +476,7 @@ int hpcg_b200_optimize(const hpcg_b200_level_desc* desc, int nlevels, int device
   }
   if (status == HPCG_B200_OK) status = alloc_vectors(p);
   for (int l = 0; l + 1 < nlevels && status == HPCG_B200_OK; ++l) status = build_transfer(p, l);
+  for (int l = 0; l < nlevels && status == HPCG_B200_OK; ++l) status = build_packed(p, l);
   if (status == HPCG_B200_OK) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { set_error("optimize sync", e); status = status_of(e); }
@@ -564,6 +650,14 @@ int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64
   if (pitch) *pitch = L.pitch;
   if (colour_start)
     for (int s = 0; s <= kColours; ++s) colour_start[s] = L.g.start[s];
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_level_packed(const hpcg_b200_problem* p, int level, int64_t* bytes) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!bytes || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  const Level& L = p->lev[level];
+  *bytes = L.colp ? L.pitch / kBulkRows * kPackRec : 0;
   return HPCG_B200_OK;
 }
 

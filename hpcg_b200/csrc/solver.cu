@@ -52,13 +52,14 @@ void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
 }
 
 // The bulk-copy pipeline (configuration 10): one block per SM (its shared
-// memory allows no second), at most one per tile. false: not launched (FP64
-// tensor maps unavailable).
-template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
-bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
-                    double* dot) {
-  auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT>;
-  constexpr int smem = GsShape<T>::smem;
+// memory allows no second), at most one per tile; PACK: the level's packed
+// columns. false: not launched (FP64 tensor maps unavailable).
+template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT, bool PACK>
+bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1,
+                      uint32_t mask, double* dot) {
+  auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT, PACK>;
+  using Shape = GsShape<T, PACK>;
+  constexpr int smem = Shape::smem;
   static CUtensorMap none;  // the FP32 kernels take no maps
   const CUtensorMap* tv = &none;
   const CUtensorMap* tc = &none;
@@ -86,7 +87,7 @@ bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof(cfg));
   cfg.gridDim = dim3(g);
-  cfg.blockDim = dim3(GsShape<T>::threads);
+  cfg.blockDim = dim3(Shape::threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
@@ -94,8 +95,16 @@ bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault, *tv, *tc);
+  cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault, *tv, *tc,
+                     (const unsigned char*)L.colp, sink_of(L));
   return true;
+}
+
+template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
+bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
+                    double* dot) {
+  if (L.colp) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, true>(c, L, val, rhs, x, r0, r1, mask, dot);
+  return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, false>(c, L, val, rhs, x, r0, r1, mask, dot);
 }
 
 // dot != nullptr: the phase also writes its r'z block partials there (FP64
@@ -242,11 +251,12 @@ inline bool bulk_slab_ok(const Level& L) {
   return true;
 }
 
-template <typename T, bool DOT, int ORDER>
+template <typename T, bool DOT, int ORDER, bool PACK>
 int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials,
                      const BulkMaps* m) {
-  auto k = k_spmv_bulk<T, DOT, ORDER>;
-  constexpr int smem = SpmvShape<T>::smem;
+  auto k = k_spmv_bulk<T, DOT, ORDER, PACK>;
+  using Shape = SpmvShape<T, PACK>;
+  constexpr int smem = Shape::smem;
   static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
   if (!(attr_set >> c->device & 1)) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -254,9 +264,18 @@ int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y,
   }
   const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sms));
-  k<<<g, SpmvShape<T>::threads, smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault,
-                                                  m->val, m->col);
+  k<<<g, Shape::threads, smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault, m->val,
+                                            m->col, (const unsigned char*)L.colp, sink_of(L));
   return g;
+}
+
+// Packed columns in slab order: every slab run starts a packed tile (colour
+// blocks on multiples of kBulkRows).
+inline bool packed_slab_ok(const Level& L) {
+  if (!L.colp) return false;
+  for (int s = 0; s < kColours; ++s)
+    if (L.g.start[s] % kBulkRows) return false;
+  return true;
 }
 
 // SpMV configuration 7 (FP64): slab order where the tiles fit it, storage order
@@ -269,8 +288,12 @@ int spmv_bulk(Context* c, const Level& L, const T* val, const T* x, T* y, double
   } else {
     const BulkMaps* m = bulk_maps(L);
     if (!m) return 0;
-    if (L.mv_order == 2 && bulk_slab_ok(L)) return spmv_bulk_launch<T, DOT, 2>(c, L, val, x, y, partials, m);
-    return spmv_bulk_launch<T, DOT, 0>(c, L, val, x, y, partials, m);
+    if (L.mv_order == 2 && bulk_slab_ok(L)) {
+      if (packed_slab_ok(L)) return spmv_bulk_launch<T, DOT, 2, true>(c, L, val, x, y, partials, m);
+      return spmv_bulk_launch<T, DOT, 2, false>(c, L, val, x, y, partials, m);
+    }
+    if (L.colp) return spmv_bulk_launch<T, DOT, 0, true>(c, L, val, x, y, partials, m);
+    return spmv_bulk_launch<T, DOT, 0, false>(c, L, val, x, y, partials, m);
   }
 }
 
@@ -300,9 +323,8 @@ void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, cons
 
 // The restriction on the bulk-copy pipeline (SpMV configuration 7, injected rows
 // in one run); false if it cannot run here.
-template <typename T>
-bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
-  if (L.tf_run < 0 || nc <= 0) return false;
+template <typename T, bool PACK>
+bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   static CUtensorMap none;  // the FP32 copy takes no maps
   const CUtensorMap* tv = &none;
   const CUtensorMap* tc = &none;
@@ -312,8 +334,9 @@ bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const 
     tv = &m->val;
     tc = &m->col;
   }
-  auto k = k_restrict_bulk<T>;
-  constexpr int smem = SpmvShape<T>::smem;
+  auto k = k_restrict_bulk<T, PACK>;
+  using Shape = SpmvShape<T, PACK>;
+  constexpr int smem = Shape::smem;
   static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
   if (!(attr_set >> c->device & 1)) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -321,9 +344,16 @@ bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const 
   }
   const int64_t tiles = ((int64_t)L.tf_run + nc - (L.tf_run & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
   const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
-  k<<<g, SpmvShape<T>::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tq, rc, L.tf_run, nc,
-                                                   c->fault, *tv, *tc);
+  k<<<g, Shape::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tq, rc, L.tf_run, nc, c->fault,
+                                            *tv, *tc, (const unsigned char*)L.colp, sink_of(L));
   return true;
+}
+
+template <typename T>
+bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
+  if (L.tf_run < 0 || nc <= 0) return false;
+  if (L.colp) return restrict_bulk_p<T, true>(c, L, val, rf, xf, rc, nc);
+  return restrict_bulk_p<T, false>(c, L, val, rf, xf, rc, nc);
 }
 
 template <typename T>

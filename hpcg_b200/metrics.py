@@ -89,16 +89,31 @@ def compulsory_bytes(nx, ny, nz, nlevels=4, vb=8):
     return b
 
 
-def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8):
+# Column-index bytes per row: 27 int32 columns, or the packed index (one record
+# per 128-row tile: 27 int32 bases + a padding word + 27 x 128 uint16 offsets).
+PACKED_INDEX_BYTES_PER_ROW = (28 * 4 + SLOTS * 128 * 2) / 128.0
+
+
+def index_bytes_per_row(packed=False):
+    return PACKED_INDEX_BYTES_PER_ROW if packed else SLOTS * 4
+
+
+def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8, packed=False):
     """Algorithmic bytes of Gauss-Seidel colour phases that together updated
     `rows_in_phase` rows of a level with `rows_in_level` rows, per phase:
-    27 ELL slots (value + int32 column) and the right-hand side read, x written,
-    for every row of the colour; and x of the seven other colours read once
-    (each row of a colour neighbours all of them). For rows_in_phase = R summed
-    over launches of one colour each, the other-colour reads are 7 R vb (the
-    colours hold an eighth of the rows each)."""
-    per_row = SLOTS * (vb + 4) + 2 * vb
+    27 ELL slots (value + column index: int32, or the packed index) and the
+    right-hand side read, x written, for every row of the colour; and x of the
+    seven other colours read once (each row of a colour neighbours all of them).
+    For rows_in_phase = R summed over launches of one colour each, the
+    other-colour reads are 7 R vb (the colours hold an eighth of the rows each)."""
+    per_row = SLOTS * vb + index_bytes_per_row(packed) + 2 * vb
     return rows_in_phase * per_row + 7.0 * rows_in_phase * vb
+
+
+def spmv_bytes(rows, vb=8, packed=False):
+    """Algorithmic bytes of y = A x over `rows` rows: 27 values and column
+    indices, x read once, y written."""
+    return rows * (SLOTS * vb + index_bytes_per_row(packed) + 2 * vb)
 
 
 def first_sweep_bytes(rows, vb=8):

@@ -267,6 +267,14 @@ int hpcg_b200_shard_cg(hpcg_b200_comm* comm, const double* const* b, double* con
 /* Rows, padded pitch and colour-block boundaries (9 ints) of one level. */
 int hpcg_b200_level_info(const hpcg_b200_problem* p, int level, int* nrow, int64_t* pitch, int* colour_start);
 
+/* Bytes of one level's packed column index, 0 if the level keeps only its
+ * 32-bit columns (a 128-row tile whose columns of one slot span more than 65534,
+ * or HPCG_B200_PACKED=0 at creation). One 7024-byte record per 128-row tile of
+ * the storage: 27 32-bit bases, a word of padding and 27 x 128 16-bit offsets
+ * (0xFFFF: the zero sink); the bulk-copy kernels read it instead of the 32-bit
+ * columns, with the same column for every entry. */
+int hpcg_b200_level_packed(const hpcg_b200_problem* p, int level, int64_t* bytes);
+
 /* Copies one level's device layout to host: new2old[nrow] (colour row -> natural
  * row), cols[27*pitch] and vals[27*pitch] (slot-major, colour order), f2c[nrow of
  * next level] (colour order, NULL allowed). */

@@ -653,6 +653,52 @@ def test_cg_forced_config_vs_oracle(oracle, binding, monkeypatch, cfg):
         D.free()
 
 
+@pytest.mark.parametrize("dims", [(32, 32, 32), (16, 24, 40)])
+def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
+    """The bulk-copy kernels read a level's packed column index (one record per
+    128-row tile: 27 bases and 16-bit offsets, 0xFFFF for the zero sink); a
+    problem made with HPCG_B200_PACKED=0 keeps only the 32-bit columns. With the
+    bulk-copy configurations forced, SpMV, SYMGS, the V-cycle, CG and CG around
+    the FP32 V-cycle give the same bits either way (16x24x40: colour blocks of
+    the coarser levels off the 128-row grid, where the slab-order SpMV keeps the
+    32-bit columns)."""
+    monkeypatch.setenv("HPCG_B200_CONFIG", "10")
+    A = binding.Problem.generate(*dims)
+    monkeypatch.setenv("HPCG_B200_PACKED", "0")
+    U = binding.Problem.generate(*dims)
+    try:
+        for lv in range(4):
+            _, pitch, _ = A.level_info(lv)
+            assert A.level_packed(lv) == pitch // 128 * 7024
+            assert U.level_packed(lv) == 0
+        n = A.nrow
+        b = A.get_rhs()
+        rng = np.random.default_rng(7)
+        v = rng.uniform(-1.0, 1.0, n)
+        outs = []
+        for P in (A, U):
+            y = np.zeros(n)
+            P.ComputeSPMV(v, y)
+            xs = v.copy()
+            P.ComputeSYMGS(b, xs)
+            xm = np.zeros(n)
+            P.ComputeMG(b, xm)
+            xc = np.zeros(n)
+            rc = P.CG(b, xc, 25, 0.0, True)
+            xf = np.zeros(n)
+            rf = P.CG_mixed(b, xf, 25, 0.0)
+            assert P.level_config(0)["gs"] == 10 and P.level_config(0)["gs32"] == 10
+            outs.append((y, xs, xm, xc, rc, xf, rf))
+        for a, u in zip(outs[0], outs[1]):
+            if isinstance(a, np.ndarray):
+                assert np.array_equal(a, u)
+            else:
+                assert a == u
+    finally:
+        A.free()
+        U.free()
+
+
 def test_bounded_wait_gives_up_and_context_survives(oracle, binding, case16):
     """The device-side wait of the bulk-copy phases ends by itself: waiting on an
     mbarrier that nothing completes returns HPCG_B200_ERR_TIMEOUT after the

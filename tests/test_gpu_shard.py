@@ -242,6 +242,21 @@ def test_local_comm_rejects_wrong_rank_order(binding):
             p.free()
 
 
+def test_far_halo_columns_stay_unpacked(binding):
+    """A rank's external columns follow its n interior rows, so on a 48^3 rank
+    with a neighbour a 128-row tile of level 0 mixes interior columns with
+    external ones more than 65534 apart: that level keeps its 32-bit columns,
+    and the coarser levels, whose spans fit, are packed."""
+    P = binding.Problem.generate_rank(48, 48, 48, 2, 1, 1, 0)
+    try:
+        assert P.level_packed(0) == 0
+        for lv in (1, 2, 3):
+            _, pitch, _ = P.level_info(lv)
+            assert P.level_packed(lv) == pitch // 128 * 7024
+    finally:
+        P.free()
+
+
 @pytest.mark.parametrize("cfg", ["1", "10"])
 def test_nccl_single_rank_equals_single_gpu_cg(binding, monkeypatch, cfg):
     """A one-rank NCCL communicator (NCCL opened, initialised and allreducing on
