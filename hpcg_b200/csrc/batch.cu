@@ -41,6 +41,8 @@ struct BGs {
   uint32_t mask;
   int first;
   int prob;
+  const unsigned char* colp;  // the level's packed columns (bulk-copy phases)
+  int sink;                   // the level's zero sink column
 };
 // residual + restriction, and prolongation, of one problem's level
 struct BRes {
@@ -97,19 +99,22 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
 }
 
 // The batched colour phase through the bulk-copy pipeline (bulk.cuh): every
-// tile is one 128-row block of its problem's blocked FP32 copy (val32, col32 of
-// the single-problem path), so it arrives by two copies; the tiles of problems
-// that have converged are skipped on both sides. Same arithmetic as k_b_gs.
-__global__ void __launch_bounds__(GsShape<float>::threads, 1)
+// tile is one 128-row block of its problem's blocked FP32 values (val32 of the
+// single-problem path) and one record of its packed columns, so it arrives by
+// two copies; the tiles of problems that have converged are skipped on both
+// sides. Same arithmetic as k_b_gs.
+using BatchShape = GsShape<float, true>;
+__global__ void __launch_bounds__(BatchShape::threads, 1)
     k_b_gs_bulk(const BGs* __restrict__ items, const BTile* __restrict__ tiles, int ntiles,
                 const BScal* __restrict__ sc, unsigned* fault) {
-  bulk_tiles_src<float, GsShape<float>>(
+  bulk_tiles_src<float, BatchShape>(
       ntiles,
       [&](int t) {
         const BTile tl = tiles[t];
         const BGs& it = items[tl.item];
         return TileSrc<float>{tl.start, it.val + mat_index<float>(0, tl.start, it.pitch),
-                              it.col + mat_index<float>(0, tl.start, it.pitch)};
+                              it.col + mat_index<float>(0, tl.start, it.pitch),
+                              it.colp + (tl.start / kBulkRows) * kPackRec};
       },
       [&](int t) { return !sc[items[tiles[t].item].prob].active; },
       [&](int t, int64_t q0, const float* sv, const int* scol, int row) {
@@ -123,7 +128,7 @@ __global__ void __launch_bounds__(GsShape<float>::threads, 1)
 #pragma unroll
           for (int k = 0; k < kSlots; ++k) {
             const float a = sv[k * kBulkRows + row];
-            const float xv = __ldg(it.x + scol[k * kBulkRows + row]);
+            const float xv = __ldg(it.x + stage_col<true>(scol, k, row, it.sink));
             sum -= a * xv;
             if (k == kDiagSlot) xd = xv;
           }
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(GsShape<float>::threads, 1)
           for (int k = 0; k < kSlots; ++k) {
             if (mask & (1u << k)) {
               const float a = sv[k * kBulkRows + row];
-              const float xv = __ldg(it.x + scol[k * kBulkRows + row]);
+              const float xv = __ldg(it.x + stage_col<true>(scol, k, row, it.sink));
               sum -= a * xv;
               if (k == kDiagSlot) xd = xv;
             }
@@ -403,6 +408,7 @@ struct hpcg_b200_batch {
   hb::BGs* gs_bitems;  // the GS items on the blocked FP32 copies (bulk-copy phases)
   hb::BTile* btiles;   // their 128-row tiles
   bool bulk;           // GS phases on k_b_gs_bulk (chosen by timing at creation)
+  bool packed;         // every level of every problem has packed columns (k_b_gs_bulk reads them)
   std::vector<hb::Step> steps;
   hb::BVec* vec;
   hb::BTile* vtiles;  // row tiles of every problem's level 0
@@ -470,11 +476,16 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       it.mask = first ? first_mask(L.g, s) : kAllSlots;
       it.first = first ? 1 : 0;
       it.prob = p;
+      it.colp = nullptr;
+      it.sink = 0;
       gs.push_back(it);
       tiles_of(tiles, item, it.r0, it.r1);
       BGs bit = it;  // the same phase on the blocked copies (item index = gs index)
       bit.val = L.val32;
       bit.col = L.col32;
+      bit.colp = L.colp;
+      bit.sink = sink_of(L);
+      if (!L.colp) B->packed = false;  // the bulk-copy phases need packed columns
       gsb.push_back(bit);
       bulk_tiles_of(btiles, item, it.r0, it.r1);
     }
@@ -534,7 +545,7 @@ int launch_step(hpcg_b200_batch* B, const Step& s) {
   const int g = grid_tiles(c, s.ntiles);
   // tiles hold indices into the whole item array, so the items go in unshifted
   if (s.kind == 0 && B->bulk) {
-    using Sh = GsShape<float>;
+    using Sh = BatchShape;
     static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
     if (!(attr_set >> c->device & 1)) {
       cudaFuncSetAttribute(k_b_gs_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::smem);
@@ -645,6 +656,10 @@ int build_graph(hpcg_b200_batch* B) {
 // Every V-cycle starts its sweeps from the right-hand side alone, so the work
 // vectors it leaves behind are rewritten by the next solve.
 int choose_bulk(hpcg_b200_batch* B) {
+  if (!B->packed) {  // a level without packed columns: the register kernel
+    B->bulk = false;
+    return HPCG_B200_OK;
+  }
   const char* force = std::getenv("HPCG_B200_BATCH_BULK");
   if (force && *force) {
     B->bulk = std::atoi(force) != 0;
@@ -722,7 +737,7 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
   B->ctx = c;
   B->m = count;
   B->gs_items = nullptr; B->res_items = nullptr; B->tiles = nullptr; B->vec = nullptr; B->vtiles = nullptr;
-  B->gs_bitems = nullptr; B->btiles = nullptr; B->bulk = false;
+  B->gs_bitems = nullptr; B->btiles = nullptr; B->bulk = false; B->packed = true;
   B->vrange = nullptr; B->partials = nullptr; B->sc = nullptr; B->sc_host = nullptr; B->ctl = nullptr;
   B->bytes = 0;
   B->graph = nullptr;

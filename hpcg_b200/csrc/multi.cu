@@ -210,7 +210,9 @@ void bulk_attr(Kern k, int smem, int device, uint64_t* done) {
 template <int K, int LANES, int BULK>
 void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, int r0, int r1, bool first,
                     uint32_t mask) {
-  const BulkMaps* bm = BULK == 2 || (BULK == 1 && !first) ? bulk_maps(L) : nullptr;
+  // the bulk-copy kernels read the packed columns: a level without them runs
+  // the register-pipelined kernels
+  const BulkMaps* bm = L.colp && (BULK == 2 || (BULK == 1 && !first)) ? bulk_maps(L) : nullptr;
   if (bm) {
     using Sh = MultiShape<LANES>;
     const int64_t tiles = ((int64_t)r1 - (r0 & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
@@ -220,12 +222,12 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
       auto k = k_gs_phase_m_bulk<K, LANES, true>;
       bulk_attr(k, Sh::smem, c->device, &done[0]);
       k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
-                                                  bm->col);
+                                                  bm->col, L.colp, sink_of(L));
     } else {
       auto k = k_gs_phase_m_bulk<K, LANES, false>;
       bulk_attr(k, Sh::smem, c->device, &done[1]);
       k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
-                                                  bm->col);
+                                                  bm->col, L.colp, sink_of(L));
     }
     return;
   }
@@ -243,7 +245,7 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
 // or a negative status.
 template <int K, int LANES, int BULK, bool DOT>
 int spmv_m(Context* c, const Level& L, const double* x, double* y, double* partials) {
-  const BulkMaps* bm = BULK ? bulk_maps(L) : nullptr;
+  const BulkMaps* bm = BULK && L.colp ? bulk_maps(L) : nullptr;
   if (bm) {
     using Sh = MultiShape<LANES>;
     auto k = k_spmv_m_bulk<K, LANES, DOT>;
@@ -252,7 +254,7 @@ int spmv_m(Context* c, const Level& L, const double* x, double* y, double* parti
     const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
     const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
     k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, x, y, L.n, partials, c->fault, bm->val,
-                                                bm->col);
+                                                bm->col, L.colp, sink_of(L));
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       set_error("k_spmv_m_bulk", e);
