@@ -398,14 +398,17 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
                 "packed_columns": packed}}
 
 
-def gpu_launches_per_set(iters, nlevels=4):
-    """Kernels the library launches for one CG call (its own kernels only)."""
+def gpu_launches_per_set(iters, nlevels=4, rtz_pass=False):
+    """Kernels the library launches for one CG call (its own kernels only).
+    rtz_pass: r'z runs as its own dot kernel (level 0 on the packed bulk-copy
+    phases) instead of coming out of the post-smoother."""
     mg = 15 * 2 + 2  # per non-coarsest level: pre and post symmetric sweeps (15 colour phases each),
     # residual-restriction, prolongation
     per_mg = mg * (nlevels - 1) + 15
-    # r'z finalize (its partials come out of the post-smoother), p update with the
-    # previous iteration's x update (k > 1), SpMV + finalize, r update + finalize
-    per_iter = per_mg + 1 + 1 + 2 + 2
+    # r'z finalize (its partials come out of the post-smoother, or out of a dot
+    # kernel), p update with the previous iteration's x update (k > 1), SpMV +
+    # finalize, r update + finalize
+    per_iter = per_mg + 1 + 1 + 2 + 2 + (1 if rtz_pass else 0)
     first_iter_adjust = -1  # k = 1 copies z to p instead of the update kernel
     loads_stores = 2 + 1    # b and x gathered in, x scattered out
     preamble = 3            # SpMV, r = b - Ax with r'r, finalize
@@ -603,7 +606,7 @@ def b200_arm(args, rank, world, local_rank):
                 "spmv_l0": round(sp_ms / (args.iters * args.steps), 3),
                 "restrict_l0": round(rs_ms / (args.iters * args.steps), 3),
                 "iteration": round(ms / (args.iters * args.steps), 3)},
-            "gpu_launches": gpu_launches_per_set(args.iters) * args.steps,
+            "gpu_launches": gpu_launches_per_set(args.iters, rtz_pass=gs_packed) * args.steps,
             "clocks": clk,
         }
         if e2e:

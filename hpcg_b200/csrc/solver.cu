@@ -493,7 +493,17 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x, double* rt
 }
 
 // The CG's r'z comes out of the post-smoother (colour mode, more than one level).
-bool rtz_fused(const hpcg_b200_problem* P) { return P->symgs_mode == HPCG_B200_SYMGS_COLOUR && P->nlev > 1; }
+// r'z from the post-smoother's partials (CG.cpp:110/113 fused into the phase
+// that writes each colour's final value), except when level 0 runs the
+// bulk-copy phases on packed columns: there the phases that also write
+// partials measured about 12% slower than the plain ones at the same bytes
+// (0.8 ms per 512^3 iteration), more than a separate r'z pass over r and z
+// (2.1 GB), so the CG runs that pass instead (0.5 ms per iteration faster).
+// Read after tuning.
+bool rtz_fused(const hpcg_b200_problem* P) {
+  const Level& L = P->lev[0];
+  return P->symgs_mode == HPCG_B200_SYMGS_COLOUR && P->nlev > 1 && !(L.gs_sched == kBulkCfg && L.colp);
+}
 
 // Autotuner: per level, times each kernel configuration (load schedule x
 // registers per thread) of the Gauss-Seidel phase and of the SpMV on scratch

@@ -658,10 +658,12 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
     """The bulk-copy kernels read a level's packed column index (one record per
     128-row tile: 27 bases and 16-bit offsets, 0xFFFF for the zero sink); a
     problem made with HPCG_B200_PACKED=0 keeps only the 32-bit columns. With the
-    bulk-copy configurations forced, SpMV, SYMGS, the V-cycle, CG and CG around
-    the FP32 V-cycle give the same bits either way (16x24x40: colour blocks of
-    the coarser levels off the 128-row grid, where the slab-order SpMV keeps the
-    32-bit columns)."""
+    bulk-copy configurations forced, SpMV, SYMGS, the V-cycle and CG around the
+    FP32 V-cycle give the same bits either way (16x24x40: colour blocks of the
+    coarser levels off the 128-row grid, where the slab-order SpMV keeps the
+    32-bit columns). The FP64 CG forms r'z by its own dot pass on the packed
+    phases and from the post-smoother's partials on the others, so its history
+    and x agree to rounding."""
     monkeypatch.setenv("HPCG_B200_CONFIG", "10")
     A = binding.Problem.generate(*dims)
     monkeypatch.setenv("HPCG_B200_PACKED", "0")
@@ -689,8 +691,13 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
             rf = P.CG_mixed(b, xf, 25, 0.0)
             assert P.level_config(0)["gs"] == 10 and P.level_config(0)["gs32"] == 10
             outs.append((y, xs, xm, xc, rc, xf, rf))
-        for a, u in zip(outs[0], outs[1]):
-            if isinstance(a, np.ndarray):
+        for i, (a, u) in enumerate(zip(outs[0], outs[1])):
+            if i in (3, 4):  # FP64 CG: r'z summed in another order
+                if isinstance(a, np.ndarray):
+                    assert np.max(np.abs(a - u)) <= 1e-12 * np.max(np.abs(u))
+                else:
+                    assert a[0] == u[0] and abs(a[1] - u[1]) <= 1e-10 * u[1] and a[2] == u[2]
+            elif isinstance(a, np.ndarray):
                 assert np.array_equal(a, u)
             else:
                 assert a == u

@@ -136,3 +136,5 @@ def test_gpu_launch_count_model():
     # 512^3 launch list; one x update after the loop.
     assert bench.gpu_launches_per_set(1) == (32 * 3 + 15) + 6 - 1 + 3 + 3 + 1
     assert bench.gpu_launches_per_set(2) - bench.gpu_launches_per_set(1) == 117
+    # level 0 on the packed bulk-copy phases: r'z as its own dot kernel
+    assert bench.gpu_launches_per_set(2, rtz_pass=True) - bench.gpu_launches_per_set(1, rtz_pass=True) == 118
