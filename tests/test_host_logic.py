@@ -52,6 +52,10 @@ def test_handle_and_argument_errors(binding):
     junk = (C.c_uint64 * 64)()
     assert lib.hpcg_b200_spmv(C.cast(junk, C.c_void_p), None, None) == binding.ERR_HANDLE
     assert lib.hpcg_b200_set_symgs_mode(C.cast(junk, C.c_void_p), 0) == binding.ERR_HANDLE
+    b = C.c_int64(-1)
+    assert lib.hpcg_b200_level_packed(None, 0, C.byref(b)) == binding.ERR_HANDLE
+    assert lib.hpcg_b200_level_packed(C.cast(junk, C.c_void_p), 0, C.byref(b)) == binding.ERR_HANDLE
+    assert b.value == -1  # nothing written on an error
 
 
 def test_no_gpu_is_a_clean_error(binding):
