@@ -546,11 +546,8 @@ int launch_step(hpcg_b200_batch* B, const Step& s) {
   // tiles hold indices into the whole item array, so the items go in unshifted
   if (s.kind == 0 && B->bulk) {
     using Sh = BatchShape;
-    static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
-    if (!(attr_set >> c->device & 1)) {
-      cudaFuncSetAttribute(k_b_gs_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::smem);
-      attr_set |= 1ull << c->device;
-    }
+    static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
+    bulk_attr(k_b_gs_bulk, Sh::smem, c->device, &attr_set);
     const int gb = s.bntiles < c->sms ? (s.bntiles < 1 ? 1 : s.bntiles) : c->sms;
     k_b_gs_bulk<<<gb, Sh::threads, Sh::smem, c->stream>>>(B->gs_bitems, B->btiles + s.btile_off, s.bntiles, B->sc,
                                                           c->fault);

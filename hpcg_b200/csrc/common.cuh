@@ -17,6 +17,7 @@
 #include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <utility>
@@ -337,8 +338,25 @@ const BulkMaps* bulk_maps(const Level& L);
 int dev_alloc(void** ptr, size_t bytes, size_t* counter);
 void dev_free(void* ptr);
 
-// true if ptr is device (or managed) memory
-bool is_device_ptr(const void* ptr);
+// Where a vector argument of a call on GPU `device` lives: *on_device = false
+// for host memory (pageable or pinned: moved through copies), true for device
+// memory of `device` or managed memory (used in place). Device memory of
+// another GPU is refused with HPCG_B200_ERR_ARG (the error text names `what`
+// and both GPUs): a kernel on `device` would fault on it.
+int locate_ptr(const void* ptr, int device, bool* on_device, const char* what);
+
+// Raises a kernel's dynamic shared-memory limit to `smem` on `device` (the
+// current device) once: `done` is the kernel's own set of devices already
+// raised. The bit is set with fetch_or after the call, so two host threads
+// driving different devices cannot lose each other's bit, and a thread that
+// sees the bit also sees the raised limit.
+template <typename Kern>
+inline void bulk_attr(Kern k, int smem, int device, std::atomic<uint64_t>* done) {
+  const uint64_t bit = 1ull << device;
+  if (done->load(std::memory_order_acquire) & bit) return;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  done->fetch_or(bit, std::memory_order_release);
+}
 
 // problem handle validity
 inline bool valid(const hpcg_b200_problem* p) { return p != nullptr && p->magic == kMagic; }

@@ -58,13 +58,25 @@ void dev_free(void* ptr) {
 
 void release_accounted(size_t bytes) { g_allocated = bytes > g_allocated ? 0 : g_allocated - bytes; }
 
-bool is_device_ptr(const void* ptr) {
+int locate_ptr(const void* ptr, int device, bool* on_device, const char* what) {
+  *on_device = false;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
     cudaGetLastError();  // plain pageable host memory on older runtimes
-    return false;
+    return HPCG_B200_OK;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) {
+    *on_device = true;
+    return HPCG_B200_OK;
+  }
+  if (a.type != cudaMemoryTypeDevice) return HPCG_B200_OK;  // pinned or registered host memory
+  if (a.device != device) {
+    std::snprintf(g_last_error, sizeof(g_last_error),
+                  "%s: a pointer to device memory of GPU %d was passed to a call on GPU %d", what, a.device, device);
+    return HPCG_B200_ERR_ARG;
+  }
+  *on_device = true;
+  return HPCG_B200_OK;
 }
 
 Context* context_for(int device) {

@@ -198,15 +198,6 @@ int ensure_state(hpcg_b200_problem* P, MultiState** out) {
   return HPCG_B200_OK;
 }
 
-// Enables a bulk kernel's shared memory on c's device (once per kernel and device).
-template <typename Kern>
-void bulk_attr(Kern k, int smem, int device, uint64_t* done) {
-  if (!(*done >> device & 1)) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    *done |= 1ull << device;
-  }
-}
-
 template <int K, int LANES, int BULK>
 void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, int r0, int r1, bool first,
                     uint32_t mask) {
@@ -217,7 +208,7 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
     using Sh = MultiShape<LANES>;
     const int64_t tiles = ((int64_t)r1 - (r0 & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
     const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
-    static uint64_t done[2] = {0, 0};
+    static std::atomic<uint64_t> done[2] = {{0}, {0}};
     if (first) {
       auto k = k_gs_phase_m_bulk<K, LANES, true>;
       bulk_attr(k, Sh::smem, c->device, &done[0]);
@@ -249,7 +240,7 @@ int spmv_m(Context* c, const Level& L, const double* x, double* y, double* parti
   if (bm) {
     using Sh = MultiShape<LANES>;
     auto k = k_spmv_m_bulk<K, LANES, DOT>;
-    static uint64_t done = 0;
+    static std::atomic<uint64_t> done{0};
     bulk_attr(k, Sh::smem, c->device, &done);
     const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
     const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
@@ -360,7 +351,9 @@ int load_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, dou
   const Level& L = P->lev[0];
   Context* c = P->ctx;
   const double* s = src;
-  if (!is_device_ptr(src)) {
+  bool dev = false;
+  HB_TRY(locate_ptr(src, P->device, &dev, "input vectors"));
+  if (!dev) {
     const size_t need = (size_t)nrhs * L.n;
     if (m->stage_cap < need) {
       cudaFree(m->stage);
@@ -382,7 +375,8 @@ template <int K>
 int store_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, double* dst) {
   const Level& L = P->lev[0];
   Context* c = P->ctx;
-  const bool dev = is_device_ptr(dst);
+  bool dev = false;
+  HB_TRY(locate_ptr(dst, P->device, &dev, "output vectors"));
   double* d = dst;
   const size_t need = (size_t)nrhs * L.n;
   if (!dev) {

@@ -23,7 +23,10 @@
 // Set-up. Host code cannot take the address of a __device__ array directly:
 // the name only stands for it on the host. The first call on each device (with
 // that device current) looks the address up with cudaGetSymbolAddress and
-// keeps it; make that first call before any stream capture on the device.
+// keeps it; make that first call before any stream capture on the device. The
+// kept address belongs to the device's context as it was then: after a
+// cudaDeviceReset on that device, do not call this entry point again in the
+// same process.
 //
 // Sharing. All calls on a device share the one array and it keeps the last
 // call's contents. Nothing in it has to start at zero: each call's first
@@ -94,7 +97,10 @@ int scratch_address(double** out) {
     hb::set_error("cudaGetDevice", e);
     return hb::status_of(e);
   }
-  if (dev < 0 || dev >= 64) return HPCG_B200_ERR_ARG;
+  if (dev < 0 || dev >= 64) {
+    hb::set_error_text("hpcg_b200_dot_noalloc: device ordinals of 64 and above are not supported");
+    return HPCG_B200_ERR_ARG;
+  }
   std::lock_guard<std::mutex> lock(g_partials_mu);
   if (!g_partials[dev]) {
     void* p = nullptr;
@@ -119,9 +125,27 @@ extern "C" int hpcg_b200_dot_noalloc(int n, const double* x, const double* y, do
     hb::set_error_text(msg);
     return HPCG_B200_ERR_ARG;
   }
-  if (!x || !y || !result || !hb::is_device_ptr(x) || !hb::is_device_ptr(y) || !hb::is_device_ptr(result)) {
+  if (!x || !y || !result) {
     hb::set_error_text("hpcg_b200_dot_noalloc: x, y and result must be device memory of the current GPU");
     return HPCG_B200_ERR_ARG;
+  }
+  int cur = 0;
+  const cudaError_t ge = cudaGetDevice(&cur);
+  if (ge != cudaSuccess) {
+    hb::set_error("cudaGetDevice", ge);
+    return hb::status_of(ge);
+  }
+  // device memory of the current GPU only: host memory, and another GPU's
+  // memory (which locate_ptr refuses with its own message), are not accepted
+  const void* args[3] = {x, y, result};
+  for (const void* a : args) {
+    bool on_device = false;
+    const int st = hb::locate_ptr(a, cur, &on_device, "hpcg_b200_dot_noalloc");
+    if (st != HPCG_B200_OK) return st;
+    if (!on_device) {
+      hb::set_error_text("hpcg_b200_dot_noalloc: x, y and result must be device memory of the current GPU");
+      return HPCG_B200_ERR_ARG;
+    }
   }
   double* partials = nullptr;
   const int s = scratch_address(&partials);

@@ -572,7 +572,9 @@ int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal) {
   Level& L = p->lev[0];
   Context* c = p->ctx;
   const double* src = diagonal;
-  if (!is_device_ptr(diagonal)) {
+  bool dev = false;
+  HB_TRY(locate_ptr(diagonal, p->device, &dev, "hpcg_b200_set_diagonal"));
+  if (!dev) {
     HB_TRY(ensure_stage(c, L.n));
     HB_CK(cudaMemcpyAsync(c->stage[1], diagonal, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
     src = c->stage[1];
@@ -598,7 +600,9 @@ int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27
   Context* c = p->ctx;
   double* tmp = nullptr;
   const double* src = values27;
-  if (!is_device_ptr(values27)) {
+  bool dev = false;
+  HB_TRY(locate_ptr(values27, p->device, &dev, "hpcg_b200_set_values"));
+  if (!dev) {
     HB_CK(cudaMalloc(&tmp, sizeof(double) * (size_t)kSlots * L.n));
     cudaError_t e = cudaMemcpy(tmp, values27, sizeof(double) * (size_t)kSlots * L.n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {

@@ -492,13 +492,16 @@ int hpcg_b200_shard_dot(hpcg_b200_comm* comm, const double* const* x, const doub
     // natural order in place (device) or staged (host): the sum runs in the caller's order
     const double* xd = x[i];
     const double* yd = y[i];
-    if (!is_device_ptr(xd) || !is_device_ptr(yd)) {
+    bool xdev = false, ydev = false;
+    HB_TRY(locate_ptr(xd, P->device, &xdev, "input vector"));
+    HB_TRY(locate_ptr(yd, P->device, &ydev, "input vector"));
+    if (!xdev || !ydev) {
       HB_TRY(ensure_stage(c, (size_t)n));
-      if (!is_device_ptr(xd)) {
+      if (!xdev) {
         HB_CK(cudaMemcpyAsync(c->stage[0], xd, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
         xd = c->stage[0];
       }
-      if (!is_device_ptr(yd)) {
+      if (!ydev) {
         HB_CK(cudaMemcpyAsync(c->stage[1], yd, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
         yd = c->stage[1];
       }

@@ -69,11 +69,8 @@ bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T
     tv = &m->val;
     tc = &m->col;
   }
-  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
-  if (!(attr_set >> c->device & 1)) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr_set |= 1ull << c->device;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
+  bulk_attr(k, smem, c->device, &attr_set);
   const int a0 = r0 & ~(kBulkRows - 1);
   const int64_t tiles = ((int64_t)r1 - a0 + kBulkRows - 1) / kBulkRows;
   int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
@@ -95,8 +92,22 @@ bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault, *tv, *tc,
-                     (const unsigned char*)L.colp, sink_of(L));
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault,
+                                     *tv, *tc, (const unsigned char*)L.colp, sink_of(L));
+  if (e != cudaSuccess && pdl) {
+    // refused with the early-launch attribute: record it and launch plainly
+    set_error("k_gs_bulk (programmatic dependent launch)", e);
+    cudaGetLastError();
+    cfg.numAttrs = 0;
+    e = cudaLaunchKernelEx(&cfg, k, val, cols_of<T>(L), L.pitch, rhs, x, r0, r1, mask, dot, c->fault, *tv, *tc,
+                           (const unsigned char*)L.colp, sink_of(L));
+  }
+  if (e != cudaSuccess) {
+    // refused outright (nothing was queued): the caller runs the register kernel instead
+    set_error("k_gs_bulk", e);
+    cudaGetLastError();
+    return false;
+  }
   return true;
 }
 
@@ -257,11 +268,8 @@ int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y,
   auto k = k_spmv_bulk<T, DOT, ORDER, PACK>;
   using Shape = SpmvShape<T, PACK>;
   constexpr int smem = Shape::smem;
-  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
-  if (!(attr_set >> c->device & 1)) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr_set |= 1ull << c->device;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
+  bulk_attr(k, smem, c->device, &attr_set);
   const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c->sms));
   k<<<g, Shape::threads, smem, c->stream>>>(L.g, val, cols_of<T>(L), L.pitch, x, y, L.n, partials, c->fault, m->val,
@@ -337,11 +345,8 @@ bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, cons
   auto k = k_restrict_bulk<T, PACK>;
   using Shape = SpmvShape<T, PACK>;
   constexpr int smem = Shape::smem;
-  static uint64_t attr_set = 0;  // devices on which the shared-memory size is enabled
-  if (!(attr_set >> c->device & 1)) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr_set |= 1ull << c->device;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
+  bulk_attr(k, smem, c->device, &attr_set);
   const int64_t tiles = ((int64_t)L.tf_run + nc - (L.tf_run & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
   const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
   k<<<g, Shape::threads, smem, c->stream>>>(val, cols_of<T>(L), L.pitch, rf, xf, L.tq, rc, L.tf_run, nc, c->fault,
@@ -1196,7 +1201,9 @@ int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst)
   const Level& L = p->lev[level];
   Context* c = p->ctx;
   const double* s = src;
-  if (!is_device_ptr(src)) {
+  bool dev = false;
+  HB_TRY(locate_ptr(src, p->device, &dev, "input vector"));
+  if (!dev) {
     HB_TRY(ensure_stage(c, L.n));
     HB_CK(cudaMemcpyAsync(c->stage[0], src, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
     s = c->stage[0];
@@ -1210,7 +1217,8 @@ int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst)
 int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
   const Level& L = p->lev[level];
   Context* c = p->ctx;
-  const bool dev = is_device_ptr(dst);
+  bool dev = false;
+  HB_TRY(locate_ptr(dst, p->device, &dev, "output vector"));
   double* d = dst;
   if (!dev) {
     HB_TRY(ensure_stage(c, L.n));
@@ -1232,7 +1240,9 @@ namespace {
 // A vector argument of the standalone routines as a device pointer: device
 // memory is used in place, host memory is staged into stage[slot].
 int device_view(Context* c, const double* v, int n, int slot, const double** out) {
-  if (is_device_ptr(v)) {
+  bool dev = false;
+  HB_TRY(locate_ptr(v, c->device, &dev, "input vector"));
+  if (dev) {
     *out = v;
     return HPCG_B200_OK;
   }
@@ -1341,7 +1351,8 @@ int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, in
   HB_TRY(store_vector(p, 0, p->x, grad_b));  // dL/db = lambda
   HB_TRY(load_vector(p, 0, x, p->Ap));       // the forward solution, colour order
   double* out = grad_values27;
-  const bool dev_out = is_device_ptr(grad_values27);
+  bool dev_out = false;
+  HB_TRY(locate_ptr(grad_values27, p->device, &dev_out, "grad_values27"));
   const size_t bytes = sizeof(double) * kSlots * (size_t)L.n;
   if (!dev_out) HB_CK(cudaMalloc(&out, bytes));
   k_adjoint_values<<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(L.g, L.col, L.pitch, L.n, p->x,
@@ -1411,7 +1422,8 @@ int hpcg_b200_waxpby(int n, double alpha, const double* x, double beta, const do
   HB_TRY(device_view(c, x, n, 0, &dx));
   if (y == x) dy = dx;
   else HB_TRY(device_view(c, y, n, 1, &dy));
-  const bool wdev = is_device_ptr(w);
+  bool wdev = false;
+  HB_TRY(locate_ptr(w, c->device, &wdev, "output vector"));
   if (!wdev) HB_TRY(ensure_stage(c, (size_t)n));
   double* dw = wdev ? w : c->stage[2];
   k_waxpby<false><<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, alpha, dx, beta, dy, dw, nullptr);

@@ -12,6 +12,8 @@
  *  - Vectors are passed as plain double pointers in the reference's natural row
  *    order (row = (iz*ny + iy)*nx + ix). A pointer may be host memory (pageable or
  *    pinned) or device memory of the problem's GPU; the library detects which.
+ *    Device memory of any other GPU is refused with HPCG_B200_ERR_ARG before
+ *    anything is launched.
  *    Host results are complete when the call returns (calls synchronise, since the
  *    reference times them with a host clock, src/mytimer.cpp).
  *  - Internally the matrix is device-resident in an 8-colour order; vectors are
@@ -197,9 +199,11 @@ int hpcg_b200_adjoint(hpcg_b200_problem* p, const double* x, const double* g, in
  * stream) and the call returns without waiting. Its only scratch is a fixed
  * 512 KiB array inside the library (present on every GPU that loads it), so
  * n is limited to HPCG_B200_DOT_NOALLOC_MAX_N; larger n returns
- * HPCG_B200_ERR_ARG. The first call on each device looks the array's address up
- * (make it before any stream capture). Calls that overlap on the GPU share the
- * array and race: serialise them. */
+ * HPCG_B200_ERR_ARG, as do host memory and another GPU's memory. The first
+ * call on each device looks the array's address up and keeps it (make it
+ * before any stream capture; after a cudaDeviceReset of that device the kept
+ * address is stale, so do not call again in that process). Calls that overlap
+ * on the GPU share the array and race: serialise them. */
 #define HPCG_B200_DOT_NOALLOC_MAX_N 268435456
 int hpcg_b200_dot_noalloc(int n, const double* x, const double* y, double* result, void* stream);
 
