@@ -379,8 +379,8 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
     fi_ms, fi_l, fi_rows = B.profile_read(B.PROF_GS32_FIRST, dev)
     B.profile(False, dev)
     peak, _ = measured_peak_hbm()
-    packed = P.level_packed(0) > 0 and P.level_config(0)["gs32"] == 10
-    full_gbs = metrics.gs_phase_bytes(fu_rows, n, vb=4, packed=packed) / (fu_ms * 1e-3) / 1e9 if fu_ms else None
+    pack = P.level_pack_width(0) if P.level_config(0)["gs32"] == 10 else 0
+    full_gbs = metrics.gs_phase_bytes(fu_rows, n, vb=4, pack=pack) / (fu_ms * 1e-3) / 1e9 if fu_ms else None
     first_gbs = metrics.first_sweep_bytes(fi_rows, vb=4) / (fi_ms * 1e-3) / 1e9 if fi_ms else None
     return {"fp64": {"iters": it64, "seconds": round(t64, 3), "scaled_residual": nr64 / nr064},
             "fp32_vcycle": {"iters": it32, "seconds": round(t32, 3), "scaled_residual": nr32 / nr032,
@@ -393,9 +393,9 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
                 "full_frac": round(full_gbs / peak, 4) if full_gbs else None,
                 "first_ms_per_iter": round(fi_ms / profile_iters, 3),
                 "first_gbs": round(first_gbs, 1) if first_gbs else None,
-                "bytes_per_row": {"full": round(metrics.gs_phase_bytes(1, 8, vb=4, packed=packed), 3),
+                "bytes_per_row": {"full": round(metrics.gs_phase_bytes(1, 8, vb=4, pack=pack), 3),
                                   "first_sweep": 130},
-                "packed_columns": packed}}
+                "column_offset_bytes": pack}}
 
 
 def gpu_launches_per_set(iters, nlevels=4, rtz_pass=False):
@@ -556,17 +556,18 @@ def b200_arm(args, rank, world, local_rank):
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         gs_cfg = tuning[0]["gs"]
-        packed0 = P.level_packed(0) > 0
-        gs_packed = packed0 and gs_cfg == 10
-        mv_packed = packed0 and tuning[0]["spmv"] == 7
-        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow, packed=gs_packed)
+        pack0 = P.level_pack_width(0)
+        gs_pack = pack0 if gs_cfg == 10 else 0
+        mv_pack = pack0 if tuning[0]["spmv"] == 7 else 0
+        gs_packed = gs_pack > 0
+        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow, pack=gs_pack)
         achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
         kernel = (f"k_gs_bulk<double,double,false> (level 0, configuration {gs_cfg}"
-                  f"{', packed columns' if gs_packed else ''})" if gs_cfg == 10 else
+                  f"{f', packed columns, {8 * gs_pack}-bit offsets' if gs_pack else ''})" if gs_cfg == 10 else
                   f"k_gs_phase<double,double,false> (level 0, configuration {gs_cfg})")
         tr = committed_traffic()
         traffic = None
-        if (tr and tr.get("n") == n and tr.get("config") == gs_cfg and bool(tr.get("packed", False)) == gs_packed
+        if (tr and tr.get("n") == n and tr.get("config") == gs_cfg and int(tr.get("pack", 0)) == gs_pack
                 and gs_launch):
             traffic = tr.get("bytes_per_launch")
         line = {
@@ -597,8 +598,8 @@ def b200_arm(args, rank, world, local_rank):
                          else peak_kind, "launches": gs_launch, "avg_launch_ms": round(gs_ms / max(gs_launch, 1), 4),
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
             "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
-                     "gbs": round(metrics.spmv_bytes(sp_rows, packed=mv_packed) / (sp_ms * 1e-3) / 1e9, 1)
-                     if sp_ms else None, "packed_columns": mv_packed},
+                     "gbs": round(metrics.spmv_bytes(sp_rows, pack=mv_pack) / (sp_ms * 1e-3) / 1e9, 1)
+                     if sp_ms else None, "column_offset_bytes": mv_pack},
             "first_sweep_gbs": round(metrics.first_sweep_bytes(gf_rows) / (gf_ms * 1e-3) / 1e9, 1) if gf_ms else None,
             "kernel_ms_per_iter": {
                 "gs_full_l0": round(gs_ms / (args.iters * args.steps), 3),

@@ -328,6 +328,15 @@ class Problem:
                "hpcg_b200_level_info")
         return n.value, pitch.value, starts
 
+    def level_pack_width(self, level):
+        """Offset width in bytes of the level's packed columns (1 or 2); 0 if it
+        keeps only its 32-bit columns."""
+        b = self.level_packed(level)
+        if b == 0:
+            return 0
+        _, pitch, _ = self.level_info(level)
+        return 1 if b == pitch // 128 * (28 * 4 + 27 * 128) else 2
+
     def level_packed(self, level):
         """Bytes of the level's packed column index (0: 32-bit columns only)."""
         b = C.c_int64(0)

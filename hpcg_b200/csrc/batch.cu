@@ -42,6 +42,7 @@ struct BGs {
   int first;
   int prob;
   const unsigned char* colp;  // the level's packed columns (bulk-copy phases)
+  int pack;                   // their offset width in bytes
   int sink;                   // the level's zero sink column
 };
 // residual + restriction, and prolongation, of one problem's level
@@ -102,8 +103,9 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
 // tile is one 128-row block of its problem's blocked FP32 values (val32 of the
 // single-problem path) and one record of its packed columns, so it arrives by
 // two copies; the tiles of problems that have converged are skipped on both
-// sides. Same arithmetic as k_b_gs.
-using BatchShape = GsShape<float, true>;
+// sides. Same arithmetic as k_b_gs. The problems' levels may pack their
+// columns with different offset widths: each tile's record states its own.
+using BatchShape = GsShape<float, -1>;
 __global__ void __launch_bounds__(BatchShape::threads, 1)
     k_b_gs_bulk(const BGs* __restrict__ items, const BTile* __restrict__ tiles, int ntiles,
                 const BScal* __restrict__ sc, unsigned* fault) {
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(BatchShape::threads, 1)
         const BGs& it = items[tl.item];
         return TileSrc<float>{tl.start, it.val + mat_index<float>(0, tl.start, it.pitch),
                               it.col + mat_index<float>(0, tl.start, it.pitch),
-                              it.colp + (tl.start / kBulkRows) * kPackRec};
+                              it.colp + (tl.start / kBulkRows) * pack_rec(it.pack), pack_rec(it.pack)};
       },
       [&](int t) { return !sc[items[tiles[t].item].prob].active; },
       [&](int t, int64_t q0, const float* sv, const int* scol, int row) {
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(BatchShape::threads, 1)
 #pragma unroll
           for (int k = 0; k < kSlots; ++k) {
             const float a = sv[k * kBulkRows + row];
-            const float xv = __ldg(it.x + stage_col<true>(scol, k, row, it.sink));
+            const float xv = __ldg(it.x + stage_col<-1>(scol, k, row, it.sink));
             sum -= a * xv;
             if (k == kDiagSlot) xd = xv;
           }
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(BatchShape::threads, 1)
           for (int k = 0; k < kSlots; ++k) {
             if (mask & (1u << k)) {
               const float a = sv[k * kBulkRows + row];
-              const float xv = __ldg(it.x + stage_col<true>(scol, k, row, it.sink));
+              const float xv = __ldg(it.x + stage_col<-1>(scol, k, row, it.sink));
               sum -= a * xv;
               if (k == kDiagSlot) xd = xv;
             }
@@ -477,6 +479,7 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       it.first = first ? 1 : 0;
       it.prob = p;
       it.colp = nullptr;
+      it.pack = 0;
       it.sink = 0;
       gs.push_back(it);
       tiles_of(tiles, item, it.r0, it.r1);
@@ -484,6 +487,7 @@ void build_vcycle(hpcg_b200_batch* B, int l, std::vector<BGs>& gs, std::vector<B
       bit.val = L.val32;
       bit.col = L.col32;
       bit.colp = L.colp;
+      bit.pack = L.pack;
       bit.sink = sink_of(L);
       if (!L.colp) B->packed = false;  // the bulk-copy phases need packed columns
       gsb.push_back(bit);

@@ -54,57 +54,93 @@ __host__ __device__ constexpr bool bulk_tensor_tile() {
 }
 // Packed columns: a level's column indices as one record per kBulkRows-row
 // tile of its storage (tile j: rows kBulkRows j ..): kSlots 32-bit bases and a
-// word of padding (the offsets start on 16 bytes), then kSlots x kBulkRows
-// 16-bit offsets, slot-major. Slot k of row t of the tile is column
-// base[k] + offset, or the level's zero sink where the offset is kPackSink.
-// A tile whose columns of one slot (sink aside) span more than kPackMaxSpan
-// does not pack; the level then keeps only its 32-bit columns. 55 bytes a row
-// instead of 108; one bulk copy per tile, as the blocked FP32 columns.
+// word that holds the offset width w (the offsets then start on 16 bytes),
+// then kSlots x kBulkRows offsets of w bytes, slot-major. Slot k of row t of
+// the tile is column base[k] + offset, or the level's zero sink where the
+// offset is pack_sink(w). w is 1 where every tile's columns of each slot (sink
+// aside) span at most pack_max_span(1) = 254, else 2 where they span at most
+// 65534; a level whose tiles span more keeps only its 32-bit columns. 27.9
+// (w = 1) or 54.9 (w = 2) bytes a row instead of 108; one bulk copy per tile,
+// as the blocked FP32 columns.
 constexpr int kPackBaseWords = 28;
-constexpr int kPackRec = kPackBaseWords * 4 + kSlots * kBulkRows * 2;  // 7024 bytes
-constexpr unsigned kPackSink = 0xFFFFu;
-constexpr int kPackMaxSpan = 0xFFFE;
-static_assert(kPackRec % 16 == 0, "a record is one bulk copy");
+__host__ __device__ constexpr int pack_rec(int w) { return kPackBaseWords * 4 + kSlots * kBulkRows * w; }
+__host__ __device__ constexpr unsigned pack_sink(int w) { return w == 1 ? 0xFFu : 0xFFFFu; }
+__host__ __device__ constexpr int pack_max_span(int w) { return w == 1 ? 0xFE : 0xFFFE; }
+static_assert(pack_rec(1) % 16 == 0 && pack_rec(2) % 16 == 0, "a record is one bulk copy");
 
 // Shape of a pipeline: G consumer groups of kBulkRows x LANES threads, each
 // with a ring of RING stages of one tile. A stage holds the tile's values and
-// its columns (32-bit, or the packed record when PACKED), rounded up to 128
-// bytes (tensor copies land on 128-byte boundaries): FP64 stages are 41.5 KB
-// (33.9 KB packed) and FP32 ones 27 KB (20.4 KB packed); all stages of a block
-// share at most 227 KB of shared memory (one block per SM).
-template <typename T, int G, int RING, int LANES = 1, bool PACKED = false>
+// its columns: 32-bit (PW = 0), or the packed record with offsets of PW bytes
+// (PW = 1, 2), or, with PW = -1, a record whose width each tile states (the
+// batched kernel, whose tiles come from several levels): staged for the wider
+// one, each fill expecting its own record's bytes. Stages are rounded up to
+// 128 bytes (tensor copies land on 128-byte boundaries): FP64 stages are 41.5
+// KB (33.9 KB with 16-bit offsets, 30.5 KB with 8-bit ones) and FP32 ones 27
+// KB (20.4 / 17 KB); all stages of a block share at most 227 KB of shared
+// memory (one block per SM).
+template <typename T, int G, int RING, int LANES = 1, int PW = 0>
 struct BulkShape {
   static constexpr int groups = G;
   static constexpr int ring = RING;
   static constexpr int lanes = LANES;
-  static constexpr bool packed = PACKED;
+  static constexpr int pack = PW;
+  static constexpr bool packed = PW != 0;
   static constexpr int group_threads = kBulkRows * LANES;
   static constexpr int stages = groups * ring;
   static constexpr int threads = 32 + groups * group_threads;  // producer warp + consumers
   static constexpr int value_bytes = kSlots * kBulkRows * (int)sizeof(T);
-  static constexpr int col_bytes = PACKED ? kPackRec : kSlots * kBulkRows * (int)sizeof(int);
-  static constexpr int tx_bytes = value_bytes + col_bytes;  // bytes landing in a stage per fill
+  static constexpr int col_bytes = PW == 0 ? kSlots * kBulkRows * (int)sizeof(int) : pack_rec(PW < 0 ? 2 : PW);
+  static constexpr int tx_bytes = value_bytes + col_bytes;  // bytes landing in a stage per fill (PW >= 0)
   static constexpr int stage_bytes = (tx_bytes + 127) / 128 * 128;
   // stages + barriers + slack to align the stages to 128 bytes (tensor copies)
   static constexpr int smem = stages * stage_bytes + 2 * stages * (int)sizeof(uint64_t) + 128;
   static_assert(smem <= 227 * 1024, "shared memory of one block");
   static_assert(threads <= 1024, "threads of one block");
+  static_assert(PW >= -1 && PW <= 2, "offset width");
 };
-// The shapes in use (measured at 512^3: two groups of two stages beat four
-// groups of one for the Gauss-Seidel phases by 8% and tied for the SpMV).
-template <typename T, bool PACKED = false>
-using GsShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2, 1, PACKED>;
-template <typename T, bool PACKED = false>
-using SpmvShape = BulkShape<T, sizeof(T) == 8 ? 2 : 3, 2, 1, PACKED>;
+// The shapes in use: rings of two stages (measured at 512^3: two groups of two
+// stages beat four groups of one for the Gauss-Seidel phases by 8% and tied for
+// the SpMV), with as many consumer groups as asked for and as fit in 227 KB.
+// A phase's consumers wait on their gathers of x, and one block per SM leaves
+// few warps to cover that latency: with 8-bit offsets (31 KB FP64 stages,
+// 17 KB FP32 ones) measured at 512^3, three FP64 groups instead of two took a
+// phase from 0.93 to 0.80 ms and four FP32 groups instead of three from 11.4
+// to 10.0 ms per iteration (five: 10.2); a third SpMV group was slower (5.84
+// to 6.46 ms), so the SpMV keeps two. A shape whose stages do not fit (32-bit
+// columns) gets fewer groups.
+#ifndef HB_GS64_GROUPS
+#define HB_GS64_GROUPS 3
+#endif
+#ifndef HB_GS32_GROUPS
+#define HB_GS32_GROUPS 4
+#endif
+#ifndef HB_SPMV_GROUPS
+#define HB_SPMV_GROUPS 2
+#endif
+template <typename T, int PW>
+__host__ __device__ constexpr int fit_groups(int want) {
+  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * 2 * want + 32 * want + 128 > 227 * 1024) --want;
+  return want;
+}
+template <typename T, int PW = 0>
+using GsShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_GS64_GROUPS : HB_GS32_GROUPS), 2, 1, PW>;
+template <typename T, int PW = 0>
+using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_GS32_GROUPS), 2, 1, PW>;
 
-// Column of slot k of row t of a tile in a stage (sc: the stage's column area).
-template <bool PACKED>
+// Column of slot k of row t of a tile in a stage (sc: the stage's column area)
+// for the column form PW of BulkShape.
+template <int PW>
 __device__ __forceinline__ int stage_col(const int* sc, int k, int t, int sink) {
-  if constexpr (PACKED) {
-    const unsigned o = reinterpret_cast<const unsigned short*>(sc + kPackBaseWords)[k * kBulkRows + t];
-    return o == kPackSink ? sink : sc[k] + (int)o;
-  } else {
+  if constexpr (PW == 0) {
     return sc[k * kBulkRows + t];
+  } else if constexpr (PW == 1) {
+    const unsigned o = reinterpret_cast<const unsigned char*>(sc + kPackBaseWords)[k * kBulkRows + t];
+    return o == pack_sink(1) ? sink : sc[k] + (int)o;
+  } else if constexpr (PW == 2) {
+    const unsigned o = reinterpret_cast<const unsigned short*>(sc + kPackBaseWords)[k * kBulkRows + t];
+    return o == pack_sink(2) ? sink : sc[k] + (int)o;
+  } else {
+    return sc[kSlots] == 1 ? stage_col<1>(sc, k, t, sink) : stage_col<2>(sc, k, t, sink);
   }
 }
 
@@ -185,13 +221,15 @@ __device__ __forceinline__ void record_fault(unsigned* fault, unsigned code) {
 
 // Where a tile comes from: its first row and, when the tile is one block of
 // the layout (whole-tile copies), the addresses of its value and column blocks;
-// with packed columns, the address of its record.
+// with packed columns, the address of its record and (read only when the
+// shape's offset width is per tile, PW = -1) the record's bytes.
 template <typename T>
 struct TileSrc {
   int64_t q0;
   const T* vals;
   const int* cols;
   const unsigned char* rec;
+  int rec_bytes;
 };
 
 // The producer/consumer pipeline of the bulk-copy kernels, run by the whole
@@ -203,7 +241,7 @@ struct TileSrc {
 // every tile of its group, t its index in the group (row t / LANES of the tile,
 // lane t % LANES), with the tile's values sv[k * kBulkRows + row] and columns
 // on chip: sc[k * kBulkRows + row], or the packed record at sc
-// (stage_col<Shape::packed> reads either).
+// (stage_col<Shape::pack> reads any of them).
 template <typename T, typename Shape, typename Src, typename Skip, typename RowFn>
 __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, RowFn row, unsigned* fault,
                                                const CUtensorMap* tm_val, const CUtensorMap* tm_col) {
@@ -246,17 +284,18 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
       if (skip(tile)) continue;
       const int kg = i / G;
       const int s = (i % G) * RING + kg % RING, use = kg / RING;
+      const TileSrc<T> ts = src(tile);
+      const int rec_bytes = Shape::pack < 0 ? ts.rec_bytes : Shape::col_bytes;
       int ok = 1;
       if (lane == 0) {
         if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) {
           record_fault(fault, 1);
           ok = 0;
         } else {
-          mbar_expect_tx(&full[s], Shape::tx_bytes);
+          mbar_expect_tx(&full[s], Shape::value_bytes + rec_bytes);
         }
       }
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
-      const TileSrc<T> ts = src(tile);
       T* sv = reinterpret_cast<T*>(smem + s * SB);
       int* sc = reinterpret_cast<int*>(smem + s * SB + VB);
       if constexpr (bulk_whole_tile<T>()) {
@@ -267,7 +306,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
         if (lane == 0) tma_load_2d(sv, tm_val, (int)ts.q0, 0, &full[s], policy);
       }
       if constexpr (Shape::packed) {
-        if (lane == 1) bulk_g2s(sc, ts.rec, kPackRec, &full[s], policy);
+        if (lane == 1) bulk_g2s(sc, ts.rec, rec_bytes, &full[s], policy);
       } else if constexpr (bulk_whole_tile<T>()) {
         if (lane == 1) bulk_g2s(sc, ts.cols, kSlots * kBulkRows * sizeof(int), &full[s], policy);
       } else {
@@ -321,8 +360,10 @@ __device__ __forceinline__ void bulk_tiles(const T* __restrict__ val, const int*
       ntiles,
       [&](int tile) {
         const int64_t q0 = first_row(tile);
+        static_assert(Shape::pack >= 0, "one offset width per level");
         return TileSrc<T>{q0, val + mat_index<T>(0, q0, pitch), col + mat_index<T>(0, q0, pitch),
-                          Shape::packed ? colp + (q0 / kBulkRows) * kPackRec : nullptr};
+                          Shape::packed ? colp + (q0 / kBulkRows) * pack_rec(Shape::pack) : nullptr,
+                          Shape::col_bytes};
       },
       [](int) { return false; },
       [&](int, int64_t q0, const T* sv, const int* sc, int t) { row(q0, sv, sc, t); }, fault, &tm_val, &tm_col);

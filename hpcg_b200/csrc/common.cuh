@@ -198,6 +198,11 @@ struct Level {
   int gs_sched32 = 1;        // kernel configuration of the Gauss-Seidel phases (FP32 V-cycle)
   int gs_first32 = 1;        // ... of its first-sweep phases
   int gs_first = 1;          // kernel configuration of the first-sweep phases (FP64)
+  // the first-sweep configuration per sweep position, tuned position by
+  // position (a phase reads 0 to 26 slots by its position); -1: gs_first /
+  // gs_first32 at every position
+  int gs_first_at[kColours] = {-1, -1, -1, -1, -1, -1, -1, -1};
+  int gs_first32_at[kColours] = {-1, -1, -1, -1, -1, -1, -1, -1};
   int mv_sched = 1;          // kernel configuration of SpMV / restriction
   int mv_order = 0;          // SpMV row order: 0 storage, 1 natural, 2 slab (see k_spmv)
   bool tuned = false;
@@ -207,8 +212,9 @@ struct Level {
   int* wave_start = nullptr; // host array [nwaves+1]
   mutable BulkMaps* maps = nullptr;  // host; built on the first bulk-copy phase
   // the columns packed for the bulk-copy kernels (one record per 128-row tile:
-  // 27 bases and 16-bit offsets), nullptr if they do not pack
+  // 27 bases and offsets of `pack` bytes), nullptr (pack 0) if they do not pack
   unsigned char* colp = nullptr;
+  int pack = 0;
 };
 
 struct Context;
@@ -233,6 +239,10 @@ struct hpcg_b200_problem {
   bool coarse_graph_failed;         // its capture was refused once: stream launches
   hb::RankGeom* geom;  // position in a run over several ranks (nullptr: one rank)
   size_t bytes;  // device bytes held
+  // hpcg_b200_cg's host right-hand side as last sent (a host copy of n entries)
+  // and whether b still holds it (every other load into b clears the flag)
+  double* b_kept_host;
+  bool b_kept;
 };
 
 namespace hb {

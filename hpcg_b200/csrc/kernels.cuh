@@ -307,9 +307,10 @@ __global__ void k_wait_selftest(unsigned long long limit_ns, unsigned* fault) {
 }
 
 // Gauss-Seidel colour phase over rows [r0, r1) through the pipeline
-// (configuration 10); PACK: the level's packed columns (colp, sink).
-template <typename T, typename TR, bool FIRST, int64_t CMASK = -1, bool DOT = false, bool PACK = false>
-__global__ void __launch_bounds__(GsShape<T, PACK>::threads, 1)
+// (configuration 10); PW: the level's column form (0: 32-bit columns; 1, 2:
+// the packed record colp with offsets of PW bytes, sink its zero column).
+template <typename T, typename TR, bool FIRST, int64_t CMASK = -1, bool DOT = false, int PW = 0>
+__global__ void __launch_bounds__(GsShape<T, PW>::threads, 1)
     k_gs_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const TR* __restrict__ rhs,
               T* x, int r0, int r1, uint32_t mask_arg, double* __restrict__ dot, unsigned* fault,
               const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(GsShape<T, PACK>::threads, 1)
   const int a0 = r0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, GsShape<T, PACK>>(
+  bulk_tiles<T, GsShape<T, PW>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t) {
         const int64_t q = q0 + t;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(GsShape<T, PACK>::threads, 1)
         for (int k = 0; k < kSlots; ++k) {
           if (mask & (1u << k)) {
             const T a = sv[k * kBulkRows + t];
-            const T xv = __ldg(x + stage_col<PACK>(sc, k, t, sink));
+            const T xv = __ldg(x + stage_col<PW>(sc, k, t, sink));
             sum -= a * xv;
             if (k == kDiagSlot) xd = xv;
           }
@@ -506,8 +507,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_spmv(ColourGrid g, 
 // colours, then the next z pair), which needs slab runs that split into whole
 // tiles and colour blocks that start on an even row (checked on the host).
 // Partials: one per block.
-template <typename T, bool DOT, int ORDER, bool PACK = false>
-__global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
+template <typename T, bool DOT, int ORDER, int PW = 0>
+__global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
     k_spmv_bulk(ColourGrid g, const T* __restrict__ val, const int* __restrict__ col, int64_t pitch,
                 const T* __restrict__ x, T* __restrict__ y, int n, double* __restrict__ partials, unsigned* fault,
                 const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
@@ -515,7 +516,7 @@ __global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
   static_assert(ORDER == 0 || ORDER == 2, "storage or slab order");
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, SpmvShape<T, PACK>>(
+  bulk_tiles<T, SpmvShape<T, PW>>(
       val, col, pitch, ntiles,
       [&](int tile) {
         return ORDER == 2 ? slab_row(g, (int64_t)tile * kBulkRows) : (int64_t)tile * kBulkRows;
@@ -527,7 +528,7 @@ __global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
         T xq = (T)0;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-          const T xv = __ldg(x + stage_col<PACK>(sc, k, t, sink));
+          const T xv = __ldg(x + stage_col<PW>(sc, k, t, sink));
           sum += sv[k * kBulkRows + t] * xv;
           if (k == kDiagSlot) xq = xv;
         }
@@ -581,8 +582,8 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
 // The restriction through the bulk-copy pipeline (with SpMV configuration 7),
 // when the injected rows are one run f0 .. f0 + nc of fine rows (tf[t] = f0 + t,
 // checked on the host): the run is tiled like a phase. Same sums as k_restrict.
-template <typename T, bool PACK = false>
-__global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
+template <typename T, int PW = 0>
+__global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
     k_restrict_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const T* __restrict__ rf,
                     const T* __restrict__ xf, const int* __restrict__ tq, T* __restrict__ rc, int f0, int nc,
                     unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
@@ -590,14 +591,14 @@ __global__ void __launch_bounds__(SpmvShape<T, PACK>::threads, 1)
   const int r1 = f0 + nc;
   const int a0 = f0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<T, SpmvShape<T, PACK>>(
+  bulk_tiles<T, SpmvShape<T, PW>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t) {
         const int64_t f = q0 + t;
         if (f < f0 || f >= r1) return;
         T sum = (T)0;
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * __ldg(xf + stage_col<PACK>(sc, k, t, sink));
+        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * __ldg(xf + stage_col<PW>(sc, k, t, sink));
         rc[tq[f - f0]] = rf[f] - sum;
       },
       fault, tm_val, tm_col, colp);

@@ -131,17 +131,17 @@ __global__ void __launch_bounds__(kThreads) k_spmv_m(const double* __restrict__ 
 
 // Pipeline shapes of the multi-system kernels: LANES threads per row, at most
 // 1024 threads a block (four lanes: one group with a ring of four stages). The
-// columns arrive packed (the level's packed record per tile).
-template <int LANES>
-using MultiShape = BulkShape<double, LANES == 4 ? 1 : 2, LANES == 4 ? 4 : 2, LANES, true>;
+// columns arrive packed (the level's packed record per tile, offsets of PW bytes).
+template <int LANES, int PW>
+using MultiShape = BulkShape<double, LANES == 4 ? 1 : 2, LANES == 4 ? 4 : 2, LANES, PW>;
 
 // k_gs_phase_m through the bulk-copy pipeline (bulk.cuh): the tile's values
 // arrive on chip by a tensor copy and its packed columns (colp, sink) by a bulk
 // copy; the lanes of a row gather their S-entry runs of x as in k_gs_phase_m,
 // in the same order: the same bits. The full-slot phases (FIRST false) take all
 // 27 slots.
-template <int K, int LANES, bool FIRST>
-__global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
+template <int K, int LANES, bool FIRST, int PW>
+__global__ void __launch_bounds__(MultiShape<LANES, PW>::threads, 1)
     k_gs_phase_m_bulk(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch,
                       const double* __restrict__ rhs, double* x, int r0, int r1, uint32_t mask_arg, unsigned* fault,
                       const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
   const uint32_t mask = FIRST ? mask_arg : kAllSlots;
   const int a0 = r0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<double, MultiShape<LANES>>(
+  bulk_tiles<double, MultiShape<LANES, PW>>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const double* sv, const int* sc, int t) {
         const int row = t / LANES;
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
           if (mask & (1u << k)) {
             const double a = sv[k * kBulkRows + row];
             double xv[S];
-            load_k<S>(x + (int64_t)stage_col<true>(sc, k, row, sink) * K + off, xv);
+            load_k<S>(x + (int64_t)stage_col<PW>(sc, k, row, sink) * K + off, xv);
 #pragma unroll
             for (int j = 0; j < S; ++j) {
               sum[j] -= a * xv[j];
@@ -188,8 +188,8 @@ __global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
 
 // k_spmv_m through the bulk-copy pipeline (packed columns), rows in storage
 // order; DOT: partials of x_j'y_j at partials[j*gridDim.x + block].
-template <int K, int LANES, bool DOT>
-__global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
+template <int K, int LANES, bool DOT, int PW>
+__global__ void __launch_bounds__(MultiShape<LANES, PW>::threads, 1)
     k_spmv_m_bulk(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch,
                   const double* __restrict__ x, double* __restrict__ y, int n, double* __restrict__ partials,
                   unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
 #pragma unroll
   for (int j = 0; j < S; ++j) acc[j] = 0.0;
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<double, MultiShape<LANES>>(
+  bulk_tiles<double, MultiShape<LANES, PW>>(
       val, col, pitch, ntiles, [&](int tile) { return (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const double* sv, const int* sc, int t) {
         const int row = t / LANES;
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(MultiShape<LANES>::threads, 1)
         for (int k = 0; k < kSlots; ++k) {
           const double a = sv[k * kBulkRows + row];
           double xv[S];
-          load_k<S>(x + (int64_t)stage_col<true>(sc, k, row, sink) * K + off, xv);
+          load_k<S>(x + (int64_t)stage_col<PW>(sc, k, row, sink) * K + off, xv);
 #pragma unroll
           for (int j = 0; j < S; ++j) {
             sum[j] += a * xv[j];

@@ -198,6 +198,27 @@ int ensure_state(hpcg_b200_problem* P, MultiState** out) {
   return HPCG_B200_OK;
 }
 
+// The multi-system phase on the bulk-copy pipeline, packed columns of PW bytes.
+template <int K, int LANES, int PW>
+void launch_phase_m_bulk(Context* c, const Level& L, const BulkMaps* bm, const double* rhs, double* x, int r0,
+                         int r1, bool first, uint32_t mask) {
+  using Sh = MultiShape<LANES, PW>;
+  const int64_t tiles = ((int64_t)r1 - (r0 & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
+  const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+  static std::atomic<uint64_t> done[2] = {{0}, {0}};
+  if (first) {
+    auto k = k_gs_phase_m_bulk<K, LANES, true, PW>;
+    bulk_attr(k, Sh::smem, c->device, &done[0]);
+    k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
+                                                bm->col, L.colp, sink_of(L));
+  } else {
+    auto k = k_gs_phase_m_bulk<K, LANES, false, PW>;
+    bulk_attr(k, Sh::smem, c->device, &done[1]);
+    k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
+                                                bm->col, L.colp, sink_of(L));
+  }
+}
+
 template <int K, int LANES, int BULK>
 void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, int r0, int r1, bool first,
                     uint32_t mask) {
@@ -205,21 +226,10 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
   // the register-pipelined kernels
   const BulkMaps* bm = L.colp && (BULK == 2 || (BULK == 1 && !first)) ? bulk_maps(L) : nullptr;
   if (bm) {
-    using Sh = MultiShape<LANES>;
-    const int64_t tiles = ((int64_t)r1 - (r0 & ~(kBulkRows - 1)) + kBulkRows - 1) / kBulkRows;
-    const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
-    static std::atomic<uint64_t> done[2] = {{0}, {0}};
-    if (first) {
-      auto k = k_gs_phase_m_bulk<K, LANES, true>;
-      bulk_attr(k, Sh::smem, c->device, &done[0]);
-      k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
-                                                  bm->col, L.colp, sink_of(L));
-    } else {
-      auto k = k_gs_phase_m_bulk<K, LANES, false>;
-      bulk_attr(k, Sh::smem, c->device, &done[1]);
-      k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, rhs, x, r0, r1, mask, c->fault, bm->val,
-                                                  bm->col, L.colp, sink_of(L));
-    }
+    if (L.pack == 1)
+      launch_phase_m_bulk<K, LANES, 1>(c, L, bm, rhs, x, r0, r1, first, mask);
+    else
+      launch_phase_m_bulk<K, LANES, 2>(c, L, bm, rhs, x, r0, r1, first, mask);
     return;
   }
   const int64_t work = (int64_t)(r1 - r0) * LANES;
@@ -232,20 +242,29 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
   }
 }
 
+// The multi-system SpMV on the bulk-copy pipeline, packed columns of PW bytes;
+// returns the grid.
+template <int K, int LANES, bool DOT, int PW>
+int spmv_m_bulk(Context* c, const Level& L, const BulkMaps* bm, const double* x, double* y, double* partials) {
+  using Sh = MultiShape<LANES, PW>;
+  auto k = k_spmv_m_bulk<K, LANES, DOT, PW>;
+  static std::atomic<uint64_t> done{0};
+  bulk_attr(k, Sh::smem, c->device, &done);
+  const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
+  const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
+  k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, x, y, L.n, partials, c->fault, bm->val, bm->col,
+                                              L.colp, sink_of(L));
+  return g;
+}
+
 // y = A x for K systems; returns the number of blocks (DOT: partial sets written)
 // or a negative status.
 template <int K, int LANES, int BULK, bool DOT>
 int spmv_m(Context* c, const Level& L, const double* x, double* y, double* partials) {
   const BulkMaps* bm = BULK && L.colp ? bulk_maps(L) : nullptr;
   if (bm) {
-    using Sh = MultiShape<LANES>;
-    auto k = k_spmv_m_bulk<K, LANES, DOT>;
-    static std::atomic<uint64_t> done{0};
-    bulk_attr(k, Sh::smem, c->device, &done);
-    const int64_t tiles = ((int64_t)L.n + kBulkRows - 1) / kBulkRows;
-    const int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
-    k<<<g, Sh::threads, Sh::smem, c->stream>>>(L.val, L.col, L.pitch, x, y, L.n, partials, c->fault, bm->val,
-                                                bm->col, L.colp, sink_of(L));
+    const int g = L.pack == 1 ? spmv_m_bulk<K, LANES, DOT, 1>(c, L, bm, x, y, partials)
+                              : spmv_m_bulk<K, LANES, DOT, 2>(c, L, bm, x, y, partials);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       set_error("k_spmv_m_bulk", e);

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <functional>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "bulk.cuh"
@@ -202,22 +203,24 @@ int build_transfer(hpcg_b200_problem* p, int l) {
   return HPCG_B200_OK;
 }
 
-// The packed columns of a level (kPackRec records, one per kBulkRows-row tile
-// of the storage): block b builds tiles b, b + gridDim.x, ..., thread t row t
-// of the tile. Rows at or beyond n are stored as the sink (they are never
-// computed). Sets *bad if the columns of a slot of a tile span more than
-// kPackMaxSpan.
+// The packed columns of a level with offsets of W bytes (records of
+// pack_rec(W) bytes, one per kBulkRows-row tile of the storage): block b builds
+// tiles b, b + gridDim.x, ..., thread t row t of the tile. Rows at or beyond n
+// are stored as the sink (they are never computed). Sets *bad if the columns
+// of a slot of a tile span more than pack_max_span(W).
+template <int W>
 __global__ void __launch_bounds__(kBulkRows) k_pack_cols(const int* __restrict__ col, int64_t pitch, int n,
                                                          int sink, int64_t ntiles, unsigned char* __restrict__ colp,
                                                          int* bad) {
-  constexpr int W = kBulkRows / 32;
-  __shared__ int wlo[W], whi[W];
+  using Off = typename std::conditional<W == 1, unsigned char, unsigned short>::type;
+  constexpr int NW = kBulkRows / 32;
+  __shared__ int wlo[NW], whi[NW];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t q = tile * kBulkRows + t;
-    int* base = reinterpret_cast<int*>(colp + tile * kPackRec);
-    unsigned short* off = reinterpret_cast<unsigned short*>(base + kPackBaseWords);
-    if (t < kPackBaseWords - kSlots) base[kSlots + t] = 0;
+    int* base = reinterpret_cast<int*>(colp + tile * pack_rec(W));
+    Off* off = reinterpret_cast<Off*>(base + kPackBaseWords);
+    if (t == 0) base[kSlots] = W;  // the record states its offset width
     for (int k = 0; k < kSlots; ++k) {
       const int c = q < n ? col[mat_index<double>(k, q, pitch)] : sink;
       const bool real = c != sink;
@@ -233,7 +236,7 @@ __global__ void __launch_bounds__(kBulkRows) k_pack_cols(const int* __restrict__
       }
       __syncthreads();
 #pragma unroll
-      for (int i = 0; i < W; ++i) {
+      for (int i = 0; i < NW; ++i) {
         lo = min(lo, wlo[i]);
         hi = max(hi, whi[i]);
       }
@@ -241,46 +244,62 @@ __global__ void __launch_bounds__(kBulkRows) k_pack_cols(const int* __restrict__
       const int b = lo == INT_MAX ? 0 : lo;
       if (t == 0) {
         base[k] = b;
-        if (lo != INT_MAX && (int64_t)hi - lo > kPackMaxSpan) *bad = 1;
+        if (lo != INT_MAX && (int64_t)hi - lo > pack_max_span(W)) *bad = 1;
       }
-      off[k * kBulkRows + t] = real ? (unsigned short)(c - b) : (unsigned short)kPackSink;
+      off[k * kBulkRows + t] = real ? (Off)(c - b) : (Off)pack_sink(W);
     }
   }
 }
 
-// The packed columns of level l for the bulk-copy kernels (k_pack_cols). The
-// level keeps only its 32-bit columns if a tile does not pack, or with
-// HPCG_B200_PACKED=0.
-int build_packed(hpcg_b200_problem* p, int l) {
+// Packs level l's columns with W-byte offsets into a new allocation; on return
+// L.colp / L.pack describe it, or are left empty if a tile does not pack.
+template <int W>
+int try_pack(hpcg_b200_problem* p, int l) {
   Level& L = p->lev[l];
-  const char* e = std::getenv("HPCG_B200_PACKED");
-  if ((e && e[0] == '0') || L.n <= 0) return HPCG_B200_OK;
   Context* c = p->ctx;
   const int64_t ntiles = L.pitch / kBulkRows;
-  const size_t bytes = (size_t)ntiles * kPackRec;
-  HB_TRY(dev_alloc((void**)&L.colp, bytes, &p->bytes));
+  const size_t bytes = (size_t)ntiles * pack_rec(W);
+  unsigned char* colp = nullptr;
+  HB_TRY(dev_alloc((void**)&colp, bytes, &p->bytes));
   int* bad = nullptr;
-  HB_CK(cudaMalloc(&bad, sizeof(int)));
+  cudaError_t err = cudaMalloc(&bad, sizeof(int));
   int h = 0;
-  cudaError_t err = cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
+  if (err == cudaSuccess) err = cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
   if (err == cudaSuccess) {
     const int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms * 16);
-    k_pack_cols<<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, L.colp, bad);
+    k_pack_cols<W><<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, colp, bad);
     err = cudaGetLastError();
   }
   if (err == cudaSuccess) err = cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   cudaFree(bad);
-  if (err != cudaSuccess) {
-    set_error("pack columns", err);
-    return status_of(err);
-  }
-  if (h) {  // a tile does not pack: give the memory back
-    dev_free(L.colp);
-    L.colp = nullptr;
+  if (err != cudaSuccess || h) {  // failed, or a tile does not pack: give the memory back
+    dev_free(colp);
     p->bytes -= bytes;
     release_accounted(bytes);
+    if (err != cudaSuccess) {
+      set_error("pack columns", err);
+      return status_of(err);
+    }
+    return HPCG_B200_OK;
   }
+  L.colp = colp;
+  L.pack = W;
+  return HPCG_B200_OK;
+}
+
+// The packed columns of level l for the bulk-copy kernels (k_pack_cols): 8-bit
+// offsets where every tile's spans allow, else 16-bit ones; the level keeps
+// only its 32-bit columns if a tile does not pack either way.
+// HPCG_B200_PACKED at creation: "0" leaves every level unpacked, "16" skips
+// the 8-bit form (for comparisons).
+int build_packed(hpcg_b200_problem* p, int l) {
+  Level& L = p->lev[l];
+  const char* e = std::getenv("HPCG_B200_PACKED");
+  if ((e && e[0] == '0') || L.n <= 0) return HPCG_B200_OK;
+  const bool allow8 = !(e && std::strcmp(e, "16") == 0);
+  if (allow8) HB_TRY(try_pack<1>(p, l));
+  if (!L.colp) HB_TRY(try_pack<2>(p, l));
   return HPCG_B200_OK;
 }
 
@@ -298,6 +317,7 @@ int free_problem(hpcg_b200_problem* p) {
   }
   void* vs[] = {p->b, p->x, p->r, p->z, p->p, p->Ap, p->zprev};
   for (void* q : vs) dev_free(q);
+  delete[] p->b_kept_host;
   free_multi(p);
   free_plans(p);
   for (int i = 0; i < 2; ++i) {
@@ -661,7 +681,7 @@ int hpcg_b200_level_packed(const hpcg_b200_problem* p, int level, int64_t* bytes
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   if (!bytes || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
   const Level& L = p->lev[level];
-  *bytes = L.colp ? L.pitch / kBulkRows * kPackRec : 0;
+  *bytes = L.colp ? L.pitch / kBulkRows * pack_rec(L.pack) : 0;
   return HPCG_B200_OK;
 }
 

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 #include "shard.cuh"
 
@@ -90,6 +91,55 @@ int nccl_status(ncclResult_t r, const char* what) {
     if (s_ != HPCG_B200_OK) return s_;           \
   } while (0)
 
+// CUDA-event timing of the parts of a CG call into the reference's times[]
+// slots (CG.cpp:132-139): 1 dot products, 2 vector updates, 3 SpMV (with its
+// halo exchange, as ComputeSPMV_ref.cpp:53 does it), 4 the allreduce step of
+// the dot products (inside their slot-1 time, as ComputeDotProduct_ref.cpp:69-72
+// measures it), 5 the preconditioner. Pairs may nest; off when `c` is null.
+struct PartTimer {
+  Context* c = nullptr;
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> parts;
+  // starts a part of `slot`; *id identifies it for stop()
+  int start(int slot, int* id) {
+    *id = -1;
+    if (!c) return HPCG_B200_OK;
+    cudaEvent_t e;
+    HB_CK(cudaEventCreate(&e));
+    parts.emplace_back(slot, e, nullptr);
+    *id = (int)parts.size() - 1;
+    HB_CK(cudaEventRecord(e, c->stream));
+    return HPCG_B200_OK;
+  }
+  int stop(int id) {
+    if (!c || id < 0) return HPCG_B200_OK;
+    cudaEvent_t e;
+    HB_CK(cudaEventCreate(&e));
+    std::get<2>(parts[id]) = e;
+    HB_CK(cudaEventRecord(e, c->stream));
+    return HPCG_B200_OK;
+  }
+  // adds the parts' durations to times[slot] (synchronises the stream)
+  int add_to(double* times) {
+    if (!c) return HPCG_B200_OK;
+    HB_CK(cudaStreamSynchronize(c->stream));
+    for (auto& p : parts) {
+      float ms = 0.f;
+      if (std::get<2>(p)) HB_CK(cudaEventElapsedTime(&ms, std::get<1>(p), std::get<2>(p)));
+      times[std::get<0>(p)] += ms * 1e-3;
+    }
+    release();
+    return HPCG_B200_OK;
+  }
+  void release() {
+    for (auto& p : parts) {
+      cudaEventDestroy(std::get<1>(p));
+      if (std::get<2>(p)) cudaEventDestroy(std::get<2>(p));
+    }
+    parts.clear();
+  }
+  ~PartTimer() { release(); }
+};
+
 }  // namespace
 
 struct Comm {
@@ -102,6 +152,7 @@ struct Comm {
   ncclComm_t nc = nullptr;
   // local: for rank i, level l, neighbour j: offset of rank i's entries in the neighbour's send buffer
   std::vector<std::vector<int> > src_off[kMaxLevels];
+  PartTimer* timer = nullptr;               // set while a CG call times its parts
 };
 
 namespace {
@@ -149,12 +200,17 @@ int exchange(Comm* C, int l, double* const* x) {
 // over the whole run, then the scalar update `op` (ComputeDotProduct_ref.cpp:70).
 int reduce(Comm* C, int op, double* out = nullptr) {
   Context* c = C->ctx;
+  int id = -1;
+  if (C->timer) HB_TRY(C->timer->start(4, &id));  // the allreduce step (times[4])
   if (C->use_nccl) {
     HB_NCCL(nccl().AllReduce(C->red, C->red + 1, 1, ncclFloat64, op == kFinMax ? ncclMax : ncclSum, C->nc, c->stream),
             "ncclAllReduce");
-    return launch_finalize_ranks(c, C->red + 1, 1, op, out);
+    HB_TRY(launch_finalize_ranks(c, C->red + 1, 1, op, out));
+  } else {
+    HB_TRY(launch_finalize_ranks(c, C->red, C->size, op, out));
   }
-  return launch_finalize_ranks(c, C->red, C->size, op, out);
+  if (C->timer) HB_TRY(C->timer->stop(id));
+  return HPCG_B200_OK;
 }
 
 // Block partials of one rank's reduction (in c->partials) -> red[i].
@@ -217,8 +273,10 @@ double now_s() {
 }
 
 // CG.cpp:59-143 (CG_ref.cpp:58-144) over every rank of the run, the driven
-// ranks' colour-order vectors resident: b -> x.
-int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* normr_out, double* normr0_out) {
+// ranks' colour-order vectors resident: b -> x. times (may be null) receives
+// the parts' device times in slots 1-5 as CG.cpp:132-139 files them.
+int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* normr_out, double* normr0_out,
+             double* times) {
   Context* c = C->ctx;
   const int nl = (int)C->ranks.size();
   std::vector<double*> xs(nl), ps(nl), rs(nl), zs(nl);
@@ -228,6 +286,14 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
     rs[i] = C->ranks[i]->r;
     zs[i] = C->ranks[i]->z;
   }
+  PartTimer timer;
+  if (times) timer.c = c;
+  C->timer = times ? &timer : nullptr;
+  struct Detach {  // the timer lives on this frame only
+    Comm* C;
+    ~Detach() { C->timer = nullptr; }
+  } detach{C};
+  int part = -1;
   // p = x; Ap = A p; r = b - Ap; normr = sqrt(r'r)   (CG.cpp:86-90)
   HB_TRY(exchange(C, 0, xs.data()));
   for (int i = 0; i < nl; ++i) {
@@ -242,6 +308,7 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
   *niters = 0;
   const bool fused = prec && rtz_from_smoother(C->ranks[0]);
   for (int k = 1; k <= max_iter && normr / normr0 > tol; ++k) {
+    HB_TRY(timer.start(5, &part));  // preconditioner (:101-106)
     if (prec) {
       HB_TRY(mg_ranks(C, 0, rs.data(), zs.data(), fused));  // CG.cpp:103
     } else {
@@ -249,11 +316,15 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
         HB_CK(cudaMemcpyAsync(zs[i], rs[i], sizeof(double) * C->ranks[i]->lev[0].n, cudaMemcpyDeviceToDevice,
                               c->stream));
     }
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(1, &part));  // rtz = r'z (:110 / :113)
     if (!fused) {
-      for (int i = 0; i < nl; ++i)  // rtz = r'z   (:110 / :113)
+      for (int i = 0; i < nl; ++i)
         HB_TRY(store_partial(C, i, launch_dot(c, C->ranks[i]->lev[0].n, rs[i], zs[i])));
     }
     HB_TRY(reduce(C, k == 1 ? kFinRtzFirst : kFinRtz));
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(2, &part));  // p = z or p = z + beta p (:109 / :115)
     for (int i = 0; i < nl; ++i) {
       const int n = C->ranks[i]->lev[0].n;
       if (k == 1) {
@@ -262,24 +333,34 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
         HB_TRY(launch_update_p(c, n, zs[i], ps[i]));  // :115
       }
     }
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(3, &part));  // Ap = A p with its halo exchange (:118)
     HB_TRY(exchange(C, 0, ps.data()));  // ComputeSPMV_ref.cpp:53
     for (int i = 0; i < nl; ++i) {
       hpcg_b200_problem* P = C->ranks[i];
       const int parts = spmv_level(P, 0, P->p, P->Ap, true);  // Ap = A p, p'Ap partials (:118-119)
       HB_TRY(store_partial(C, i, parts));
     }
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(1, &part));  // pAp (:119)
     HB_TRY(reduce(C, kFinPap));  // alpha = rtz / pAp (:120)
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(2, &part));  // x and r updates (:121-123), r'r partials with them
     for (int i = 0; i < nl; ++i) {
       hpcg_b200_problem* P = C->ranks[i];
       HB_TRY(store_partial(C, i, launch_update_xr(c, P->lev[0].n, P->x, P->p, P->r, P->Ap)));  // :121-123
     }
+    HB_TRY(timer.stop(part));
+    HB_TRY(timer.start(1, &part));  // normr = sqrt(r'r) (:124)
     HB_TRY(reduce(C, kFinNormr));
+    HB_TRY(timer.stop(part));
     HB_TRY(read_scal(c));
     normr = std::sqrt(c->scal_host->normr2);
     *niters = k;
   }
   *normr_out = normr;
   *normr0_out = normr0;
+  if (times) HB_TRY(timer.add_to(times));
   return HPCG_B200_OK;
 }
 
@@ -530,7 +611,7 @@ int hpcg_b200_shard_cg(hpcg_b200_comm* comm, const double* const* b, double* con
     HB_TRY(load(C, i, 0, b[i], C->ranks[i]->b));
     HB_TRY(load(C, i, 0, x[i], C->ranks[i]->x));
   }
-  HB_TRY(cg_ranks(C, max_iter, tolerance, do_preconditioning != 0, niters, normr, normr0));
+  HB_TRY(cg_ranks(C, max_iter, tolerance, do_preconditioning != 0, niters, normr, normr0, times));
   for (int i = 0; i < (int)C->ranks.size(); ++i) HB_TRY(store_vector(C->ranks[i], 0, C->ranks[i]->x, x[i]));
   if (times) times[0] += now_s() - t0;
   return HPCG_B200_OK;

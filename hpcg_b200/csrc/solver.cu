@@ -1,9 +1,12 @@
 // Entry points of the PCG path: SpMV, SYMGS, the V-cycle, CG and the vector
 // routines, with the host-side drivers that sequence the kernels.
+#include <atomic>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <new>
+#include <thread>
 #include <vector>
 
 #include <algorithm>
@@ -52,13 +55,13 @@ void gs_tile_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* 
 }
 
 // The bulk-copy pipeline (configuration 10): one block per SM (its shared
-// memory allows no second), at most one per tile; PACK: the level's packed
-// columns. false: not launched (FP64 tensor maps unavailable).
-template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT, bool PACK>
+// memory allows no second), at most one per tile; PW: the level's column form
+// (L.pack). false: not launched (FP64 tensor maps unavailable, or refused).
+template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT, int PW>
 bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1,
                       uint32_t mask, double* dot) {
-  auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT, PACK>;
-  using Shape = GsShape<T, PACK>;
+  auto k = k_gs_bulk<T, TR, FIRST, CMASK, DOT, PW>;
+  using Shape = GsShape<T, PW>;
   constexpr int smem = Shape::smem;
   static CUtensorMap none;  // the FP32 kernels take no maps
   const CUtensorMap* tv = &none;
@@ -114,8 +117,9 @@ bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T
 template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
 bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                     double* dot) {
-  if (L.colp) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, true>(c, L, val, rhs, x, r0, r1, mask, dot);
-  return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, false>(c, L, val, rhs, x, r0, r1, mask, dot);
+  if (L.pack == 1) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 1>(c, L, val, rhs, x, r0, r1, mask, dot);
+  if (L.pack == 2) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 2>(c, L, val, rhs, x, r0, r1, mask, dot);
+  return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 0>(c, L, val, rhs, x, r0, r1, mask, dot);
 }
 
 // dot != nullptr: the phase also writes its r'z block partials there (FP64
@@ -262,11 +266,11 @@ inline bool bulk_slab_ok(const Level& L) {
   return true;
 }
 
-template <typename T, bool DOT, int ORDER, bool PACK>
+template <typename T, bool DOT, int ORDER, int PW>
 int spmv_bulk_launch(Context* c, const Level& L, const T* val, const T* x, T* y, double* partials,
                      const BulkMaps* m) {
-  auto k = k_spmv_bulk<T, DOT, ORDER, PACK>;
-  using Shape = SpmvShape<T, PACK>;
+  auto k = k_spmv_bulk<T, DOT, ORDER, PW>;
+  using Shape = SpmvShape<T, PW>;
   constexpr int smem = Shape::smem;
   static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
   bulk_attr(k, smem, c->device, &attr_set);
@@ -297,11 +301,15 @@ int spmv_bulk(Context* c, const Level& L, const T* val, const T* x, T* y, double
     const BulkMaps* m = bulk_maps(L);
     if (!m) return 0;
     if (L.mv_order == 2 && bulk_slab_ok(L)) {
-      if (packed_slab_ok(L)) return spmv_bulk_launch<T, DOT, 2, true>(c, L, val, x, y, partials, m);
-      return spmv_bulk_launch<T, DOT, 2, false>(c, L, val, x, y, partials, m);
+      if (packed_slab_ok(L)) {
+        if (L.pack == 1) return spmv_bulk_launch<T, DOT, 2, 1>(c, L, val, x, y, partials, m);
+        return spmv_bulk_launch<T, DOT, 2, 2>(c, L, val, x, y, partials, m);
+      }
+      return spmv_bulk_launch<T, DOT, 2, 0>(c, L, val, x, y, partials, m);
     }
-    if (L.colp) return spmv_bulk_launch<T, DOT, 0, true>(c, L, val, x, y, partials, m);
-    return spmv_bulk_launch<T, DOT, 0, false>(c, L, val, x, y, partials, m);
+    if (L.pack == 1) return spmv_bulk_launch<T, DOT, 0, 1>(c, L, val, x, y, partials, m);
+    if (L.pack == 2) return spmv_bulk_launch<T, DOT, 0, 2>(c, L, val, x, y, partials, m);
+    return spmv_bulk_launch<T, DOT, 0, 0>(c, L, val, x, y, partials, m);
   }
 }
 
@@ -331,7 +339,7 @@ void restrict_launch(Context* c, const Level& L, const T* val, const T* rf, cons
 
 // The restriction on the bulk-copy pipeline (SpMV configuration 7, injected rows
 // in one run); false if it cannot run here.
-template <typename T, bool PACK>
+template <typename T, int PW>
 bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   static CUtensorMap none;  // the FP32 copy takes no maps
   const CUtensorMap* tv = &none;
@@ -342,8 +350,8 @@ bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, cons
     tv = &m->val;
     tc = &m->col;
   }
-  auto k = k_restrict_bulk<T, PACK>;
-  using Shape = SpmvShape<T, PACK>;
+  auto k = k_restrict_bulk<T, PW>;
+  using Shape = SpmvShape<T, PW>;
   constexpr int smem = Shape::smem;
   static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
   bulk_attr(k, smem, c->device, &attr_set);
@@ -357,8 +365,9 @@ bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, cons
 template <typename T>
 bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   if (L.tf_run < 0 || nc <= 0) return false;
-  if (L.colp) return restrict_bulk_p<T, true>(c, L, val, rf, xf, rc, nc);
-  return restrict_bulk_p<T, false>(c, L, val, rf, xf, rc, nc);
+  if (L.pack == 1) return restrict_bulk_p<T, 1>(c, L, val, rf, xf, rc, nc);
+  if (L.pack == 2) return restrict_bulk_p<T, 2>(c, L, val, rf, xf, rc, nc);
+  return restrict_bulk_p<T, 0>(c, L, val, rf, xf, rc, nc);
 }
 
 template <typename T>
@@ -382,7 +391,9 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
                                     : (first ? kProfGsFirst : kProfGsFull);
   cudaEvent_t ev0 = nullptr;
   HB_TRY(prof_begin(c, kind, &ev0));
-  const int cfg = sizeof(T) == 4 ? (first ? L.gs_first32 : L.gs_sched32) : first ? L.gs_first : L.gs_sched;
+  const int at = first ? (sizeof(T) == 4 ? L.gs_first32_at[s] : L.gs_first_at[s]) : -1;
+  const int cfg = at >= 0 ? at
+                  : sizeof(T) == 4 ? (first ? L.gs_first32 : L.gs_sched32) : first ? L.gs_first : L.gs_sched;
   if (first)
     gs_first_dispatch<T, TR>(c, L, cfg, val, rhs, x, r0, r1, s, first_mask(L.g, s));
   else
@@ -546,6 +557,30 @@ bool level_config_override(int l, int v[6]) {
   return true;
 }
 
+// The first-sweep choice from per-position timings t[s][cfg]: the fastest
+// configuration at each sweep position into at[s] (-1 for an empty colour),
+// and into *one the configuration with the least time summed over the sweep
+// (reported by hpcg_b200_level_config, and used where a position has none).
+void pick_first(const float (&t)[kColours][kGsConfigs], int (&at)[kColours], int* one) {
+  double sum[kGsConfigs] = {};
+  for (int s = 0; s < kColours; ++s) {
+    at[s] = -1;
+    float best = 1e30f;
+    for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
+      if (t[s][cfg] >= 1e30f) continue;
+      sum[cfg] += t[s][cfg];
+      if (t[s][cfg] < best) {
+        best = t[s][cfg];
+        at[s] = cfg;
+      }
+    }
+  }
+  int b = *one;
+  for (int cfg = 0; cfg < kGsConfigs; ++cfg)
+    if (sum[cfg] > 0.0 && (sum[b] <= 0.0 || sum[cfg] < sum[b])) b = cfg;
+  *one = b;
+}
+
 int autotune(hpcg_b200_problem* P) {
   Context* c = P->ctx;
   const char* force = std::getenv("HPCG_B200_CONFIG");
@@ -578,9 +613,10 @@ int autotune(hpcg_b200_problem* P) {
     // Repetitions run round-robin over the configurations, so that a drift of
     // the clocks during tuning (the power cap settling) biases none of them.
     const int kOrders = 3;  // SpMV row orders: storage, natural, slab
-    float t_gs[kGsConfigs], t_first[kGsConfigs], t_mv[kConfigs][kOrders];
+    float t_gs[kGsConfigs], t_first[kColours][kGsConfigs], t_mv[kConfigs][kOrders];
     for (int k = 0; k < kGsConfigs; ++k) {
-      t_gs[k] = t_first[k] = 1e30f;
+      t_gs[k] = 1e30f;
+      for (int s = 0; s < kColours; ++s) t_first[s][k] = 1e30f;
       if (k < kConfigs)
         for (int v = 0; v < kOrders; ++v) t_mv[k][v] = 1e30f;
     }
@@ -600,11 +636,14 @@ int autotune(hpcg_b200_problem* P) {
         HB_TRY(time_it(t_gs[sched], [&] {
           gs_dispatch<double, double, false>(c, L, sched, L.val, rs, xs, r0, r1, kAllSlots);
         }));
-        // the first-sweep phase of a middle sweep position (about half its slots)
-        HB_TRY(time_it(t_first[sched], [&] {
-          gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, L.g.start[4], L.g.start[5], 4,
-                                            first_mask(L.g, 4));
-        }));
+        // the first-sweep phase of every sweep position (0 to 26 slots)
+        for (int s = 0; s < kColours; ++s) {
+          if (L.g.start[s + 1] <= L.g.start[s]) continue;
+          HB_TRY(time_it(t_first[s][sched], [&] {
+            gs_first_dispatch<double, double>(c, L, sched, L.val, rs, xs, L.g.start[s], L.g.start[s + 1], s,
+                                              first_mask(L.g, s));
+          }));
+        }
         for (int v = 0; v < kOrders && sched < kConfigs; ++v) {
           if (sched == kBulkMvCfg && v == 1) continue;  // the bulk SpMV has no natural order
           L.mv_sched = sched;
@@ -616,13 +655,13 @@ int autotune(hpcg_b200_problem* P) {
     }
     L.mv_sched = keep_sched;
     L.mv_order = keep_order;
-    float best_gs = 1e30f, best_mv = 1e30f, best_first = 1e30f;
+    float best_gs = 1e30f, best_mv = 1e30f;
     for (int sched = 0; sched < kGsConfigs; ++sched) {
       if (t_gs[sched] < best_gs) { best_gs = t_gs[sched]; L.gs_sched = sched; }
-      if (t_first[sched] < best_first) { best_first = t_first[sched]; L.gs_first = sched; }
       for (int v = 0; v < kOrders && sched < kConfigs; ++v)
         if (t_mv[sched][v] < best_mv) { best_mv = t_mv[sched][v]; L.mv_sched = sched; L.mv_order = v; }
     }
+    pick_first(t_first, L.gs_first_at, &L.gs_first);
     const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
     if (fo && *fo) L.mv_order = std::atoi(fo);
     cudaEventDestroy(e0);
@@ -986,8 +1025,11 @@ int ensure_f32(hpcg_b200_problem* P) {
       cudaEvent_t e0, e1;
       HB_CK(cudaEventCreate(&e0));
       HB_CK(cudaEventCreate(&e1));
-      float t[kGsConfigs], tf[kGsConfigs];
-      for (int cfg = 0; cfg < kGsConfigs; ++cfg) t[cfg] = tf[cfg] = 1e30f;
+      float t[kGsConfigs], tf[kColours][kGsConfigs];
+      for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
+        t[cfg] = 1e30f;
+        for (int s = 0; s < kColours; ++s) tf[s][cfg] = 1e30f;
+      }
       auto time_it = [&](float& best_ms, auto&& launch) -> int {
         HB_CK(cudaEventRecord(e0, c->stream));
         launch();
@@ -1003,24 +1045,24 @@ int ensure_f32(hpcg_b200_problem* P) {
           HB_TRY(time_it(t[cfg], [&] {
             gs_dispatch<float, float, false>(c, L, cfg, L.val32, L.r32, L.x32, r0, r1, kAllSlots);
           }));
-          // the first-sweep phase of a middle sweep position, as in autotune
-          HB_TRY(time_it(tf[cfg], [&] {
-            gs_first_dispatch<float, float>(c, L, cfg, L.val32, L.r32, L.x32, L.g.start[4], L.g.start[5], 4,
-                                            first_mask(L.g, 4));
-          }));
+          // the first-sweep phase of every sweep position, as in autotune
+          for (int s = 0; s < kColours; ++s) {
+            if (L.g.start[s + 1] <= L.g.start[s]) continue;
+            HB_TRY(time_it(tf[s][cfg], [&] {
+              gs_first_dispatch<float, float>(c, L, cfg, L.val32, L.r32, L.x32, L.g.start[s], L.g.start[s + 1], s,
+                                              first_mask(L.g, s));
+            }));
+          }
         }
       }
-      float best = 1e30f, best_first = 1e30f;
+      float best = 1e30f;
       for (int cfg = 0; cfg < kGsConfigs; ++cfg) {
         if (t[cfg] < best) {
           best = t[cfg];
           L.gs_sched32 = cfg;
         }
-        if (tf[cfg] < best_first) {
-          best_first = tf[cfg];
-          L.gs_first32 = cfg;
-        }
       }
+      pick_first(tf, L.gs_first32_at, &L.gs_first32);
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       HB_CK(cudaGetLastError());
@@ -1200,6 +1242,7 @@ int launch_finalize_ranks(Context* c, const double* vals, int nvals, int op, dou
 int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst) {
   const Level& L = p->lev[level];
   Context* c = p->ctx;
+  if (dst == p->b) p->b_kept = false;  // b no longer holds hpcg_b200_cg's kept right-hand side
   const double* s = src;
   bool dev = false;
   HB_TRY(locate_ptr(src, p->device, &dev, "input vector"));
@@ -1229,6 +1272,96 @@ int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst
   if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * L.n, cudaMemcpyDeviceToHost, c->stream));
   HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
+}
+
+// ---- hpcg_b200_cg's host inputs ------------------------------------------------
+// The reference's timed loop zeroes x on the host and calls CG with the same b
+// for every set (src/main.cpp:334-340). For host vectors hpcg_b200_cg therefore
+// sends b only when it differs from the b it sent last (an exact comparison,
+// bit for bit, against a host copy kept with the problem), and zeroes x on the
+// device when the host x is all zero bits, instead of sending it. Both checks
+// read host memory on several threads, which outruns a copy from pageable
+// memory. HPCG_B200_HOST_REUSE=0 sends both every call.
+
+bool host_reuse_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HPCG_B200_HOST_REUSE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// body(begin, end) over [0, n) on up to 16 host threads (one below 1 Mi entries)
+template <typename F>
+void host_parallel(int64_t n, F&& body) {
+  unsigned t = std::thread::hardware_concurrency();
+  t = t == 0 ? 1 : std::min(t, 16u);
+  if (n < (1 << 20) || t == 1) {
+    body((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const int64_t chunk = (n + t - 1) / t;
+  for (unsigned i = 1; i < t; ++i) {
+    const int64_t b = (int64_t)i * chunk, e = std::min<int64_t>(n, b + chunk);
+    if (b < e) pool.emplace_back([&body, b, e] { body(b, e); });
+  }
+  body((int64_t)0, std::min<int64_t>(n, chunk));
+  for (auto& th : pool) th.join();
+}
+
+bool host_same_bits(const double* a, const double* b, int64_t n) {
+  std::atomic<bool> same{true};
+  host_parallel(n, [&](int64_t lo, int64_t hi) {
+    constexpr int64_t kStep = 1 << 16;  // entries compared between looks at the others' verdict
+    for (int64_t i = lo; i < hi && same.load(std::memory_order_relaxed); i += kStep) {
+      const int64_t m = std::min(kStep, hi - i);
+      if (std::memcmp(a + i, b + i, sizeof(double) * (size_t)m) != 0) same.store(false, std::memory_order_relaxed);
+    }
+  });
+  return same.load();
+}
+
+bool host_all_zero_bits(const double* a, int64_t n) {
+  std::atomic<bool> zero{true};
+  host_parallel(n, [&](int64_t lo, int64_t hi) {
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
+    constexpr int64_t kStep = 1 << 16;
+    for (int64_t i = lo; i < hi && zero.load(std::memory_order_relaxed); i += kStep) {
+      const int64_t e = std::min(hi, i + kStep);
+      uint64_t acc = 0;
+      for (int64_t j = i; j < e; ++j) acc |= w[j];
+      if (acc) zero.store(false, std::memory_order_relaxed);
+    }
+  });
+  return zero.load();
+}
+
+int load_cg_rhs(hpcg_b200_problem* p, const double* b) {
+  bool dev = false;
+  HB_TRY(locate_ptr(b, p->device, &dev, "b"));
+  const int n = p->lev[0].n;
+  if (dev || !host_reuse_enabled()) return load_vector(p, 0, b, p->b);
+  if (p->b_kept && host_same_bits(p->b_kept_host, b, n)) return HPCG_B200_OK;
+  if (!p->b_kept_host) p->b_kept_host = new (std::nothrow) double[n];  // no host memory: send every call
+  if (p->b_kept_host)
+    host_parallel(n, [&](int64_t lo, int64_t hi) {
+      std::memcpy(p->b_kept_host + lo, b + lo, sizeof(double) * (size_t)(hi - lo));
+    });
+  HB_TRY(load_vector(p, 0, b, p->b));  // a copy from pageable memory has read b when it returns
+  p->b_kept = p->b_kept_host != nullptr;
+  return HPCG_B200_OK;
+}
+
+int load_cg_guess(hpcg_b200_problem* p, const double* x) {
+  bool dev = false;
+  HB_TRY(locate_ptr(x, p->device, &dev, "x"));
+  const Level& L = p->lev[0];
+  if (!dev && host_reuse_enabled() && host_all_zero_bits(x, L.n)) {
+    HB_CK(cudaMemsetAsync(p->x, 0, sizeof(double) * L.pitch, p->ctx->stream));
+    return HPCG_B200_OK;
+  }
+  return load_vector(p, 0, x, p->x);
 }
 
 }  // namespace hb
@@ -1299,8 +1432,8 @@ int hpcg_b200_cg(hpcg_b200_problem* p, const double* b, double* x, int max_iter,
   if (is_rank(p)) return HPCG_B200_ERR_UNSUPPORTED;  // a rank: use the hpcg_b200_shard_* routines
   if (!b || !x || !niters || !normr || !normr0 || max_iter < 0) return HPCG_B200_ERR_ARG;
   Setter dev(p->device);
-  HB_TRY(load_vector(p, 0, b, p->b));
-  HB_TRY(load_vector(p, 0, x, p->x));
+  HB_TRY(load_cg_rhs(p, b));
+  HB_TRY(load_cg_guess(p, x));
   HB_TRY(run_cg(p, max_iter, tolerance, do_preconditioning != 0, niters, normr, normr0, times));
   return store_vector(p, 0, p->x, x);
 }

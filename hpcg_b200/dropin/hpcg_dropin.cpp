@@ -14,7 +14,9 @@
 // and TestCG rewrites the fine diagonal in place (src/TestCG.cpp:79, :114). So
 // every call takes its vectors from the host arrays, and the calls that use
 // the fine matrix first compare its diagonal with the copy last sent to the
-// device and resend it if the host changed it.
+// device and resend it if the host changed it. CG's b and x go through
+// hpcg_b200_cg, which sends b only when it changed since its last call and
+// zeroes an all-zero x on the device instead of sending it.
 //
 // MPI builds (HPCG_NO_MPI undefined) with more than one rank: each rank's block
 // and halo plan are generated on its GPU (hpcg_b200_generate_rank, the same
@@ -44,6 +46,7 @@
 #include "Vector.hpp"
 #include "hpcg.hpp"
 #include "hpcg_b200.h"
+#include "mytimer.hpp"
 
 namespace {
 
@@ -236,17 +239,26 @@ int CG(const SparseMatrix& A, CGData& data, const Vector& b, Vector& x, const in
        const double tolerance, int& niters, double& normr, double& normr0, double* times,
        bool doPreconditioning) {
   (void)data;  // the iteration vectors live on the device
+  // times[0] covers the whole call, as src/CG.cpp:63 and :140 measure it (the
+  // vectors' way to and from the device included); the library files the
+  // parts' device times into times[1..5]
+  const double t_begin = mytimer();
   DropinState* st = state_of(A);
   if (!st) return HPCG_B200_ERR_HANDLE;
   if (!doPreconditioning && A.geom->rank == 0)
     HPCG_fout << "WARNING: PERFORMING UNPRECONDITIONED ITERATIONS" << std::endl;  // as src/CG.cpp:75
+  double parts[6] = {0, 0, 0, 0, 0, 0};
   int s = sync_diagonal(A, st);
   if (!s && st->comm)
     s = hpcg_b200_shard_cg(st->comm, &b.values, &x.values, max_iter, tolerance, doPreconditioning ? 1 : 0,
-                           &niters, &normr, &normr0, times);
+                           &niters, &normr, &normr0, times ? parts : 0);
   else if (!s)
     s = hpcg_b200_cg(st->problem, b.values, x.values, max_iter, tolerance, doPreconditioning ? 1 : 0, &niters,
-                     &normr, &normr0, times);
+                     &normr, &normr0, times ? parts : 0);
   if (s) log_error("CG", s);
+  if (times) {
+    for (int i = 1; i < 6; ++i) times[i] += parts[i];
+    times[0] += mytimer() - t_begin;
+  }
   return s;
 }

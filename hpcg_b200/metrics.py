@@ -89,16 +89,16 @@ def compulsory_bytes(nx, ny, nz, nlevels=4, vb=8):
     return b
 
 
-# Column-index bytes per row: 27 int32 columns, or the packed index (one record
-# per 128-row tile: 27 int32 bases + a padding word + 27 x 128 uint16 offsets).
-PACKED_INDEX_BYTES_PER_ROW = (28 * 4 + SLOTS * 128 * 2) / 128.0
+def index_bytes_per_row(pack=0):
+    """Column-index bytes per row: 27 int32 columns (pack 0), or the packed
+    index with offsets of `pack` bytes (one record per 128-row tile: 27 int32
+    bases, the width word, 27 x 128 offsets): 27.875 B (pack 1), 54.875 B (2)."""
+    if pack:
+        return (28 * 4 + SLOTS * 128 * pack) / 128.0
+    return SLOTS * 4
 
 
-def index_bytes_per_row(packed=False):
-    return PACKED_INDEX_BYTES_PER_ROW if packed else SLOTS * 4
-
-
-def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8, packed=False):
+def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8, pack=0):
     """Algorithmic bytes of Gauss-Seidel colour phases that together updated
     `rows_in_phase` rows of a level with `rows_in_level` rows, per phase:
     27 ELL slots (value + column index: int32, or the packed index) and the
@@ -106,14 +106,14 @@ def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8, packed=False):
     seven other colours read once (each row of a colour neighbours all of them).
     For rows_in_phase = R summed over launches of one colour each, the
     other-colour reads are 7 R vb (the colours hold an eighth of the rows each)."""
-    per_row = SLOTS * vb + index_bytes_per_row(packed) + 2 * vb
+    per_row = SLOTS * vb + index_bytes_per_row(pack) + 2 * vb
     return rows_in_phase * per_row + 7.0 * rows_in_phase * vb
 
 
-def spmv_bytes(rows, vb=8, packed=False):
+def spmv_bytes(rows, vb=8, pack=0):
     """Algorithmic bytes of y = A x over `rows` rows: 27 values and column
     indices, x read once, y written."""
-    return rows * (SLOTS * vb + index_bytes_per_row(packed) + 2 * vb)
+    return rows * (SLOTS * vb + index_bytes_per_row(pack) + 2 * vb)
 
 
 def first_sweep_bytes(rows, vb=8):
@@ -125,3 +125,50 @@ def first_sweep_bytes(rows, vb=8):
     swept colours' x (28 colour-eighths over 8 phases = 3.5 entries per row)."""
     return rows * (13 * (vb + 4) + vb + 2 * vb + 3.5 * vb)
 
+
+
+def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False):
+    """Algorithmic HBM bytes of one CG iteration as this library runs it, kernel
+    by kernel (the floor its kernels move when each streams its data once):
+
+    per level l with N_l rows, full-phase row bytes F_l = 36 vb + I_l (27
+    values, the column index I_l = index_bytes_per_row(pack[l]), right-hand
+    side, x written, the other seven colours' x), vb the V-cycle's value bytes
+    (8 in the FP64 form, 4 in the FP32 V-cycle):
+
+    * pre-smoother: the first forward sweep from x = 0 (first_sweep_bytes,
+      13 slots with int32 columns on average) and the backward sweep's 7
+      phases, 7/8 N_l F_l (the colour at the turn is not recomputed);
+    * residual + restriction (levels above the coarsest): N_l/8 coarse rows of
+      27 vb + I_l + 2 vb + 4 (rf read, rc written, the coarse row's index) and
+      the fine x read once, N_l vb;
+    * prolongation: N_l/8 (8 + 3 vb) (pair indices, xc read, xf read and written);
+    * post-smoother: 15 phases, 15/8 N_l F_l;
+    * coarsest level: one symmetric sweep (first sweep + 7 phases);
+    * top level, always FP64: the CG SpMV fused with p'Ap (spmv_bytes with
+      level 0's index) and the vector kernels: 80 B/row in the FP64 form
+      (r'z pass 16, p and x update 40, r update 24) and 96 B/row around the
+      FP32 V-cycle (z widened with both flexible dots 28, p and x update 40, r
+      update with r narrowed 28).
+
+    With parts=True also returns the per-term split (GB)."""
+    lv = level_sizes(nx, ny, nz, nlevels)
+    split = {}
+    total = 0.0
+    for l, (n_l, _) in enumerate(lv):
+        ib = index_bytes_per_row(pack[l])
+        full = 36.0 * vb + ib
+        b = first_sweep_bytes(n_l, vb) + 7.0 / 8.0 * n_l * full
+        if l < nlevels - 1:
+            b += n_l / 8.0 * (27.0 * vb + ib + 2.0 * vb + 4.0) + n_l * vb
+            b += n_l / 8.0 * (8.0 + 3.0 * vb)
+            b += 15.0 / 8.0 * n_l * full
+        split[f"level{l}"] = b / 1e9
+        total += b
+    n0 = lv[0][0]
+    sp = spmv_bytes(n0, 8, pack[0])
+    vec = (80.0 if vb == 8 else 96.0) * n0
+    split["spmv"] = sp / 1e9
+    split["vectors"] = vec / 1e9
+    total += sp + vec
+    return (total, split) if parts else total

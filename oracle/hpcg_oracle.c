@@ -302,6 +302,12 @@ int ora_mg_f32_skip(const ora_level_f32* L, int nlev, int lev, const float* r, f
 int ora_cg_mixed(const ora_level* L, const ora_level_f32* L32, int nlev, const double* b, double* x,
                  int max_iter, double tolerance, int* niters, double* normr_out, double* normr0_out,
                  double* hist) {
+  return ora_cg_mixed_skip(L, L32, nlev, b, x, max_iter, tolerance, niters, normr_out, normr0_out, hist, NULL);
+}
+
+int ora_cg_mixed_skip(const ora_level* L, const ora_level_f32* L32, int nlev, const double* b, double* x,
+                      int max_iter, double tolerance, int* niters, double* normr_out, double* normr0_out,
+                      double* hist, const int* skip) {
   const ora_level* A = &L[0];
   const int n = A->n;
   double* r = (double*)malloc(sizeof(double) * (size_t)n);
@@ -322,7 +328,7 @@ int ora_cg_mixed(const ora_level* L, const ora_level_f32* L32, int nlev, const d
   *niters = 0;
   for (int k = 1; k <= max_iter && normr / normr0 > tolerance; ++k) {
     for (int i = 0; i < n; ++i) r32[i] = (float)r[i];
-    err = ora_mg_f32(L32, nlev, 0, r32, z32);
+    err = ora_mg_f32_skip(L32, nlev, 0, r32, z32, skip);
     if (err) break;
     for (int i = 0; i < n; ++i) z[i] = (double)z32[i];
     if (k == 1) {

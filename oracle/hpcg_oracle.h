@@ -128,6 +128,11 @@ int ora_mg_f32_skip(const ora_level_f32* levels, int nlev, int lev, const float*
 int ora_cg_mixed(const ora_level* levels, const ora_level_f32* levels32, int nlev, const double* b,
                  double* x, int max_iter, double tolerance, int* niters, double* normr, double* normr0,
                  double* hist);
+/* The same around the FP32 V-cycle of ora_mg_f32_skip (skip: per-level rows not
+ * repeated at the turn of each sweep, NULL for the reference's sweep). */
+int ora_cg_mixed_skip(const ora_level* levels, const ora_level_f32* levels32, int nlev, const double* b,
+                      double* x, int max_iter, double tolerance, int* niters, double* normr, double* normr0,
+                      double* hist, const int* skip);
 
 #ifdef __cplusplus
 }

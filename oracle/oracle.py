@@ -85,6 +85,10 @@ def _load_oracle():
     lib.ora_cg_mixed.argtypes = [C.POINTER(_Level), C.POINTER(_Level32), C.c_int, _f64p, _f64p, C.c_int,
                                  C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                  C.POINTER(C.c_double), _f64p]
+    lib.ora_cg_mixed_skip.restype = C.c_int
+    lib.ora_cg_mixed_skip.argtypes = [C.POINTER(_Level), C.POINTER(_Level32), C.c_int, _f64p, _f64p, C.c_int,
+                                      C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), _f64p, C.c_void_p]
     return lib
 
 
@@ -280,15 +284,18 @@ def mg_f32(l32, r, skip=None):
     return x
 
 
-def cg_mixed(levels, b, x0, max_iter, tolerance):
-    """FP64 flexible PCG around the FP32 V-cycle. Returns (x, niters, normr, normr0, hist)."""
+def cg_mixed(levels, b, x0, max_iter, tolerance, skip=None):
+    """FP64 flexible PCG around the FP32 V-cycle (mg_f32 with `skip`). Returns
+    (x, niters, normr, normr0, hist[0..niters])."""
     l32 = to_f32(levels)
     x = np.array(x0, np.float64, copy=True)
     hist = np.zeros(max_iter + 1)
     ni, nr, nr0 = C.c_int(0), C.c_double(0), C.c_double(0)
-    err = lib().ora_cg_mixed(_levels_c(levels), _levels32_c(l32), len(levels),
-                             np.ascontiguousarray(b, np.float64), x, max_iter, tolerance,
-                             C.byref(ni), C.byref(nr), C.byref(nr0), hist)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.int32)
+    err = lib().ora_cg_mixed_skip(_levels_c(levels), _levels32_c(l32), len(levels),
+                                  np.ascontiguousarray(b, np.float64), x, max_iter, tolerance,
+                                  C.byref(ni), C.byref(nr), C.byref(nr0), hist,
+                                  sk.ctypes.data if sk is not None else None)
     assert err == 0
     return x, ni.value, nr.value, nr0.value, hist[: ni.value + 1].copy()
 

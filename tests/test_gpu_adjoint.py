@@ -4,8 +4,11 @@ torch.autograd shim), on the perturbed symmetric stencil at 16^3:
 * against the FP64 host adjoint built on the oracle's CG_ref restatement
   (relative 1e-8 of the largest component);
 * against central finite differences with step 1e-6 on 64 seeded coordinates
-  (48 value slots, 16 right-hand-side entries): relative 1e-6 per coordinate
-  (components below 1e-3 of the largest are held to 1e-6 of that floor)."""
+  (48 value slots, 16 right-hand-side entries): |fd - adj| <= 1e-6 |adj| per
+  coordinate. The coordinates are drawn from those whose gradient is at least
+  1e-3 of the largest component of its kind: below that the forward and
+  adjoint solves' stopping tolerance (1e-12 relative), not the adjoint, sets
+  the agreement, so those draws are skipped, not held to a looser bound."""
 import numpy as np
 import pytest
 
@@ -62,20 +65,30 @@ def test_adjoint_matches_finite_differences(adj_case):
     A = sparse_from_slots(v, N, N, N).tocsc()
     rng = np.random.default_rng(0x48504347)
     floor_v = 1e-3 * np.abs(c["gv"]).max()
-    slots = 0
+    slots = skipped = 0
     while slots < 48:
         i, k = int(rng.integers(n)), int(rng.integers(27))
         if v[i, k] == 0.0:
             continue
-        fd = central_difference_slot(v, b, xt, i, k, 1e-6, N, N, N)
         adj = c["gv"][i, k]
-        assert abs(fd - adj) <= 1e-6 * max(abs(adj), floor_v), (i, k, fd, adj)
+        if abs(adj) < floor_v:
+            skipped += 1
+            continue
+        fd = central_difference_slot(v, b, xt, i, k, 1e-6, N, N, N)
+        assert abs(fd - adj) <= 1e-6 * abs(adj), (i, k, fd, adj)
         slots += 1
     floor_b = 1e-3 * np.abs(c["gb"]).max()
-    for i in rng.integers(n, size=16):
-        fd = central_difference_rhs(A, b, xt, x, int(i), 1e-6)
+    rhs = 0
+    while rhs < 16:
+        i = int(rng.integers(n))
         adj = c["gb"][i]
-        assert abs(fd - adj) <= 1e-6 * max(abs(adj), floor_b), (i, fd, adj)
+        if abs(adj) < floor_b:
+            skipped += 1
+            continue
+        fd = central_difference_rhs(A, b, xt, x, i, 1e-6)
+        assert abs(fd - adj) <= 1e-6 * abs(adj), (i, fd, adj)
+        rhs += 1
+    assert skipped <= 16  # the floor leaves most coordinates in
 
 
 def test_autograd_shim(binding, adj_case):

@@ -1,17 +1,31 @@
 """The packed column format of the bulk-copy kernels, restated with numpy on the
 host: the level's 27-slot ELL columns in colour order, one record per 128-row
-tile (27 bases, 16-bit offsets, 0xFFFF for the zero sink). The device builds
-the records in problem.cu (k_pack_cols) and decodes them in bulk.cuh
-(stage_col); the GPU tests check that the decoded columns give the same bits as
-the 32-bit ones. Here: the encoding round-trips, the stencil's colour order
-keeps every tile's slot within a few hundred rows, and a matrix whose columns
-scatter does not pack."""
+tile (27 bases, a word holding the offset width w, then 27 x 128 offsets of w
+bytes; the all-ones offset marks the zero sink). w is 1 where every tile's
+columns of each slot span at most 254, else 2 where they span at most 65534,
+else the level is not packed. The device builds the records in problem.cu
+(k_pack_cols) and decodes them in bulk.cuh (stage_col); the GPU tests check
+that the decoded columns give the same bits as the 32-bit ones and that each
+level gets the width predicted here (packed_width). Here: the encoding
+round-trips in both widths, the stencil's colour order keeps every tile's slot
+within one tile of rows where colour blocks fill whole tiles, and a matrix
+whose columns scatter does not pack."""
 import numpy as np
 import pytest
 
 ROWS = 128
-SINK = 0xFFFF
-MAX_SPAN = 0xFFFE
+
+
+def sink_code(w):
+    return 0xFF if w == 1 else 0xFFFF
+
+
+def max_span(w):
+    return 0xFE if w == 1 else 0xFFFE
+
+
+def rec_bytes(w):
+    return 28 * 4 + 27 * ROWS * w
 
 
 def colour_ell(binding, nx, ny, nz):
@@ -36,7 +50,7 @@ def colour_ell(binding, nx, ny, nz):
     return cols, n, pitch
 
 
-def pack(cols, n, pitch, sink):
+def pack(cols, n, pitch, sink, w=2):
     """(bases [tiles][27], offsets [tiles][27][128], packs, max span)."""
     t = pitch // ROWS
     c = np.where(np.arange(pitch) < n, cols, sink).reshape(27, t, ROWS).transpose(1, 0, 2)
@@ -46,29 +60,53 @@ def pack(cols, n, pitch, sink):
     hi = np.where(real, c, np.iinfo(np.int64).min).max(axis=2)
     span = np.where(any_real, hi - lo, 0)
     base = np.where(any_real, lo, 0)
-    off = np.where(real, c - base[:, :, None], SINK)
-    packs = bool((span <= MAX_SPAN).all())
-    return base.astype(np.int32), off.astype(np.uint16), packs, int(span.max())
+    packs = bool((span <= max_span(w)).all())
+    off = np.where(real, c - base[:, :, None], sink_code(w))
+    if packs:
+        off = off.astype(np.uint8 if w == 1 else np.uint16)
+    return base.astype(np.int32), off, packs, int(span.max())
 
 
-def unpack(base, off, sink):
-    c = np.where(off == SINK, sink, base[:, :, None].astype(np.int64) + off)
+def unpack(base, off, sink, w=2):
+    c = np.where(off == sink_code(w), sink, base[:, :, None].astype(np.int64) + off)
     return c.transpose(1, 0, 2).reshape(27, -1)
 
 
+def packed_width(binding, nx, ny, nz):
+    """The offset width the library gives a single-rank level of this grid:
+    1, 2, or 0 (not packed)."""
+    cols, n, pitch = colour_ell(binding, nx, ny, nz)
+    for w in (1, 2):
+        if pack(cols, n, pitch, n, w)[2]:
+            return w
+    return 0
+
+
+@pytest.mark.parametrize("w", [1, 2])
 @pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 40), (64, 64, 64)])
-def test_stencil_columns_pack_and_round_trip(binding, dims):
+def test_stencil_columns_pack_and_round_trip(binding, dims, w):
     cols, n, pitch = colour_ell(binding, *dims)
-    base, off, packs, span = pack(cols, n, pitch, n)
+    base, off, packs, span = pack(cols, n, pitch, n, w)
     assert packs
     # a tile is consecutive rows of one colour, and slot k of each is the
     # matching row of one neighbouring colour: the slot spans the tile's own
-    # 128 rows (the sink aside), whatever the grid
+    # 128 rows (the sink aside), whatever the grid, as long as every colour
+    # block is a whole number of tiles
     assert span == ROWS - 1
-    back = unpack(base, off, n)
+    back = unpack(base, off, n, w)
     assert np.array_equal(back[:, :n], cols[:, :n])
-    # one record per tile: 27 bases + a padding word, 27 x 128 offsets
-    assert base.shape[0] * (28 * 4 + 27 * ROWS * 2) == pitch // ROWS * 7024
+    # one record per tile: 27 bases + the width word, 27 x 128 offsets
+    assert base.shape[0] * rec_bytes(w) == pitch // ROWS * (3568 if w == 1 else 7024)
+
+
+@pytest.mark.parametrize("dims,width", [((24, 24, 24), 2), ((48, 48, 48), 1), ((8, 8, 8), 2),
+                                        ((4, 4, 4), 1), ((12, 12, 12), 2), ((64, 32, 16), 1)])
+def test_width_follows_the_colour_blocks(binding, dims, width):
+    """8-bit offsets hold every level whose colour blocks fill whole 128-row
+    tiles (spans 127) and every level of at most 255 columns; a tile that
+    straddles two colour blocks spans the distance between their neighbour
+    colours, which at 24^3 or 8^3 needs 16 bits."""
+    assert packed_width(binding, *dims) == width
 
 
 def test_scattered_columns_do_not_pack(binding):
@@ -78,6 +116,12 @@ def test_scattered_columns_do_not_pack(binding):
     far = cols.copy()
     far[14, 5] = n - 1
     far[14, 6] = 0
-    assert n - 1 > MAX_SPAN
-    _, _, packs, span = pack(far, n, pitch, n)
-    assert not packs and span == n - 1
+    assert n - 1 > max_span(2)
+    for w in (1, 2):
+        _, _, packs, span = pack(far, n, pitch, n, w)
+        assert not packs and span == n - 1
+    # a jump of 300 rows: too far for 8 bits, near enough for 16
+    near = cols.copy()
+    near[14, 5] = cols[14, 5] + 300
+    assert pack(near, n, pitch, n, 1)[2] is False
+    assert pack(near, n, pitch, n, 2)[2] is True
