@@ -38,6 +38,7 @@ EXPORTS = (
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
     "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
+    "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest",
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
@@ -105,6 +106,8 @@ def lib():
         l.hpcg_b200_batch_problem.argtypes = [vp, i, C.POINTER(vp)]
         l.hpcg_b200_batch_cg_mixed.argtypes = [vp, vp, vp, i, d, vp, vp, vp]
         l.hpcg_b200_batch_free.argtypes = [vp]
+        l.hpcg_b200_batch_form.argtypes = [vp, C.POINTER(i)]
+        l.hpcg_b200_grid_wait_selftest.argtypes = [i, d]
         l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
         l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
@@ -507,6 +510,13 @@ class Batch:
                                               nr.ctypes.data, nr0.ctypes.data), "hpcg_b200_batch_cg_mixed")
         return ni, nr, nr0
 
+    def form(self):
+        """0: one launch per step (register phases), 1: the same with bulk-copy
+        phases, 2: the whole iteration in one cooperative launch."""
+        f = C.c_int(-1)
+        _check(lib().hpcg_b200_batch_form(self._h, C.byref(f)), "hpcg_b200_batch_form")
+        return f.value
+
     def free(self):
         if self._h and self._h.value:
             for p in self.problems:
@@ -545,6 +555,13 @@ def wait_selftest(seconds, device=0):
     """Status of hpcg_b200_wait_selftest: a device-side wait on a barrier that
     nothing completes, given up after `seconds` (ERR_TIMEOUT expected)."""
     return lib().hpcg_b200_wait_selftest(device, float(seconds))
+
+
+def grid_wait_selftest(seconds, device=0):
+    """Status of hpcg_b200_grid_wait_selftest: every block of a cooperative
+    launch waits at a grid barrier for one arrival too many, and gives up after
+    `seconds` (ERR_TIMEOUT expected)."""
+    return lib().hpcg_b200_grid_wait_selftest(device, float(seconds))
 
 
 def ComputeDotProduct(n, x, y):

@@ -84,7 +84,7 @@ struct BCtl {
 
 // ---- kernels -----------------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_gs(const BGs* __restrict__ items, const BTile* __restrict__ tiles,
                                                    int ntiles, const BScal* __restrict__ sc) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile tl = tiles[t];
@@ -98,6 +98,8 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
       gs_row<float, float, false, kPlain, 0>(it.val, it.col, it.pitch, it.rhs, it.x, q, it.mask);
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items, const BTile* __restrict__ tiles,
+                                                   int ntiles, const BScal* __restrict__ sc) { b_gs(items, tiles, ntiles, sc); }
 
 // The batched colour phase through the bulk-copy pipeline (bulk.cuh): every
 // tile is one 128-row block of its problem's blocked FP32 values (val32 of the
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(BatchShape::threads, 1)
 }
 
 // rc = (rf - A xf) at the injected rows (ComputeMG_ref.cpp:49-51, sorted pairs)
-__global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict__ items,
+__device__ __forceinline__ void b_restrict(const BRes* __restrict__ items,
                                                          const BTile* __restrict__ tiles, int ntiles,
                                                          const BScal* __restrict__ sc) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -170,10 +172,13 @@ __global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict_
     it.rc[it.tq[u]] = it.rf[f] - sum;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_restrict(const BRes* __restrict__ items,
+                                                         const BTile* __restrict__ tiles, int ntiles,
+                                                         const BScal* __restrict__ sc) { b_restrict(items, tiles, ntiles, sc); }
 
 // xf[f] += xc[q] (ComputeProlongation_ref.cpp:49); prolongation items carry xc in
 // rf and the fine solution in rc
-__global__ void __launch_bounds__(kThreads) k_b_prolong(const BRes* __restrict__ items,
+__device__ __forceinline__ void b_prolong(const BRes* __restrict__ items,
                                                         const BTile* __restrict__ tiles, int ntiles,
                                                         const BScal* __restrict__ sc) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -185,10 +190,13 @@ __global__ void __launch_bounds__(kThreads) k_b_prolong(const BRes* __restrict__
     it.rc[it.tf[u]] += it.rf[it.tq[u]];
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_prolong(const BRes* __restrict__ items,
+                                                        const BTile* __restrict__ tiles, int ntiles,
+                                                        const BScal* __restrict__ sc) { b_prolong(items, tiles, ntiles, sc); }
 
 // y = A x (FP64 outer SpMV, CG.cpp:118); DOT: partial of x'y per tile
 template <bool DOT>
-__global__ void __launch_bounds__(kThreads) k_b_spmv(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_spmv(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                      int ntiles, int use_p, const BScal* __restrict__ sc,
                                                      double* __restrict__ partials) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -215,9 +223,13 @@ __global__ void __launch_bounds__(kThreads) k_b_spmv(const BVec* __restrict__ v,
     }
   }
 }
+template <bool DOT>
+__global__ void __launch_bounds__(kThreads) k_b_spmv(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                     int ntiles, int use_p, const BScal* __restrict__ sc,
+                                                     double* __restrict__ partials) { b_spmv<DOT>(v, tiles, ntiles, use_p, sc, partials); }
 
 // r = 1.0 b + (-1.0) Ap (CG.cpp:88) and partial of r'r
-__global__ void __launch_bounds__(kThreads) k_b_resid(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_resid(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                       int ntiles, double* __restrict__ partials) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile tl = tiles[t];
@@ -233,9 +245,11 @@ __global__ void __launch_bounds__(kThreads) k_b_resid(const BVec* __restrict__ v
     if (threadIdx.x == 0) partials[t] = s;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_resid(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                      int ntiles, double* __restrict__ partials) { b_resid(v, tiles, ntiles, partials); }
 
 // r32 = (float) r: the FP32 V-cycle's right-hand side
-__global__ void __launch_bounds__(kThreads) k_b_to32(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_to32(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                      int ntiles, const BScal* __restrict__ sc) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BTile tl = tiles[t];
@@ -245,9 +259,11 @@ __global__ void __launch_bounds__(kThreads) k_b_to32(const BVec* __restrict__ v,
     if (q < it.n) it.r32[q] = (float)it.r[q];
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_to32(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                     int ntiles, const BScal* __restrict__ sc) { b_to32(v, tiles, ntiles, sc); }
 
 // z = (double) x32; partials of r'z and r'zprev (flexible beta)
-__global__ void __launch_bounds__(kThreads) k_b_to64_dots(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_to64_dots(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                           int ntiles, const BScal* __restrict__ sc,
                                                           double* __restrict__ partials) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -270,9 +286,12 @@ __global__ void __launch_bounds__(kThreads) k_b_to64_dots(const BVec* __restrict
     }
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_to64_dots(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                          int ntiles, const BScal* __restrict__ sc,
+                                                          double* __restrict__ partials) { b_to64_dots(v, tiles, ntiles, sc, partials); }
 
 // iteration 1: p = z; later: p = z + beta p; then zprev = z
-__global__ void __launch_bounds__(kThreads) k_b_update_p(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_update_p(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                          int ntiles, const BScal* __restrict__ sc,
                                                          const BCtl* __restrict__ ctl) {
   const bool first = ctl->iter == 0;
@@ -289,9 +308,12 @@ __global__ void __launch_bounds__(kThreads) k_b_update_p(const BVec* __restrict_
     }
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_update_p(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                         int ntiles, const BScal* __restrict__ sc,
+                                                         const BCtl* __restrict__ ctl) { b_update_p(v, tiles, ntiles, sc, ctl); }
 
 // x += alpha p, r += (-alpha) Ap (CG.cpp:121-122); partial of r'r
-__global__ void __launch_bounds__(kThreads) k_b_update_xr(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+__device__ __forceinline__ void b_update_xr(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
                                                           int ntiles, const BScal* __restrict__ sc,
                                                           double* __restrict__ partials) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -313,56 +335,194 @@ __global__ void __launch_bounds__(kThreads) k_b_update_xr(const BVec* __restrict
     if (threadIdx.x == 0) partials[t] = s;
   }
 }
+__global__ void __launch_bounds__(kThreads) k_b_update_xr(const BVec* __restrict__ v, const BTile* __restrict__ tiles,
+                                                          int ntiles, const BScal* __restrict__ sc,
+                                                          double* __restrict__ partials) { b_update_xr(v, tiles, ntiles, sc, partials); }
 
 enum BFin : int { kBNorm0 = 0, kBRtz = 1, kBPap = 2, kBNormr = 3 };
 
-// One block per problem: fixed-order sum over the problem's tiles, then its scalar step.
+// Problem p's fixed-order sum over its tiles, then its scalar step; block b
+// takes problems b, b + gridDim.x, ...
+__device__ __forceinline__ void b_finalize(BScal* sc, const double* __restrict__ partials, int ntiles,
+                                           const int* __restrict__ range, int op, const BCtl* __restrict__ ctl,
+                                           int m) {
+  for (int p = blockIdx.x; p < m; p += gridDim.x) {
+    const int t0 = range[p], t1 = range[p + 1];
+    double a1 = 0.0, a2 = 0.0;
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+      a1 += partials[t];
+      if (op == kBRtz) a2 += partials[ntiles + t];
+    }
+    const double s1 = block_sum(a1);
+    const double s2 = op == kBRtz ? block_sum(a2) : 0.0;
+    if (threadIdx.x != 0) continue;
+    BScal& s = sc[p];
+    switch (op) {
+      case kBNorm0:
+        s.normr2 = s1;
+        s.normr0 = sqrt(s1);
+        s.active = s.normr0 / s.normr0 > ctl->tol ? 1 : 0;
+        s.niters = 0;
+        break;
+      case kBRtz:
+        if (!s.active) break;
+        if (ctl->iter == 0) {
+          s.rtz = s1;
+        } else {
+          s.oldrtz = s.rtz;
+          s.rtz = s1;
+          s.rzprev = s2;
+          s.beta = (s1 - s2) / s.oldrtz;  // Polak-Ribiere
+        }
+        break;
+      case kBPap:
+        if (!s.active) break;
+        s.pAp = s1;
+        s.alpha = s.rtz / s1;
+        break;
+      case kBNormr:
+        s.normr2 = s1;
+        if (s.active) {
+          s.niters = ctl->iter + 1;
+          s.active = sqrt(s1) / s.normr0 > ctl->tol ? 1 : 0;
+        }
+        break;
+      default: break;
+    }
+  }
+}
+
+// One block per problem.
 __global__ void __launch_bounds__(kThreads) k_b_finalize(BScal* sc, const double* __restrict__ partials,
                                                          int ntiles, const int* __restrict__ range, int op,
-                                                         const BCtl* __restrict__ ctl) {
-  const int p = blockIdx.x;
-  const int t0 = range[p], t1 = range[p + 1];
-  double a1 = 0.0, a2 = 0.0;
-  for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-    a1 += partials[t];
-    if (op == kBRtz) a2 += partials[ntiles + t];
-  }
-  const double s1 = block_sum(a1);
-  const double s2 = op == kBRtz ? block_sum(a2) : 0.0;
-  if (threadIdx.x != 0) return;
-  BScal& s = sc[p];
-  switch (op) {
-    case kBNorm0:
-      s.normr2 = s1;
-      s.normr0 = sqrt(s1);
-      s.active = s.normr0 / s.normr0 > ctl->tol ? 1 : 0;
-      s.niters = 0;
-      break;
-    case kBRtz:
-      if (!s.active) break;
-      if (ctl->iter == 0) {
-        s.rtz = s1;
-      } else {
-        s.oldrtz = s.rtz;
-        s.rtz = s1;
-        s.rzprev = s2;
-        s.beta = (s1 - s2) / s.oldrtz;  // Polak-Ribiere
+                                                         const BCtl* __restrict__ ctl, int m) {
+  b_finalize(sc, partials, ntiles, range, op, ctl, m);
+}
+
+// ---- the whole iteration in one launch ------------------------------------------
+// A cooperative launch (every block resident at once) walks the iteration's
+// steps, the same work lists as the launches above, in the same order, with a
+// grid barrier wherever a step reads what the step before wrote. So each
+// problem computes the same bits as with one launch per step on the register
+// kernels.
+//
+// The barrier: every block's thread 0 reads the barrier's generation, arrives
+// on its counter, and the last to arrive resets the counter and advances the
+// generation; the others wait for the generation to move. Each wait gives up
+// after kBatchWaitNs of global time: it records fault code 5 in the context's
+// fault word and the block leaves the kernel. A block that left stops arriving,
+// so every other block's next wait runs out too and the launch ends; the
+// loop's condition kernel reads the fault word and ends the loop, and the
+// host's stream synchronisation returns HPCG_B200_ERR_TIMEOUT.
+constexpr unsigned long long kBatchWaitNs = 1000000000ull;  // 1 s per wait
+
+// The barrier's state (device memory): arrivals and generation.
+struct BBar {
+  unsigned count;
+  unsigned gen;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// true once every block of the grid has arrived; false if the wait gave up
+// (the caller leaves the kernel)
+__device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned expected, unsigned* fault,
+                                             unsigned long long limit_ns = kBatchWaitNs) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const unsigned g = ld_acquire_u32(&bar->gen);
+    __threadfence();  // this block's writes are visible before its arrival
+    if (atomicAdd(&bar->count, 1u) + 1u == expected) {
+      bar->count = 0;  // nobody touches the counter until the generation moves
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire_u32(&bar->gen) == g) {
+        if (global_ns() - t0 > limit_ns) {
+          record_fault(fault, 5);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
       }
-      break;
-    case kBPap:
-      if (!s.active) break;
-      s.pAp = s1;
-      s.alpha = s.rtz / s1;
-      break;
-    case kBNormr:
-      s.normr2 = s1;
-      if (s.active) {
-        s.niters = ctl->iter + 1;
-        s.active = sqrt(s1) / s.normr0 > ctl->tol ? 1 : 0;
-      }
-      break;
-    default: break;
+    }
+    __threadfence();
   }
+  __syncthreads();
+  return ok != 0;
+}
+
+// A step of the V-cycle on the device: 0 colour phase, 1 restriction, 2 prolongation.
+struct DStep {
+  int kind, tile_off, ntiles;
+};
+
+struct BIter {
+  const DStep* steps;
+  int nsteps;
+  const BGs* gs_items;
+  const BRes* res_items;
+  const BTile* tiles;
+  const BVec* vec;
+  const BTile* vtiles;
+  int nvt;
+  const int* vrange;
+  double* partials;
+  BScal* sc;
+  const BCtl* ctl;
+  int m;
+  BBar* bar;
+  unsigned* fault;
+  int vcycle_only;  // 1: the V-cycle's steps alone (timing at creation)
+};
+
+// One flexible-CG iteration of every active problem (the launches of
+// iteration() below, in one launch).
+__global__ void __launch_bounds__(kThreads) k_b_iteration(BIter a) {
+  const unsigned nb = gridDim.x;
+  if (*(volatile unsigned*)a.fault) return;  // an earlier launch gave up: do nothing
+  if (!a.vcycle_only) {
+    b_to32(a.vec, a.vtiles, a.nvt, a.sc);
+    if (!grid_barrier(a.bar, nb, a.fault)) return;
+  }
+  for (int i = 0; i < a.nsteps; ++i) {
+    const DStep st = a.steps[i];
+    if (st.kind == 0)
+      b_gs(a.gs_items, a.tiles + st.tile_off, st.ntiles, a.sc);
+    else if (st.kind == 1)
+      b_restrict(a.res_items, a.tiles + st.tile_off, st.ntiles, a.sc);
+    else
+      b_prolong(a.res_items, a.tiles + st.tile_off, st.ntiles, a.sc);
+    if (!grid_barrier(a.bar, nb, a.fault)) return;
+  }
+  if (a.vcycle_only) return;
+  b_to64_dots(a.vec, a.vtiles, a.nvt, a.sc, a.partials);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBRtz, a.ctl, a.m);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_update_p(a.vec, a.vtiles, a.nvt, a.sc, a.ctl);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_spmv<true>(a.vec, a.vtiles, a.nvt, 1, a.sc, a.partials);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBPap, a.ctl, a.m);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_update_xr(a.vec, a.vtiles, a.nvt, a.sc, a.partials);
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
+  b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBNormr, a.ctl, a.m);
+}
+
+// Check of the barrier's bounded wait: every block waits for one more arrival
+// than the grid holds, so every wait runs out; records fault code 5 and returns.
+__global__ void __launch_bounds__(kThreads) k_b_barrier_selftest(BBar* bar, unsigned long long limit_ns,
+                                                                 unsigned* fault) {
+  grid_barrier(bar, gridDim.x + 1, fault, limit_ns);
 }
 
 __global__ void k_b_setup(BCtl* ctl, int max_iter, double tol) {
@@ -373,14 +533,17 @@ __global__ void k_b_setup(BCtl* ctl, int max_iter, double tol) {
   }
 }
 
-// while (iter < max_iter && any problem active)
+// while (iter < max_iter && any problem active), and no bounded wait gave up;
+// resets the persistent iteration's barrier for the next launch
 __global__ void k_b_condition(BCtl* ctl, const BScal* __restrict__ sc, int m, cudaGraphConditionalHandle h,
-                              int advance) {
+                              int advance, BBar* bar, const unsigned* fault) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   if (advance) ctl->iter += 1;
   bool any = false;
   for (int p = 0; p < m; ++p) any = any || sc[p].active;
-  cudaGraphSetConditional(h, any && ctl->iter < ctl->max_iter ? 1u : 0u);
+  bar->count = 0;
+  const bool gave_up = *(volatile const unsigned*)fault != 0;
+  cudaGraphSetConditional(h, any && !gave_up && ctl->iter < ctl->max_iter ? 1u : 0u);
 }
 
 // ---- host ---------------------------------------------------------------------
@@ -410,6 +573,10 @@ struct hpcg_b200_batch {
   hb::BGs* gs_bitems;  // the GS items on the blocked FP32 copies (bulk-copy phases)
   hb::BTile* btiles;   // their 128-row tiles
   bool bulk;           // GS phases on k_b_gs_bulk (chosen by timing at creation)
+  bool persist;        // the whole iteration as one cooperative launch (k_b_iteration), chosen likewise
+  int persist_grid;    // its blocks: as many as the SMs hold at once
+  hb::DStep* dsteps;   // the V-cycle's steps for k_b_iteration
+  hb::BBar* bar;       // its grid barrier
   bool packed;         // every level of every problem has packed columns (k_b_gs_bulk reads them)
   std::vector<hb::Step> steps;
   hb::BVec* vec;
@@ -566,7 +733,7 @@ int launch_step(hpcg_b200_batch* B, const Step& s) {
 }
 
 int finalize_b(hpcg_b200_batch* B, int op) {
-  k_b_finalize<<<B->m, kThreads, 0, B->ctx->stream>>>(B->sc, B->partials, B->nvt, B->vrange, op, B->ctl);
+  k_b_finalize<<<B->m, kThreads, 0, B->ctx->stream>>>(B->sc, B->partials, B->nvt, B->vrange, op, B->ctl, B->m);
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
 }
@@ -590,6 +757,41 @@ int iteration(hpcg_b200_batch* B) {
   return finalize_b(B, kBNormr);
 }
 
+// k_b_iteration as a cooperative launch (vcycle_only: the V-cycle's steps alone)
+int launch_iteration(hpcg_b200_batch* B, bool vcycle_only) {
+  Context* c = B->ctx;
+  if (B->persist_grid < 1) return HPCG_B200_ERR_UNSUPPORTED;
+  BIter a;
+  a.steps = B->dsteps;
+  a.nsteps = (int)B->steps.size();
+  a.gs_items = B->gs_items;
+  a.res_items = B->res_items;
+  a.tiles = B->tiles;
+  a.vec = B->vec;
+  a.vtiles = B->vtiles;
+  a.nvt = B->nvt;
+  a.vrange = B->vrange;
+  a.partials = B->partials;
+  a.sc = B->sc;
+  a.ctl = B->ctl;
+  a.m = B->m;
+  a.bar = B->bar;
+  a.fault = c->fault;
+  a.vcycle_only = vcycle_only ? 1 : 0;
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(B->persist_grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  HB_CK(cudaLaunchKernelEx(&cfg, k_b_iteration, a));
+  return HPCG_B200_OK;
+}
+
 int end_capture_b(cudaStream_t st, int status) {
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(st, &g);
@@ -610,7 +812,7 @@ int build_graph(hpcg_b200_batch* B) {
   if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0,
                                                             cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 0);
+    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 0, B->bar, c->fault);
     e = cudaGetLastError();
     st = end_capture_b(c->stream, e == cudaSuccess ? HPCG_B200_OK : status_of(e));
   }
@@ -635,9 +837,9 @@ int build_graph(hpcg_b200_batch* B) {
     if (e != cudaSuccess) set_error("batch graph", e);
     return st != HPCG_B200_OK ? st : status_of(e);
   }
-  st = iteration(B);
+  st = B->persist ? launch_iteration(B, false) : iteration(B);
   if (st == HPCG_B200_OK) {
-    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 1);
+    k_b_condition<<<1, 32, 0, c->stream>>>(B->ctl, B->sc, B->m, h, 1, B->bar, c->fault);
     if (cudaGetLastError() != cudaSuccess) st = HPCG_B200_ERR_CUDA;
   }
   st = end_capture_b(c->stream, st);
@@ -652,18 +854,25 @@ int build_graph(hpcg_b200_batch* B) {
   return st;
 }
 
-// GS phases on the bulk-copy kernel or on k_b_gs: the faster V-cycle (all
-// problems active, three rounds each way, round-robin), or HPCG_B200_BATCH_BULK.
+// The form of an iteration: one launch per step with the colour phases on the
+// register kernel (k_b_gs) or on the bulk-copy kernel (k_b_gs_bulk, every
+// level packed), or the whole iteration as one cooperative launch
+// (k_b_iteration, register phases). The fastest V-cycle (all problems active,
+// three rounds each way, round-robin), or HPCG_B200_BATCH_PERSIST (1: one
+// launch) / HPCG_B200_BATCH_BULK (one launch per step; 1: bulk-copy phases).
 // Every V-cycle starts its sweeps from the right-hand side alone, so the work
 // vectors it leaves behind are rewritten by the next solve.
-int choose_bulk(hpcg_b200_batch* B) {
-  if (!B->packed) {  // a level without packed columns: the register kernel
-    B->bulk = false;
+int choose_form(hpcg_b200_batch* B) {
+  const char* fp = std::getenv("HPCG_B200_BATCH_PERSIST");
+  const char* fb = std::getenv("HPCG_B200_BATCH_BULK");
+  if (fp && *fp) {
+    B->persist = std::atoi(fp) != 0 && B->persist_grid > 0;
+    B->bulk = !B->persist && B->packed && fb && *fb && std::atoi(fb) != 0;
     return HPCG_B200_OK;
   }
-  const char* force = std::getenv("HPCG_B200_BATCH_BULK");
-  if (force && *force) {
-    B->bulk = std::atoi(force) != 0;
+  if (fb && *fb) {
+    B->persist = false;
+    B->bulk = B->packed && std::atoi(fb) != 0;
     return HPCG_B200_OK;
   }
   Context* c = B->ctx;
@@ -676,25 +885,35 @@ int choose_bulk(hpcg_b200_batch* B) {
   cudaEvent_t e0, e1;
   HB_CK(cudaEventCreate(&e0));
   HB_CK(cudaEventCreate(&e1));
-  float best[2] = {1e30f, 1e30f};
+  float best[3] = {1e30f, 1e30f, 1e30f};
+  const bool can[3] = {true, B->packed, B->persist_grid > 0};
   int st = HPCG_B200_OK;
   for (int rep = 0; rep < 3 && st == HPCG_B200_OK; ++rep) {
-    for (int b = 0; b < 2 && st == HPCG_B200_OK; ++b) {
-      B->bulk = b != 0;
+    for (int f = 0; f < 3 && st == HPCG_B200_OK; ++f) {
+      if (!can[f]) continue;
+      B->bulk = f == 1;
       if (cudaEventRecord(e0, c->stream) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
-      for (const Step& s : B->steps)
-        if (st == HPCG_B200_OK) st = launch_step(B, s);
+      if (f == 2) {
+        if (st == HPCG_B200_OK) st = launch_iteration(B, true);
+      } else {
+        for (const Step& s : B->steps)
+          if (st == HPCG_B200_OK) st = launch_step(B, s);
+      }
       if (st == HPCG_B200_OK && cudaEventRecord(e1, c->stream) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
       if (st == HPCG_B200_OK) st = stream_sync(c);
       float ms = 0.f;
       if (st == HPCG_B200_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
-      if (st == HPCG_B200_OK && ms < best[b]) best[b] = ms;
+      if (st == HPCG_B200_OK && ms < best[f]) best[f] = ms;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   HB_TRY(st);
-  B->bulk = best[1] < best[0];
+  int f = 0;
+  for (int i = 1; i < 3; ++i)
+    if (best[i] < best[f]) f = i;
+  B->bulk = f == 1;
+  B->persist = f == 2;
   HB_CK(cudaMemset(B->sc, 0, sizeof(BScal) * B->m));
   return HPCG_B200_OK;
 }
@@ -705,7 +924,7 @@ void destroy(hpcg_b200_batch* B) {
   if (B->ctx) cudaStreamSynchronize(B->ctx->stream);
   if (B->graph) cudaGraphExecDestroy(B->graph);
   void* v[] = {B->gs_items, B->res_items, B->tiles, B->gs_bitems, B->btiles, B->vec, B->vtiles, B->vrange,
-               B->partials, B->sc, B->ctl};
+               B->partials, B->sc, B->ctl, B->dsteps, B->bar};
   for (void* q : v) cudaFree(q);
   for (float* q : B->val32) cudaFree(q);
   if (B->sc_host) cudaFreeHost(B->sc_host);
@@ -739,6 +958,7 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
   B->m = count;
   B->gs_items = nullptr; B->res_items = nullptr; B->tiles = nullptr; B->vec = nullptr; B->vtiles = nullptr;
   B->gs_bitems = nullptr; B->btiles = nullptr; B->bulk = false; B->packed = true;
+  B->persist = false; B->persist_grid = 0; B->dsteps = nullptr; B->bar = nullptr;
   B->vrange = nullptr; B->partials = nullptr; B->sc = nullptr; B->sc_host = nullptr; B->ctl = nullptr;
   B->bytes = 0;
   B->graph = nullptr;
@@ -793,9 +1013,24 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
     if (!st) st = dev_alloc((void**)&B->partials, sizeof(double) * 2 * B->nvt, &B->bytes);
     if (!st) st = dev_alloc((void**)&B->sc, sizeof(BScal) * count, &B->bytes);
     if (!st) st = dev_alloc((void**)&B->ctl, sizeof(BCtl), &B->bytes);
+    if (!st) {
+      std::vector<DStep> ds;
+      for (const Step& x : B->steps) ds.push_back(DStep{x.kind, x.tile_off, x.ntiles});
+      st = alloc_copy(B, (void**)&B->dsteps, ds.data(), sizeof(DStep) * ds.size());
+    }
+    if (!st) st = dev_alloc((void**)&B->bar, sizeof(BBar), &B->bytes);
+    if (!st && cudaMemset(B->bar, 0, sizeof(BBar)) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+    if (!st) {
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_iteration, kThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+      }
+      B->persist_grid = c->sms * std::min(per_sm, kBlocksPerSm);
+    }
     if (!st && cudaMallocHost(&B->sc_host, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_NOMEM;
     if (!st && cudaMemset(B->sc, 0, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
-    if (!st) st = choose_bulk(B);
+    if (!st) st = choose_form(B);
   }
   if (st != HPCG_B200_OK) {
     destroy(B);
@@ -831,7 +1066,15 @@ int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* B, const double* const* b, double*
   k_b_resid<<<gv, kThreads, 0, c->stream>>>(B->vec, B->vtiles, B->nvt, B->partials);
   HB_CK(cudaGetLastError());
   HB_TRY(finalize_b(B, kBNorm0));
-  if (!B->graph) HB_TRY(build_graph(B));
+  if (!B->graph) {
+    int gs = build_graph(B);
+    if (gs != HPCG_B200_OK && B->persist) {  // a cooperative launch refused inside a capture
+      cudaGetLastError();
+      B->persist = false;
+      gs = build_graph(B);
+    }
+    HB_TRY(gs);
+  }
   HB_CK(cudaGraphLaunch(B->graph, c->stream));
   HB_CK(cudaMemcpyAsync(B->sc_host, B->sc, sizeof(BScal) * B->m, cudaMemcpyDeviceToHost, c->stream));
   HB_TRY(stream_sync(c));
@@ -842,6 +1085,45 @@ int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* B, const double* const* b, double*
     HB_TRY(store_vector(B->probs[p], 0, B->probs[p]->x, x[p]));
   }
   return HPCG_B200_OK;
+}
+
+int hpcg_b200_batch_form(const hpcg_b200_batch* B, int* form) {
+  if (!valid_batch(B)) return HPCG_B200_ERR_HANDLE;
+  if (!form) return HPCG_B200_ERR_ARG;
+  *form = B->persist ? 2 : B->bulk ? 1 : 0;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_grid_wait_selftest(int device, double seconds) {
+  if (!(seconds > 0.0 && seconds <= 2.0)) return HPCG_B200_ERR_ARG;
+  Context* c = context_for(device);
+  if (!c) return HPCG_B200_ERR_CUDA;
+  HB_CK(cudaSetDevice(device));
+  BBar* bar = nullptr;
+  HB_CK(cudaMalloc(&bar, sizeof(BBar)));
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(BBar), c->stream);
+  if (e == cudaSuccess) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(c->sms);
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_b_barrier_selftest, bar, (unsigned long long)(seconds * 1e9), c->fault);
+  }
+  if (e != cudaSuccess) {
+    set_error("grid wait self-test", e);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(bar);
+    return status_of(e);
+  }
+  const int st = stream_sync(c);
+  cudaFree(bar);
+  return st;
 }
 
 int hpcg_b200_batch_free(hpcg_b200_batch* B) {

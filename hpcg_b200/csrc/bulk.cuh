@@ -117,15 +117,24 @@ struct BulkShape {
 #ifndef HB_SPMV_GROUPS
 #define HB_SPMV_GROUPS 2
 #endif
+#ifndef HB_BULK_RING
+#define HB_BULK_RING 2
+#endif
+#ifndef HB_SPMV_RING
+#define HB_SPMV_RING 2
+#endif
 template <typename T, int PW>
-__host__ __device__ constexpr int fit_groups(int want) {
-  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * 2 * want + 32 * want + 128 > 227 * 1024) --want;
+__host__ __device__ constexpr int fit_groups(int want, int ring) {
+  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * ring * want + 16 * ring * want + 128 > 227 * 1024)
+    --want;
   return want;
 }
 template <typename T, int PW = 0>
-using GsShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_GS64_GROUPS : HB_GS32_GROUPS), 2, 1, PW>;
+using GsShape =
+    BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_GS64_GROUPS : HB_GS32_GROUPS, HB_BULK_RING), HB_BULK_RING, 1, PW>;
 template <typename T, int PW = 0>
-using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_GS32_GROUPS), 2, 1, PW>;
+using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_GS32_GROUPS, sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING),
+                            sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING, 1, PW>;
 
 // Column of slot k of row t of a tile in a stage (sc: the stage's column area)
 // for the column form PW of BulkShape.

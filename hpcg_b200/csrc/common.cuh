@@ -17,9 +17,11 @@
 #include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -313,6 +315,11 @@ struct Context {
   Scalars* scal_host = nullptr;    // pinned mirror
   double* stage[3] = {nullptr, nullptr, nullptr};  // natural-order staging
   size_t stage_cap = 0;            // entries per staging buffer
+  // pinned chunks for copies from and to pageable host memory (host_to_device,
+  // device_to_host), allocated on first use; pin_ev[i]: the last copy that
+  // used pin[i]
+  double* pin[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   // launch profiler: CUDA events around selected launches on `stream`
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;                   // free events
@@ -337,6 +344,12 @@ Context* context_for(int device);
 Context* current_context();
 // Grows the staging buffers to at least n entries.
 int ensure_stage(Context* c, size_t n);
+// n doubles from host memory to device memory, queued on c's stream; returns
+// once src has been read (the copy itself may still be in flight).
+int host_to_device(Context* c, double* dst, const double* src, size_t n);
+// n doubles from device memory (after the work queued on c's stream) to host
+// memory; dst is complete on return.
+int device_to_host(Context* c, double* dst, const double* src, size_t n);
 // Synchronises c's stream; HPCG_B200_ERR_TIMEOUT if a kernel's bounded wait gave
 // up since the last call (the fault word is cleared).
 int stream_sync(Context* c);
@@ -354,6 +367,25 @@ void dev_free(void* ptr);
 // another GPU is refused with HPCG_B200_ERR_ARG (the error text names `what`
 // and both GPUs): a kernel on `device` would fault on it.
 int locate_ptr(const void* ptr, int device, bool* on_device, const char* what);
+
+// body(begin, end) over [0, n) on up to 16 host threads (one below 1 Mi entries)
+template <typename F>
+inline void host_parallel(int64_t n, F&& body) {
+  unsigned t = std::thread::hardware_concurrency();
+  t = t == 0 ? 1 : std::min(t, 16u);
+  if (n < (1 << 20) || t == 1) {
+    body((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const int64_t chunk = (n + t - 1) / t;
+  for (unsigned i = 1; i < t; ++i) {
+    const int64_t b = (int64_t)i * chunk, e = std::min<int64_t>(n, b + chunk);
+    if (b < e) pool.emplace_back([&body, b, e] { body(b, e); });
+  }
+  body((int64_t)0, std::min<int64_t>(n, chunk));
+  for (auto& th : pool) th.join();
+}
 
 // Raises a kernel's dynamic shared-memory limit to `smem` on `device` (the
 // current device) once: `done` is the kernel's own set of devices already

@@ -130,6 +130,84 @@ int ensure_stage(Context* c, size_t n) {
   return HPCG_B200_OK;
 }
 
+// ---- host memory <-> device through pinned chunks ----------------------------
+// A copy from or to pageable host memory runs through the driver's own bounce
+// buffers at a fraction of the link's speed. Large ones go through the
+// context's two pinned chunks instead, double-buffered: host threads copy
+// chunk i between the caller's memory and one pinned chunk while the copy
+// engine moves the neighbouring chunk through the other. Pinned host memory,
+// and copies of under kPinMin entries, go directly.
+namespace {
+constexpr size_t kPinChunk = (size_t)1 << 23;  // doubles per chunk (64 MB)
+constexpr size_t kPinMin = (size_t)1 << 20;
+
+bool pageable(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+int ensure_pin(Context* c) {
+  if (c->pin[0]) return HPCG_B200_OK;
+  for (int i = 0; i < 2; ++i) {
+    HB_CK(cudaMallocHost(&c->pin[i], kPinChunk * sizeof(double)));
+    HB_CK(cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming));
+    HB_CK(cudaEventRecord(c->pin_ev[i], c->stream));
+  }
+  return HPCG_B200_OK;
+}
+
+void host_copy(double* dst, const double* src, size_t n) {
+  host_parallel((int64_t)n, [&](int64_t lo, int64_t hi) {
+    std::memcpy(dst + lo, src + lo, sizeof(double) * (size_t)(hi - lo));
+  });
+}
+}  // namespace
+
+int host_to_device(Context* c, double* dst, const double* src, size_t n) {
+  if (n < kPinMin || !pageable(src)) {
+    HB_CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    return HPCG_B200_OK;
+  }
+  HB_TRY(ensure_pin(c));
+  for (size_t off = 0, i = 0; off < n; off += kPinChunk, ++i) {
+    const size_t len = std::min(kPinChunk, n - off);
+    const int b = (int)(i & 1);
+    HB_CK(cudaEventSynchronize(c->pin_ev[b]));  // the copy engine is done with this chunk's last use
+    host_copy(c->pin[b], src + off, len);
+    HB_CK(cudaMemcpyAsync(dst + off, c->pin[b], sizeof(double) * len, cudaMemcpyHostToDevice, c->stream));
+    HB_CK(cudaEventRecord(c->pin_ev[b], c->stream));
+  }
+  return HPCG_B200_OK;
+}
+
+int device_to_host(Context* c, double* dst, const double* src, size_t n) {
+  if (n < kPinMin || !pageable(dst)) {
+    HB_CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    HB_CK(cudaStreamSynchronize(c->stream));
+    return HPCG_B200_OK;
+  }
+  HB_TRY(ensure_pin(c));
+  const size_t chunks = (n + kPinChunk - 1) / kPinChunk;
+  auto issue = [&](size_t i) -> int {
+    const size_t off = i * kPinChunk, len = std::min(kPinChunk, n - off);
+    HB_CK(cudaMemcpyAsync(c->pin[i & 1], src + off, sizeof(double) * len, cudaMemcpyDeviceToHost, c->stream));
+    HB_CK(cudaEventRecord(c->pin_ev[i & 1], c->stream));
+    return HPCG_B200_OK;
+  };
+  HB_TRY(issue(0));
+  for (size_t i = 0; i < chunks; ++i) {
+    if (i + 1 < chunks) HB_TRY(issue(i + 1));  // the other chunk is free: its host copy finished below
+    HB_CK(cudaEventSynchronize(c->pin_ev[i & 1]));
+    const size_t off = i * kPinChunk;
+    host_copy(dst + off, c->pin[i & 1], std::min(kPinChunk, n - off));
+  }
+  return HPCG_B200_OK;
+}
+
 // cuTensorMapEncodeTiled, looked up once through the runtime (no link to the driver library).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -182,8 +260,10 @@ int stream_sync(Context* c) {
   HB_CK(cudaStreamSynchronize(c->stream));
   volatile unsigned* f = c->fault;
   if (f && *f) {
+    const unsigned code = *f;
     *f = 0;
-    set_error_text("a device-side wait gave up (bounded mbarrier wait in a Gauss-Seidel phase)");
+    set_error_text(code == 5 ? "a device-side wait gave up (bounded wait at the batched iteration's grid barrier)"
+                             : "a device-side wait gave up (bounded mbarrier wait of the bulk-copy pipeline)");
     return HPCG_B200_ERR_TIMEOUT;
   }
   return HPCG_B200_OK;

@@ -381,7 +381,7 @@ int load_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, dou
       HB_CK(cudaMalloc(&m->stage, sizeof(double) * need));
       m->stage_cap = need;
     }
-    HB_CK(cudaMemcpyAsync(m->stage, src, sizeof(double) * need, cudaMemcpyHostToDevice, c->stream));
+    HB_TRY(host_to_device(c, m->stage, src, need));
     s = m->stage;
   }
   auto k = k_gather_in_m<K>;
@@ -411,7 +411,7 @@ int store_m(hpcg_b200_problem* P, MultiState* m, int nrhs, const double* src, do
   auto k = k_scatter_out_m<K>;
   k<<<grid_of(c, k, L.n), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n, nrhs);
   HB_CK(cudaGetLastError());
-  if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+  if (!dev) HB_TRY(device_to_host(c, dst, d, need));
   return stream_sync(c);
 }
 

@@ -596,7 +596,7 @@ int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal) {
   HB_TRY(locate_ptr(diagonal, p->device, &dev, "hpcg_b200_set_diagonal"));
   if (!dev) {
     HB_TRY(ensure_stage(c, L.n));
-    HB_CK(cudaMemcpyAsync(c->stage[1], diagonal, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
+    HB_TRY(host_to_device(c, c->stage[1], diagonal, (size_t)L.n));
     src = c->stage[1];
   }
   k_set_diag<<<grid_for(c, L.n, 256, 8), 256, 0, c->stream>>>(src, L.old2new, L.val + kDiagSlot * L.pitch, L.n);

@@ -579,11 +579,11 @@ int hpcg_b200_shard_dot(hpcg_b200_comm* comm, const double* const* x, const doub
     if (!xdev || !ydev) {
       HB_TRY(ensure_stage(c, (size_t)n));
       if (!xdev) {
-        HB_CK(cudaMemcpyAsync(c->stage[0], xd, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        HB_TRY(host_to_device(c, c->stage[0], xd, (size_t)n));
         xd = c->stage[0];
       }
       if (!ydev) {
-        HB_CK(cudaMemcpyAsync(c->stage[1], yd, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        HB_TRY(host_to_device(c, c->stage[1], yd, (size_t)n));
         yd = c->stage[1];
       }
     }

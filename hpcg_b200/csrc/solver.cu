@@ -1248,7 +1248,7 @@ int load_vector(hpcg_b200_problem* p, int level, const double* src, double* dst)
   HB_TRY(locate_ptr(src, p->device, &dev, "input vector"));
   if (!dev) {
     HB_TRY(ensure_stage(c, L.n));
-    HB_CK(cudaMemcpyAsync(c->stage[0], src, sizeof(double) * L.n, cudaMemcpyHostToDevice, c->stream));
+    HB_TRY(host_to_device(c, c->stage[0], src, L.n));
     s = c->stage[0];
   }
   k_gather<double><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(dst, s, L.new2old, L.n);
@@ -1269,7 +1269,7 @@ int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst
   }
   k_gather<double><<<grid_for(c, L.n, kThreads, kPerSm), kThreads, 0, c->stream>>>(d, src, L.old2new, L.n);
   HB_CK(cudaGetLastError());
-  if (!dev) HB_CK(cudaMemcpyAsync(dst, d, sizeof(double) * L.n, cudaMemcpyDeviceToHost, c->stream));
+  if (!dev) HB_TRY(device_to_host(c, dst, d, L.n));
   HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }
@@ -1289,25 +1289,6 @@ bool host_reuse_enabled() {
     return !(e && e[0] == '0');
   }();
   return on;
-}
-
-// body(begin, end) over [0, n) on up to 16 host threads (one below 1 Mi entries)
-template <typename F>
-void host_parallel(int64_t n, F&& body) {
-  unsigned t = std::thread::hardware_concurrency();
-  t = t == 0 ? 1 : std::min(t, 16u);
-  if (n < (1 << 20) || t == 1) {
-    body((int64_t)0, n);
-    return;
-  }
-  std::vector<std::thread> pool;
-  const int64_t chunk = (n + t - 1) / t;
-  for (unsigned i = 1; i < t; ++i) {
-    const int64_t b = (int64_t)i * chunk, e = std::min<int64_t>(n, b + chunk);
-    if (b < e) pool.emplace_back([&body, b, e] { body(b, e); });
-  }
-  body((int64_t)0, std::min<int64_t>(n, chunk));
-  for (auto& th : pool) th.join();
 }
 
 bool host_same_bits(const double* a, const double* b, int64_t n) {
@@ -1380,7 +1361,7 @@ int device_view(Context* c, const double* v, int n, int slot, const double** out
     return HPCG_B200_OK;
   }
   HB_TRY(ensure_stage(c, (size_t)n));
-  HB_CK(cudaMemcpyAsync(c->stage[slot], v, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  HB_TRY(host_to_device(c, c->stage[slot], v, (size_t)n));
   *out = c->stage[slot];
   return HPCG_B200_OK;
 }
@@ -1561,7 +1542,7 @@ int hpcg_b200_waxpby(int n, double alpha, const double* x, double beta, const do
   double* dw = wdev ? w : c->stage[2];
   k_waxpby<false><<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, alpha, dx, beta, dy, dw, nullptr);
   HB_CK(cudaGetLastError());
-  if (!wdev) HB_CK(cudaMemcpyAsync(w, dw, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  if (!wdev) HB_TRY(device_to_host(c, w, dw, (size_t)n));
   HB_TRY(stream_sync(c));
   return HPCG_B200_OK;
 }

@@ -157,11 +157,12 @@ int hpcg_b200_mg_multi(hpcg_b200_problem* p, int nrhs, const double* r, double* 
 
 /* Many independent problems of different sizes solved together (flexible FP64
  * CG around the FP32 V-cycle, as hpcg_b200_cg_mixed for each). Every step of an
- * iteration is one kernel launch over a work list of row tiles spanning all the
- * problems, and the iteration loop is one CUDA graph launch (a conditional while
- * node runs while any problem is above its tolerance); converged problems skip
- * their tiles. Every grid dimension must be a multiple of 16. No reference
- * counterpart (changed form). */
+ * iteration walks a work list of row tiles spanning all the problems, either
+ * as one kernel launch per step or all steps in one cooperative launch
+ * (hpcg_b200_batch_form), and the iteration loop is one CUDA graph launch (a
+ * conditional while node runs while any problem is above its tolerance);
+ * converged problems skip their tiles. Every grid dimension must be a
+ * multiple of 16. No reference counterpart (changed form). */
 typedef struct hpcg_b200_batch hpcg_b200_batch;
 
 /* Generates problem i on the device as hpcg_b200_generate(nx[i], ny[i], nz[i], 4). */
@@ -175,6 +176,21 @@ int hpcg_b200_batch_problem(hpcg_b200_batch* batch, int i, hpcg_b200_problem** o
 int hpcg_b200_batch_cg_mixed(hpcg_b200_batch* batch, const double* const* b, double* const* x, int max_iter,
                              double tolerance, int* niters, double* normr, double* normr0);
 int hpcg_b200_batch_free(hpcg_b200_batch* batch);
+/* How the batch runs an iteration, chosen by timing at creation (or by
+ * HPCG_B200_BATCH_PERSIST / HPCG_B200_BATCH_BULK): 0 one launch per step with
+ * the colour phases on the register kernel, 1 the same on the bulk-copy
+ * kernel, 2 the whole iteration as one cooperative launch whose steps are
+ * separated by grid barriers with bounded waits (a wait that gives up ends the
+ * solve with HPCG_B200_ERR_TIMEOUT). */
+int hpcg_b200_batch_form(const hpcg_b200_batch* batch, int* form);
+
+/* Check of the bounded wait of the batched iteration's grid barrier: a
+ * cooperative launch of one block per SM in which every block waits for one
+ * arrival more than the grid holds, so every wait gives up after `seconds`
+ * (0 < seconds <= 2) and records the fault. Returns HPCG_B200_ERR_TIMEOUT (the
+ * expected outcome) with the device context still usable. No reference
+ * counterpart: test support for the wait path. */
+int hpcg_b200_grid_wait_selftest(int device, double seconds);
 
 /* ---- changed form 3: implicit adjoint of the solve ------------------------ */
 

@@ -2,7 +2,10 @@
 together must follow their one-at-a-time solves (hpcg_b200_cg_mixed): the same
 V-cycle bits per problem, dots in another (fixed) order, so the same iteration
 counts within one, scaled residuals within 1e-10 * max(r, 1e-9) on fixed
-iteration counts, and solutions within 1e-7 at the tolerance."""
+iteration counts, and solutions within 1e-7 at the tolerance. The one-launch
+iteration (every step in one cooperative launch) equals the launch-per-step
+form on the register phases bit for bit, and its grid barrier's bounded wait
+ends by itself."""
 import numpy as np
 import pytest
 
@@ -79,5 +82,60 @@ def test_batch_both_phase_kernels_follow_single_solves(binding, monkeypatch, bul
             s = r1 / r01
             assert abs(nr[i] / nr0[i] - s) <= 1e-10 * max(s, 1e-9), (i, nr[i] / nr0[i], s)
             assert np.max(np.abs(xs[i] - x1)) <= 1e-9 * max(np.max(np.abs(x1)), 1.0)
+    finally:
+        B.free()
+
+
+def test_batch_one_launch_iteration_equals_launch_per_step(binding, monkeypatch):
+    """The whole iteration as one cooperative launch (steps separated by grid
+    barriers) computes the same bits as one launch per step on the register
+    phases: the same work lists, the same per-tile partials, the same order.
+    Compared on fixed iteration counts and at a tolerance, with a problem that
+    converges early (zero right-hand side)."""
+    dims = [(16, 32, 48), (32, 16, 16), (16, 16, 16)]
+    outs = []
+    for persist in ("1", "0"):
+        monkeypatch.setenv("HPCG_B200_BATCH_PERSIST", persist)
+        monkeypatch.setenv("HPCG_B200_BATCH_BULK", "0")
+        B = binding.Batch(dims)
+        try:
+            assert B.form() == (2 if persist == "1" else 0)
+            bs = [p.get_rhs() for p in B.problems]
+            bs[2] = np.zeros_like(bs[2])
+            res = []
+            for iters, tol in ((7, 0.0), (500, 1e-9)):
+                xs = [np.zeros(p.nrow) for p in B.problems]
+                ni, nr, nr0 = B.CG_mixed(bs, xs, iters, tol)
+                res.append((ni.copy(), nr.copy(), nr0.copy(), [x.copy() for x in xs]))
+            outs.append(res)
+        finally:
+            B.free()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+        for xa, xb in zip(a[3], b[3]):
+            assert np.array_equal(xa, xb)
+    assert outs[0][1][0][2] == 0 and np.all(outs[0][1][1][:2] / outs[0][1][2][:2] <= 1e-9)
+
+
+def test_grid_barrier_wait_gives_up_and_context_survives(binding, monkeypatch):
+    """The grid barrier of the one-launch iteration ends by itself: with one
+    arrival more expected than the grid holds, every block's wait gives up
+    after the limit and the call returns HPCG_B200_ERR_TIMEOUT; the same context
+    then runs a batched solve in the one-launch form."""
+    import time
+    t0 = time.perf_counter()
+    st = binding.grid_wait_selftest(0.25)
+    dt = time.perf_counter() - t0
+    assert st == binding.ERR_TIMEOUT
+    assert 0.2 <= dt < 30.0
+    assert "gave up" in binding.last_error()
+    monkeypatch.setenv("HPCG_B200_BATCH_PERSIST", "1")
+    B = binding.Batch([(16, 16, 32), (32, 16, 16)])
+    try:
+        assert B.form() == 2
+        bs = [p.get_rhs() for p in B.problems]
+        xs = [np.zeros(p.nrow) for p in B.problems]
+        ni, nr, nr0 = B.CG_mixed(bs, xs, 200, 1e-8)
+        assert np.all(nr / nr0 <= 1e-8)
     finally:
         B.free()

@@ -131,6 +131,24 @@ def test_flop_and_byte_models(oracle):
     assert abs(per_iter / 5.0162e10 - 1) < 5e-3  # 5.0007e10 by the exact formula
 
 
+def test_iteration_byte_model():
+    """metrics.iteration_bytes, the floor the library's kernels move per CG
+    iteration: the index width enters only through the bulk-copy kernels'
+    records (27.875 / 54.875 / 108 B per row), the FP32 V-cycle halves the
+    V-cycle's value and vector bytes but not the FP64 SpMV and CG vectors."""
+    from hpcg_b200 import metrics
+    assert metrics.index_bytes_per_row(1) == 27.875 and metrics.index_bytes_per_row(2) == 54.875
+    assert metrics.index_bytes_per_row(0) == 108
+    b = {w: metrics.iteration_bytes(512, 512, 512, 8, (w,) * 4) for w in (0, 1, 2)}
+    assert b[1] < b[2] < b[0]
+    assert abs(b[2] / 1e9 - 232.97) < 0.01  # 16-bit offsets, every level
+    assert abs(b[1] / 1e9 - 217.46) < 0.01  # 8-bit offsets, every level
+    t, parts = metrics.iteration_bytes(512, 512, 512, 4, (1,) * 4, parts=True)
+    assert abs(sum(parts.values()) * 1e9 - t) < 1.0
+    assert parts["spmv"] == metrics.spmv_bytes(512 ** 3, 8, 1) / 1e9 and parts["vectors"] == 96 * 512 ** 3 / 1e9
+    assert 0.66 < t / b[1] < 0.67
+
+
 def test_gpu_launch_count_model():
     import bench
     # 16 launches per symmetric sweep would double count; the model is 15 per sweep.
