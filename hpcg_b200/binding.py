@@ -332,13 +332,14 @@ class Problem:
         return n.value, pitch.value, starts
 
     def level_pack_width(self, level):
-        """Offset width in bytes of the level's packed columns (1 or 2); 0 if it
-        keeps only its 32-bit columns."""
+        """Form of the level's packed columns: 1 or 2 (offset bytes), 3 (the
+        diagonal form); 0 if it keeps only its 32-bit columns."""
         b = self.level_packed(level)
         if b == 0:
             return 0
         _, pitch, _ = self.level_info(level)
-        return 1 if b == pitch // 128 * (28 * 4 + 27 * 128) else 2
+        per_tile = b // (pitch // 128)
+        return {28 * 4 + 27 * 128: 1, 28 * 4 + 27 * 256: 2, 28 * 4 + 27 * 16: 3}[per_tile]
 
     def level_packed(self, level):
         """Bytes of the level's packed column index (0: 32-bit columns only)."""

@@ -54,26 +54,35 @@ __host__ __device__ constexpr bool bulk_tensor_tile() {
 }
 // Packed columns: a level's column indices as one record per kBulkRows-row
 // tile of its storage (tile j: rows kBulkRows j ..): kSlots 32-bit bases and a
-// word that holds the offset width w (the offsets then start on 16 bytes),
-// then kSlots x kBulkRows offsets of w bytes, slot-major. Slot k of row t of
-// the tile is column base[k] + offset, or the level's zero sink where the
-// offset is pack_sink(w). w is 1 where every tile's columns of each slot (sink
-// aside) span at most pack_max_span(1) = 254, else 2 where they span at most
-// 65534; a level whose tiles span more keeps only its 32-bit columns. 27.9
-// (w = 1) or 54.9 (w = 2) bytes a row instead of 108; one bulk copy per tile,
-// as the blocked FP32 columns.
+// word that holds the record's form w (the rest then starts on 16 bytes), then
+//  - w = 1, 2: kSlots x kBulkRows offsets of w bytes, slot-major. Slot k of row
+//    t is column base[k] + offset, or the level's zero sink where the offset is
+//    pack_sink(w). w = 1 where every tile's columns of each slot (sink aside)
+//    span at most pack_max_span(1) = 254, else 2 where they span at most 65534;
+//  - w = 3 (diagonal): kSlots x 4 words of sink bits. Slot k of row t is column
+//    base[k] + t, or the sink where bit t of the slot's 128 bits is set: for
+//    tiles whose every slot's columns, sink aside, are one diagonal (column -
+//    row the same for every row). In the colour order of a 27-point stencil
+//    whose colour blocks fill whole tiles every tile is so;
+// tried in the order 3, 1, 2; a level that fits none keeps only its 32-bit
+// columns. 4.25 (w = 3), 27.9 (w = 1) or 54.9 (w = 2) bytes a row instead of
+// 108; one bulk copy per tile, as the blocked FP32 columns.
 constexpr int kPackBaseWords = 28;
-__host__ __device__ constexpr int pack_rec(int w) { return kPackBaseWords * 4 + kSlots * kBulkRows * w; }
+constexpr int kPackDiag = 3;  // the diagonal form's code
+__host__ __device__ constexpr int pack_rec(int w) {
+  return kPackBaseWords * 4 + (w == kPackDiag ? kSlots * (kBulkRows / 32) * 4 : kSlots * kBulkRows * w);
+}
 __host__ __device__ constexpr unsigned pack_sink(int w) { return w == 1 ? 0xFFu : 0xFFFFu; }
 __host__ __device__ constexpr int pack_max_span(int w) { return w == 1 ? 0xFE : 0xFFFE; }
-static_assert(pack_rec(1) % 16 == 0 && pack_rec(2) % 16 == 0, "a record is one bulk copy");
+static_assert(pack_rec(1) % 16 == 0 && pack_rec(2) % 16 == 0 && pack_rec(kPackDiag) % 16 == 0,
+              "a record is one bulk copy");
 
 // Shape of a pipeline: G consumer groups of kBulkRows x LANES threads, each
 // with a ring of RING stages of one tile. A stage holds the tile's values and
-// its columns: 32-bit (PW = 0), or the packed record with offsets of PW bytes
-// (PW = 1, 2), or, with PW = -1, a record whose width each tile states (the
-// batched kernel, whose tiles come from several levels): staged for the wider
-// one, each fill expecting its own record's bytes. Stages are rounded up to
+// its columns: 32-bit (PW = 0), or the packed record of form PW (1, 2: offsets
+// of PW bytes; 3: diagonal), or, with PW = -1, a record whose form each tile
+// states (the batched kernel, whose tiles come from several levels): staged
+// for the largest one, each fill expecting its own record's bytes. Stages are rounded up to
 // 128 bytes (tensor copies land on 128-byte boundaries): FP64 stages are 41.5
 // KB (33.9 KB with 16-bit offsets, 30.5 KB with 8-bit ones) and FP32 ones 27
 // KB (20.4 / 17 KB); all stages of a block share at most 227 KB of shared
@@ -96,7 +105,7 @@ struct BulkShape {
   static constexpr int smem = stages * stage_bytes + 2 * stages * (int)sizeof(uint64_t) + 128;
   static_assert(smem <= 227 * 1024, "shared memory of one block");
   static_assert(threads <= 1024, "threads of one block");
-  static_assert(PW >= -1 && PW <= 2, "offset width");
+  static_assert(PW >= -1 && PW <= kPackDiag, "column form");
 };
 // The shapes in use: rings of two stages (measured at 512^3: two groups of two
 // stages beat four groups of one for the Gauss-Seidel phases by 8% and tied for
@@ -148,8 +157,14 @@ __device__ __forceinline__ int stage_col(const int* sc, int k, int t, int sink) 
   } else if constexpr (PW == 2) {
     const unsigned o = reinterpret_cast<const unsigned short*>(sc + kPackBaseWords)[k * kBulkRows + t];
     return o == pack_sink(2) ? sink : sc[k] + (int)o;
+  } else if constexpr (PW == kPackDiag) {
+    // the warp's 32 rows share one word of sink bits (a broadcast load)
+    const unsigned bits = reinterpret_cast<const unsigned*>(sc + kPackBaseWords)[k * (kBulkRows / 32) + (t >> 5)];
+    return (bits >> (t & 31)) & 1u ? sink : sc[k] + t;
   } else {
-    return sc[kSlots] == 1 ? stage_col<1>(sc, k, t, sink) : stage_col<2>(sc, k, t, sink);
+    const int w = sc[kSlots];
+    return w == 1 ? stage_col<1>(sc, k, t, sink) : w == 2 ? stage_col<2>(sc, k, t, sink)
+                                                           : stage_col<kPackDiag>(sc, k, t, sink);
   }
 }
 

@@ -226,7 +226,9 @@ void launch_phase_m(Context* c, const Level& L, const double* rhs, double* x, in
   // the register-pipelined kernels
   const BulkMaps* bm = L.colp && (BULK == 2 || (BULK == 1 && !first)) ? bulk_maps(L) : nullptr;
   if (bm) {
-    if (L.pack == 1)
+    if (L.pack == kPackDiag)
+      launch_phase_m_bulk<K, LANES, kPackDiag>(c, L, bm, rhs, x, r0, r1, first, mask);
+    else if (L.pack == 1)
       launch_phase_m_bulk<K, LANES, 1>(c, L, bm, rhs, x, r0, r1, first, mask);
     else
       launch_phase_m_bulk<K, LANES, 2>(c, L, bm, rhs, x, r0, r1, first, mask);
@@ -263,8 +265,9 @@ template <int K, int LANES, int BULK, bool DOT>
 int spmv_m(Context* c, const Level& L, const double* x, double* y, double* partials) {
   const BulkMaps* bm = BULK && L.colp ? bulk_maps(L) : nullptr;
   if (bm) {
-    const int g = L.pack == 1 ? spmv_m_bulk<K, LANES, DOT, 1>(c, L, bm, x, y, partials)
-                              : spmv_m_bulk<K, LANES, DOT, 2>(c, L, bm, x, y, partials);
+    const int g = L.pack == kPackDiag ? spmv_m_bulk<K, LANES, DOT, kPackDiag>(c, L, bm, x, y, partials)
+                  : L.pack == 1       ? spmv_m_bulk<K, LANES, DOT, 1>(c, L, bm, x, y, partials)
+                                      : spmv_m_bulk<K, LANES, DOT, 2>(c, L, bm, x, y, partials);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       set_error("k_spmv_m_bulk", e);

@@ -251,8 +251,64 @@ __global__ void __launch_bounds__(kBulkRows) k_pack_cols(const int* __restrict__
   }
 }
 
+// The packed columns of a level in the diagonal form (records of
+// pack_rec(kPackDiag) bytes): slot k's base is column - row of the tile's
+// columns that are not the sink, and its sink bits mark the rest. Rows at or
+// beyond n are stored as the sink. Sets *bad if a slot's columns of a tile are
+// not one diagonal (column - row differs between two of its rows).
+__global__ void __launch_bounds__(kBulkRows) k_pack_cols_diag(const int* __restrict__ col, int64_t pitch, int n,
+                                                              int sink, int64_t ntiles,
+                                                              unsigned char* __restrict__ colp, int* bad) {
+  constexpr int NW = kBulkRows / 32;
+  __shared__ int wlo[NW], whi[NW];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t q = tile * kBulkRows + t;
+    int* base = reinterpret_cast<int*>(colp + tile * pack_rec(kPackDiag));
+    unsigned* bits = reinterpret_cast<unsigned*>(base + kPackBaseWords);
+    if (t == 0) base[kSlots] = kPackDiag;  // the record states its form
+    for (int k = 0; k < kSlots; ++k) {
+      const int c = q < n ? col[mat_index<double>(k, q, pitch)] : sink;
+      const bool real = c != sink;
+      const int d = c - t;  // the diagonal this row's column lies on
+      int lo = real ? d : INT_MAX, hi = real ? d : INT_MIN;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      }
+      const unsigned sinks = __ballot_sync(0xffffffffu, !real);
+      if (lane == 0) {
+        wlo[w] = lo;
+        whi[w] = hi;
+        bits[k * NW + w] = sinks;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < NW; ++i) {
+        lo = min(lo, wlo[i]);
+        hi = max(hi, whi[i]);
+      }
+      __syncthreads();
+      if (t == 0) {
+        base[k] = lo == INT_MAX ? 0 : lo;
+        if (lo != INT_MAX && lo != hi) *bad = 1;
+      }
+    }
+  }
+}
+
 // Packs level l's columns with W-byte offsets into a new allocation; on return
 // L.colp / L.pack describe it, or are left empty if a tile does not pack.
+template <int W>
+void launch_pack(Context* c, const Level& L, int64_t ntiles, unsigned char* colp, int* bad) {
+  const int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms * 16);
+  if constexpr (W == kPackDiag)
+    k_pack_cols_diag<<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, colp, bad);
+  else
+    k_pack_cols<W><<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, colp, bad);
+}
+
 template <int W>
 int try_pack(hpcg_b200_problem* p, int l) {
   Level& L = p->lev[l];
@@ -266,8 +322,7 @@ int try_pack(hpcg_b200_problem* p, int l) {
   int h = 0;
   if (err == cudaSuccess) err = cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
   if (err == cudaSuccess) {
-    const int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms * 16);
-    k_pack_cols<W><<<g, kBulkRows, 0, c->stream>>>(L.col, L.pitch, L.n, sink_of(L), ntiles, colp, bad);
+    launch_pack<W>(c, L, ntiles, colp, bad);
     err = cudaGetLastError();
   }
   if (err == cudaSuccess) err = cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
@@ -288,17 +343,20 @@ int try_pack(hpcg_b200_problem* p, int l) {
   return HPCG_B200_OK;
 }
 
-// The packed columns of level l for the bulk-copy kernels (k_pack_cols): 8-bit
-// offsets where every tile's spans allow, else 16-bit ones; the level keeps
-// only its 32-bit columns if a tile does not pack either way.
-// HPCG_B200_PACKED at creation: "0" leaves every level unpacked, "16" skips
-// the 8-bit form (for comparisons).
+// The packed columns of level l for the bulk-copy kernels: the diagonal form
+// where every tile's slots are diagonals, else 8-bit offsets where every
+// tile's spans allow, else 16-bit ones; the level keeps only its 32-bit
+// columns if a tile does not pack any of these ways.
+// HPCG_B200_PACKED at creation (for comparisons): "0" leaves every level
+// unpacked, "8" starts at the 8-bit offsets, "16" takes 16-bit ones only.
 int build_packed(hpcg_b200_problem* p, int l) {
   Level& L = p->lev[l];
   const char* e = std::getenv("HPCG_B200_PACKED");
   if ((e && e[0] == '0') || L.n <= 0) return HPCG_B200_OK;
-  const bool allow8 = !(e && std::strcmp(e, "16") == 0);
-  if (allow8) HB_TRY(try_pack<1>(p, l));
+  const bool only16 = e && std::strcmp(e, "16") == 0;
+  const bool from8 = e && std::strcmp(e, "8") == 0;
+  if (!only16 && !from8) HB_TRY(try_pack<kPackDiag>(p, l));
+  if (!L.colp && !only16) HB_TRY(try_pack<1>(p, l));
   if (!L.colp) HB_TRY(try_pack<2>(p, l));
   return HPCG_B200_OK;
 }

@@ -117,6 +117,8 @@ bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T
 template <typename T, typename TR, bool FIRST, int64_t CMASK, bool DOT>
 bool gs_bulk_launch(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int r0, int r1, uint32_t mask,
                     double* dot) {
+  if (L.pack == kPackDiag)
+    return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, kPackDiag>(c, L, val, rhs, x, r0, r1, mask, dot);
   if (L.pack == 1) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 1>(c, L, val, rhs, x, r0, r1, mask, dot);
   if (L.pack == 2) return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 2>(c, L, val, rhs, x, r0, r1, mask, dot);
   return gs_bulk_launch_p<T, TR, FIRST, CMASK, DOT, 0>(c, L, val, rhs, x, r0, r1, mask, dot);
@@ -302,11 +304,13 @@ int spmv_bulk(Context* c, const Level& L, const T* val, const T* x, T* y, double
     if (!m) return 0;
     if (L.mv_order == 2 && bulk_slab_ok(L)) {
       if (packed_slab_ok(L)) {
+        if (L.pack == kPackDiag) return spmv_bulk_launch<T, DOT, 2, kPackDiag>(c, L, val, x, y, partials, m);
         if (L.pack == 1) return spmv_bulk_launch<T, DOT, 2, 1>(c, L, val, x, y, partials, m);
         return spmv_bulk_launch<T, DOT, 2, 2>(c, L, val, x, y, partials, m);
       }
       return spmv_bulk_launch<T, DOT, 2, 0>(c, L, val, x, y, partials, m);
     }
+    if (L.pack == kPackDiag) return spmv_bulk_launch<T, DOT, 0, kPackDiag>(c, L, val, x, y, partials, m);
     if (L.pack == 1) return spmv_bulk_launch<T, DOT, 0, 1>(c, L, val, x, y, partials, m);
     if (L.pack == 2) return spmv_bulk_launch<T, DOT, 0, 2>(c, L, val, x, y, partials, m);
     return spmv_bulk_launch<T, DOT, 0, 0>(c, L, val, x, y, partials, m);
@@ -365,6 +369,7 @@ bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, cons
 template <typename T>
 bool restrict_bulk(Context* c, const Level& L, const T* val, const T* rf, const T* xf, T* rc, int nc) {
   if (L.tf_run < 0 || nc <= 0) return false;
+  if (L.pack == kPackDiag) return restrict_bulk_p<T, kPackDiag>(c, L, val, rf, xf, rc, nc);
   if (L.pack == 1) return restrict_bulk_p<T, 1>(c, L, val, rf, xf, rc, nc);
   if (L.pack == 2) return restrict_bulk_p<T, 2>(c, L, val, rf, xf, rc, nc);
   return restrict_bulk_p<T, 0>(c, L, val, rf, xf, rc, nc);

@@ -91,8 +91,11 @@ def compulsory_bytes(nx, ny, nz, nlevels=4, vb=8):
 
 def index_bytes_per_row(pack=0):
     """Column-index bytes per row: 27 int32 columns (pack 0), or the packed
-    index with offsets of `pack` bytes (one record per 128-row tile: 27 int32
-    bases, the width word, 27 x 128 offsets): 27.875 B (pack 1), 54.875 B (2)."""
+    index, one record per 128-row tile of 27 int32 bases and the form word
+    followed by 27 x 128 offsets of `pack` bytes, 27.875 B (pack 1) or 54.875 B
+    (2) a row, or by 27 x 128 sink bits (the diagonal form, pack 3), 4.25 B."""
+    if pack == 3:
+        return (28 * 4 + SLOTS * 4 * 4) / 128.0
     if pack:
         return (28 * 4 + SLOTS * 128 * pack) / 128.0
     return SLOTS * 4

@@ -662,21 +662,26 @@ def test_cg_forced_config_vs_oracle(oracle, binding, monkeypatch, cfg):
 @pytest.mark.parametrize("dims", [(32, 32, 32), (16, 24, 40), (24, 24, 24)])
 def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
     """The bulk-copy kernels read a level's packed column index (one record per
-    128-row tile: 27 bases, the offset width, then 8-bit offsets where every
-    tile's slot spans at most 254 rows, else 16-bit ones); a problem made with
-    HPCG_B200_PACKED=16 takes 16-bit offsets everywhere, and one made with
-    HPCG_B200_PACKED=0 keeps only the 32-bit columns. Each level gets the width
-    the numpy restatement of the format predicts. With the bulk-copy
-    configurations forced, SpMV, SYMGS, the V-cycle and CG around the FP32
-    V-cycle give the same bits all three ways (16x24x40 and 24^3: colour blocks
-    off the 128-row grid on some levels, which then take 16-bit offsets, and
-    where the slab-order SpMV keeps the 32-bit columns). The FP64 CG forms r'z
-    by its own dot pass on the packed phases and from the post-smoother's
-    partials on the unpacked ones, so its history and x agree to rounding there
-    and bit for bit between the two packed forms."""
+    128-row tile: 27 bases and the record's form, then either the diagonal
+    form's sink bits, where every slot's columns across a tile are one
+    diagonal, or 8-bit offsets where every tile's slot spans at most 254 rows,
+    else 16-bit ones). Problems made with HPCG_B200_PACKED=8 (no diagonal
+    form), =16 (16-bit offsets everywhere) and =0 (only the 32-bit columns)
+    are the other three forms. Each level gets the form the numpy restatement
+    of the format predicts. With the bulk-copy configurations forced, SpMV,
+    SYMGS, the V-cycle and CG around the FP32 V-cycle give the same bits all
+    four ways (16x24x40 and 24^3: colour blocks off the 128-row grid on some
+    levels, which then take offsets, and where the slab-order SpMV keeps the
+    32-bit columns). The FP64 CG forms r'z by its own dot pass on the packed
+    phases and from the post-smoother's partials on the unpacked ones, so its
+    history and x agree to rounding there and bit for bit among the packed
+    forms."""
     from tests.test_packed_format import packed_width
+    rec = {1: 3568, 2: 7024, 3: 544}
     monkeypatch.setenv("HPCG_B200_CONFIG", "10")
     A = binding.Problem.generate(*dims)
+    monkeypatch.setenv("HPCG_B200_PACKED", "8")
+    E = binding.Problem.generate(*dims)
     monkeypatch.setenv("HPCG_B200_PACKED", "16")
     W = binding.Problem.generate(*dims)
     monkeypatch.setenv("HPCG_B200_PACKED", "0")
@@ -684,9 +689,12 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
     try:
         for lv in range(4):
             _, pitch, _ = A.level_info(lv)
-            w = packed_width(binding, dims[0] >> lv, dims[1] >> lv, dims[2] >> lv)
-            assert w in (1, 2)
-            assert A.level_packed(lv) == pitch // 128 * (3568 if w == 1 else 7024)
+            sides = (dims[0] >> lv, dims[1] >> lv, dims[2] >> lv)
+            f = packed_width(binding, *sides)
+            w = packed_width(binding, *sides, diagonal=False)
+            assert f in (1, 2, 3) and w in (1, 2)
+            assert A.level_packed(lv) == pitch // 128 * rec[f] and A.level_pack_width(lv) == f
+            assert E.level_packed(lv) == pitch // 128 * rec[w]
             assert W.level_packed(lv) == pitch // 128 * 7024
             assert U.level_packed(lv) == 0
         n = A.nrow
@@ -694,7 +702,7 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
         rng = np.random.default_rng(7)
         v = rng.uniform(-1.0, 1.0, n)
         outs = []
-        for P in (A, W, U):
+        for P in (A, E, W, U):
             y = np.zeros(n)
             P.ComputeSPMV(v, y)
             xs = v.copy()
@@ -707,7 +715,7 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
             rf = P.CG_mixed(b, xf, 25, 0.0)
             assert P.level_config(0)["gs"] == 10 and P.level_config(0)["gs32"] == 10
             outs.append((y, xs, xm, xc, rc, xf, rf))
-        for other, exact_cg in ((outs[1], True), (outs[2], False)):
+        for other, exact_cg in ((outs[1], True), (outs[2], True), (outs[3], False)):
             for i, (a, u) in enumerate(zip(outs[0], other)):
                 if i in (3, 4) and not exact_cg:  # FP64 CG: r'z summed in another order
                     if isinstance(a, np.ndarray):
@@ -721,6 +729,7 @@ def test_packed_columns_equal_plain_columns(binding, monkeypatch, dims):
                     assert a == u
     finally:
         A.free()
+        E.free()
         W.free()
         U.free()
 

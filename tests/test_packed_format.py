@@ -1,15 +1,17 @@
 """The packed column format of the bulk-copy kernels, restated with numpy on the
 host: the level's 27-slot ELL columns in colour order, one record per 128-row
-tile (27 bases, a word holding the offset width w, then 27 x 128 offsets of w
-bytes; the all-ones offset marks the zero sink). w is 1 where every tile's
-columns of each slot span at most 254, else 2 where they span at most 65534,
-else the level is not packed. The device builds the records in problem.cu
-(k_pack_cols) and decodes them in bulk.cuh (stage_col); the GPU tests check
-that the decoded columns give the same bits as the 32-bit ones and that each
-level gets the width predicted here (packed_width). Here: the encoding
-round-trips in both widths, the stencil's colour order keeps every tile's slot
-within one tile of rows where colour blocks fill whole tiles, and a matrix
-whose columns scatter does not pack."""
+tile (27 bases and a word holding the record's form w, then either 27 x 128
+offsets of w = 1 or 2 bytes, the all-ones offset marking the zero sink, or, for
+the diagonal form w = 3, 27 x 128 sink bits with column = base + row
+elsewhere). The diagonal form is taken where every tile's slots are diagonals,
+else w = 1 where every tile's columns of each slot span at most 254, else 2
+where they span at most 65534, else the level is not packed. The device builds
+the records in problem.cu (k_pack_cols, k_pack_cols_diag) and decodes them in
+bulk.cuh (stage_col); the GPU tests check that the decoded columns give the
+same bits as the 32-bit ones and that each level gets the form predicted here
+(packed_width). Here: the encodings round-trip, the stencil's colour order
+makes every tile's slot a diagonal where colour blocks fill whole tiles, and a
+matrix whose columns scatter does not pack."""
 import numpy as np
 import pytest
 
@@ -25,7 +27,7 @@ def max_span(w):
 
 
 def rec_bytes(w):
-    return 28 * 4 + 27 * ROWS * w
+    return 28 * 4 + (27 * 4 * 4 if w == 3 else 27 * ROWS * w)
 
 
 def colour_ell(binding, nx, ny, nz):
@@ -72,10 +74,37 @@ def unpack(base, off, sink, w=2):
     return c.transpose(1, 0, 2).reshape(27, -1)
 
 
-def packed_width(binding, nx, ny, nz):
-    """The offset width the library gives a single-rank level of this grid:
-    1, 2, or 0 (not packed)."""
+def pack_diag(cols, n, pitch, sink):
+    """The diagonal form: (bases [tiles][27], sink bits [tiles][27][4] uint32,
+    packs). A slot's base is column - row of its non-sink rows, which must agree."""
+    t = pitch // ROWS
+    c = np.where(np.arange(pitch) < n, cols, sink).reshape(27, t, ROWS).transpose(1, 0, 2)
+    real = c != sink
+    d = c - np.arange(ROWS)[None, None, :]
+    lo = np.where(real, d, np.iinfo(np.int64).max).min(axis=2)
+    hi = np.where(real, d, np.iinfo(np.int64).min).max(axis=2)
+    any_real = real.any(axis=2)
+    packs = bool(np.all(~any_real | (lo == hi)))
+    base = np.where(any_real, lo, 0)
+    sinks = (~real).reshape(t, 27, 4, 32)
+    bits = (sinks.astype(np.uint64) << np.arange(32, dtype=np.uint64)).sum(axis=3).astype(np.uint32)
+    return base.astype(np.int64), bits, packs
+
+
+def unpack_diag(base, bits, sink):
+    t = base.shape[0]
+    sinks = ((bits[:, :, :, None] >> np.arange(32, dtype=np.uint32)) & 1).reshape(t, 27, ROWS).astype(bool)
+    c = np.where(sinks, sink, base[:, :, None] + np.arange(ROWS)[None, None, :])
+    return c.transpose(1, 0, 2).reshape(27, -1)
+
+
+def packed_width(binding, nx, ny, nz, diagonal=True):
+    """The column form the library gives a single-rank level of this grid: 3
+    (diagonal), 1, 2 (offset bytes), or 0 (not packed); diagonal=False: as with
+    HPCG_B200_PACKED=8."""
     cols, n, pitch = colour_ell(binding, nx, ny, nz)
+    if diagonal and pack_diag(cols, n, pitch, n)[2]:
+        return 3
     for w in (1, 2):
         if pack(cols, n, pitch, n, w)[2]:
             return w
@@ -99,14 +128,30 @@ def test_stencil_columns_pack_and_round_trip(binding, dims, w):
     assert base.shape[0] * rec_bytes(w) == pitch // ROWS * (3568 if w == 1 else 7024)
 
 
-@pytest.mark.parametrize("dims,width", [((24, 24, 24), 2), ((48, 48, 48), 1), ((8, 8, 8), 2),
-                                        ((4, 4, 4), 1), ((12, 12, 12), 2), ((64, 32, 16), 1)])
-def test_width_follows_the_colour_blocks(binding, dims, width):
-    """8-bit offsets hold every level whose colour blocks fill whole 128-row
-    tiles (spans 127) and every level of at most 255 columns; a tile that
-    straddles two colour blocks spans the distance between their neighbour
-    colours, which at 24^3 or 8^3 needs 16 bits."""
-    assert packed_width(binding, *dims) == width
+@pytest.mark.parametrize("dims", [(16, 16, 16), (32, 32, 32), (16, 24, 40), (64, 64, 64)])
+def test_stencil_columns_are_tile_diagonals(binding, dims):
+    """Where every colour block is a whole number of tiles, each slot's columns
+    across a tile are one diagonal (column = base + row) apart from the sink:
+    the diagonal form holds them in 4.25 bytes a row and decodes every column."""
+    cols, n, pitch = colour_ell(binding, *dims)
+    base, bits, packs = pack_diag(cols, n, pitch, n)
+    assert packs
+    back = unpack_diag(base, bits, n)
+    assert np.array_equal(back[:, :n], cols[:, :n])
+    assert np.all(back[:, n:] == n)
+    assert base.shape[0] * rec_bytes(3) == pitch // ROWS * 544
+
+
+@pytest.mark.parametrize("dims,form,width", [((24, 24, 24), 2, 2), ((48, 48, 48), 3, 1), ((8, 8, 8), 2, 2),
+                                             ((4, 4, 4), 1, 1), ((12, 12, 12), 2, 2), ((64, 32, 16), 3, 1)])
+def test_form_follows_the_colour_blocks(binding, dims, form, width):
+    """The diagonal form holds every level whose colour blocks fill whole
+    128-row tiles; 8-bit offsets (the form without it) hold those and every
+    level of at most 255 columns; a tile that straddles two colour blocks spans
+    the distance between their neighbour colours, which at 24^3 or 8^3 needs
+    16 bits."""
+    assert packed_width(binding, *dims) == form
+    assert packed_width(binding, *dims, diagonal=False) == width
 
 
 def test_scattered_columns_do_not_pack(binding):
@@ -120,8 +165,10 @@ def test_scattered_columns_do_not_pack(binding):
     for w in (1, 2):
         _, _, packs, span = pack(far, n, pitch, n, w)
         assert not packs and span == n - 1
-    # a jump of 300 rows: too far for 8 bits, near enough for 16
+    assert not pack_diag(far, n, pitch, n)[2]
+    # a jump of 300 rows: off the diagonal, too far for 8 bits, near enough for 16
     near = cols.copy()
     near[14, 5] = cols[14, 5] + 300
+    assert not pack_diag(near, n, pitch, n)[2]
     assert pack(near, n, pitch, n, 1)[2] is False
     assert pack(near, n, pitch, n, 2)[2] is True
