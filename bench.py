@@ -338,7 +338,10 @@ def batched(dev, count=16, tol=1e-9, max_iter=2000):
             (it, _, _), t = timed(lib_stream, lambda: p.CG_mixed(b, x, max_iter, tol))
             iters_single.append(it)
             t_single += t
+        form = {0: "one launch per step, register phases", 1: "one launch per step, bulk-copy phases",
+                2: "one cooperative launch per iteration"}[bt.form()]
         return {"problems": count, "dims": dims, "tolerance": tol, "form": "FP64 flexible CG, FP32 V-cycle",
+                "iteration_form": form,
                 "batched": {"iters": [int(v) for v in ni], "seconds": round(t_batch, 4),
                             "solves_per_s": round(count / t_batch, 2),
                             "max_scaled_residual": float(np.max(nr / nr0))},

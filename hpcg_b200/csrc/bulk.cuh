@@ -129,6 +129,9 @@ struct BulkShape {
 #ifndef HB_BULK_RING
 #define HB_BULK_RING 2
 #endif
+#ifndef HB_SPMV_GATHER_FIRST
+#define HB_SPMV_GATHER_FIRST 0
+#endif
 #ifndef HB_SPMV_RING
 #define HB_SPMV_RING 2
 #endif

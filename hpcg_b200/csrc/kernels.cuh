@@ -526,12 +526,22 @@ __global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
         if (q >= n) return;
         T sum = (T)0;
         T xq = (T)0;
+#if HB_SPMV_GATHER_FIRST
+        // all 27 gathers issued before the first product (the same sum)
+        T xv[kSlots];
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) xv[k] = __ldg(x + stage_col<PW>(sc, k, t, sink));
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) sum += sv[k * kBulkRows + t] * xv[k];
+        xq = xv[kDiagSlot];
+#else
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
           const T xv = __ldg(x + stage_col<PW>(sc, k, t, sink));
           sum += sv[k * kBulkRows + t] * xv;
           if (k == kDiagSlot) xq = xv;
         }
+#endif
         y[q] = sum;
         if (DOT) acc += (double)xq * (double)sum;
       },

@@ -520,10 +520,17 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x, double* rt
 // partials measured about 12% slower than the plain ones at the same bytes
 // (0.8 ms per 512^3 iteration), more than a separate r'z pass over r and z
 // (2.1 GB), so the CG runs that pass instead (0.5 ms per iteration faster).
-// Read after tuning.
+// Read after tuning. Measurement knob HPCG_B200_RTZ: "fused" or "pass" forces
+// one way (colour mode with more than one level only).
 bool rtz_fused(const hpcg_b200_problem* P) {
   const Level& L = P->lev[0];
-  return P->symgs_mode == HPCG_B200_SYMGS_COLOUR && P->nlev > 1 && !(L.gs_sched == kBulkCfg && L.colp);
+  if (P->symgs_mode != HPCG_B200_SYMGS_COLOUR || P->nlev < 2) return false;
+  static const int force = [] {
+    const char* e = std::getenv("HPCG_B200_RTZ");
+    return !e ? 0 : std::strcmp(e, "fused") == 0 ? 1 : std::strcmp(e, "pass") == 0 ? 2 : 0;
+  }();
+  if (force) return force == 1;
+  return !(L.gs_sched == kBulkCfg && L.colp);
 }
 
 // Autotuner: per level, times each kernel configuration (load schedule x

@@ -14,8 +14,13 @@ and CG_ref.cpp:58-144).
   After it, the FP64 residuals differ in their last bits (dot products summed
   in another order) and a last-bit difference can flip the rounding of r to
   FP32 at the V-cycle's input: later iterations agree within FP32 rounding,
-  |d| <= 2^-23 * max(r, 1e-9) (measured up to 1.5e-8 relative); x within
-  1e-6 of max|x|.
+  |d| <= 2^-23 * max(r, 1e-9), checked at every iteration count whose scaled
+  residual is still at or above 1e-5 (measured up to 1.5e-8 relative there).
+  The difference then grows by about 1.75x per iteration (3.5e-4 relative at
+  iteration 30, scaled residual 2.4e-12): two runs of the form whose FP32
+  roundings of r differ follow trajectories that separate geometrically while
+  both converge. So beyond that point only the solutions are compared: x after
+  30 iterations within 1e-6 of max|x|.
 * Several right-hand sides (hpcg_b200_mg_multi / _cg_multi): each system's
   V-cycle bit for bit the oracle's V-cycle, each system's CG history within
   the same bound of the oracle's CG_ref, on U[-1,1] right-hand sides.
@@ -71,14 +76,18 @@ def test_mixed_cg_history_vs_oracle(oracle, binding, dims, rhs):
     K = 30
     xo, nio, _, _, hist = oracle.cg_mixed(PL, b[perms[0]], np.zeros(n), K, 0.0, skip=skip)
     assert nio == K
+    checked = [k for k in (1, 2, 3, 5, 8, 10, 12, 14) if hist[k] / hist[0] >= 1e-5]
+    assert len(checked) >= 5
     D = binding.Problem.generate(*dims)
     try:
-        for k in (1, 2, 5, 12, K):
+        for k in checked:
             x = np.zeros(n)
             ni, nr, nr0 = D.CG_mixed(b, x, k, 0.0)
             assert ni == k
             assert abs(nr0 - hist[0]) <= 1e-13 * hist[0]
             _mixed_close(k, nr / nr0, hist)
+        x = np.zeros(n)
+        assert D.CG_mixed(b, x, K, 0.0)[0] == K
         xn = _natural(xo, perms[0])
         assert np.max(np.abs(x - xn)) <= 1e-6 * max(np.max(np.abs(xn)), 1.0)
     finally:
@@ -131,6 +140,7 @@ def test_batched_vs_oracle(oracle, binding):
             for i, h in enumerate(hists):
                 assert ni[i] == k
                 assert abs(nr0[i] - h[0]) <= 1e-13 * h[0]
-                _mixed_close(k, nr[i] / nr0[i], h)
+                if h[k] / h[0] >= 1e-5:  # see the module docstring
+                    _mixed_close(k, nr[i] / nr0[i], h)
     finally:
         B.free()
