@@ -60,7 +60,34 @@ def parse():
                     help="with N > 1 GPUs: N independent problems instead of one decomposed problem")
     ap.add_argument("--decomposed", action="store_true",
                     help="run the decomposed (halo + allreduce) arm even on one GPU (a one-rank grid)")
+    ap.add_argument("--case", type=int, default=0, metavar="N",
+                    help="the small profiling case instead of the bench: an N^3 problem, two V-cycles and a "
+                         "3-iteration CG, every kernel launched on the stream (the ncu summaries in profiles/)")
     return ap.parse_args()
+
+
+def profile_case(n):
+    """The case the ncu summaries capture: a few launches of every kernel of a
+    CG iteration at n^3, launched one by one on the stream (kernels inside the
+    CG loop's graph cannot be captured by the profiler). Prints the tuned
+    configurations and each level's column form."""
+    os.environ.setdefault("HPCG_B200_GRAPH", "0")
+    import torch
+    from hpcg_b200 import binding as B
+    P = B.Problem.generate(n, n, n, 4, 0)
+    r = torch.rand(n ** 3, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    z = torch.zeros_like(r)
+    for _ in range(2):
+        P.ComputeMG(r, z)
+    b = torch.empty_like(r)
+    P.get_rhs(b)
+    x = torch.zeros_like(r)
+    P.CG(b, x, 3, 0.0, True)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": n, "configs": [P.level_config(l) for l in range(4)],
+                      "column_forms": [P.level_pack_width(l) for l in range(4)]}))
+    P.free()
+    return 0
 
 
 # ---------------------------------------------------------------------------
@@ -640,6 +667,7 @@ def b200_arm(args, rank, world, local_rank):
                 line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
     if line:
         line["config"]["autotuned"] = tuning
+        line["config"]["level_config"] = P.level_config_string()
     P.free()
     if dist:
         dist.barrier()
@@ -769,6 +797,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.case:
+        return profile_case(args.case)
     if args.impl == "reference":
         return reference_arm(args, rank)
     if (world > 1 and not args.replicas) or args.decomposed:

@@ -38,7 +38,7 @@ EXPORTS = (
     "hpcg_b200_export_level", "hpcg_b200_colour_permutation", "hpcg_b200_stream", "hpcg_b200_profile",
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
     "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
-    "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest",
+    "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest", "hpcg_b200_level_first_config",
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
@@ -108,6 +108,7 @@ def lib():
         l.hpcg_b200_batch_free.argtypes = [vp]
         l.hpcg_b200_batch_form.argtypes = [vp, C.POINTER(i)]
         l.hpcg_b200_grid_wait_selftest.argtypes = [i, d]
+        l.hpcg_b200_level_first_config.argtypes = [vp, i, vp, vp]
         l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
         l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
@@ -353,6 +354,26 @@ class Problem:
         _check(lib().hpcg_b200_level_config(self._h, level, out.ctypes.data), "hpcg_b200_level_config")
         keys = ("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned", "gs32_first")
         return dict(zip(keys, (int(v) for v in out)))
+
+    def level_first_config(self, level):
+        """The first sweep's configuration at each of the 8 sweep positions:
+        (fp64 list, fp32 list)."""
+        a = np.zeros(8, np.int32)
+        b = np.zeros(8, np.int32)
+        _check(lib().hpcg_b200_level_first_config(self._h, level, a.ctypes.data, b.ctypes.data),
+               "hpcg_b200_level_first_config")
+        return [int(v) for v in a], [int(v) for v in b]
+
+    def level_config_string(self):
+        """HPCG_B200_LEVEL_CONFIG that repeats this problem's tuned choices (the
+        first sweeps per sweep position)."""
+        parts = []
+        for lv in range(self.nlevels):
+            c = self.level_config(lv)
+            f64, f32 = self.level_first_config(lv)
+            parts.append(",".join([str(c["gs"]), "/".join(map(str, f64)), str(c["spmv"]), str(c["spmv_order"]),
+                                   str(c["gs32"]), "/".join(map(str, f32))]))
+        return ";".join(parts)
 
     def export_level(self, level):
         n, pitch, starts = self.level_info(level)

@@ -542,9 +542,13 @@ bool rtz_fused(const hpcg_b200_problem* P) {
 // Measurement knob HPCG_B200_LEVEL_CONFIG: the configurations of every level
 // given instead of tuned, "gs,gs_first,spmv,spmv_order,gs32,gs32_first" per
 // level, levels separated by ';' (a profiler run then uses the plain run's
-// choices: under a profiler the tuner's timings are not the real ones).
-// Fills v[6] for level l; false if the variable is unset or has no such level.
-bool level_config_override(int l, int v[6]) {
+// choices: under a profiler the tuner's timings are not the real ones). The
+// two first-sweep fields may list one configuration per sweep position,
+// separated by '/' (8 of them), as hpcg_b200_level_first_config reports them.
+// Fills v[6] and the per-position lists at64/at32 (-1: v[1] / v[5] at every
+// position) for level l; false if the variable is unset, malformed or has no
+// such level.
+bool level_config_override(int l, int v[6], int (&at64)[kColours], int (&at32)[kColours]) {
   const char* s = std::getenv("HPCG_B200_LEVEL_CONFIG");
   if (!s || !*s) return false;
   for (int i = 0; i < l; ++i) {
@@ -552,12 +556,25 @@ bool level_config_override(int l, int v[6]) {
     if (!s) return false;
     ++s;
   }
+  for (int p = 0; p < kColours; ++p) at64[p] = at32[p] = -1;
   for (int i = 0; i < 6; ++i) {
     char* end = nullptr;
     const long x = std::strtol(s, &end, 10);
     if (end == s) return false;
     v[i] = (int)x;
     s = end;
+    if ((i == 1 || i == 5) && *s == '/') {  // one configuration per sweep position
+      int* at = i == 1 ? at64 : at32;
+      at[0] = v[i];
+      for (int p = 1; p < kColours; ++p) {
+        if (*s != '/') return false;
+        ++s;
+        const long y = std::strtol(s, &end, 10);
+        if (end == s || y < 0 || y >= kGsConfigs) return false;
+        at[p] = (int)y;
+        s = end;
+      }
+    }
     if (i < 5) {
       if (*s != ',') return false;
       ++s;
@@ -600,12 +617,13 @@ int autotune(hpcg_b200_problem* P) {
     Level& L = P->lev[l];
     if (L.tuned) continue;
     L.tuned = true;
-    int ov[6];
-    if (level_config_override(l, ov)) {
+    int ov[6], at64[kColours], at32[kColours];
+    if (level_config_override(l, ov, at64, at32)) {
       L.gs_sched = ov[0];
       L.gs_first = ov[1];
       L.mv_sched = ov[2];
       L.mv_order = ov[3];
+      for (int s = 0; s < kColours; ++s) L.gs_first_at[s] = at64[s];
       continue;
     }
     if (force && *force) {
@@ -1020,10 +1038,11 @@ int ensure_f32(hpcg_b200_problem* P) {
       HB_CK(cudaMemsetAsync(L.x32, 0, sizeof(float) * L.pitch, c->stream));
       // FP32 phases load half the bytes per instruction: tune them on their own
       // (on the level's FP32 work vectors, which every V-cycle rewrites)
-      int ov[6];
-      if (level_config_override(l, ov)) {
+      int ov[6], at64[kColours], at32[kColours];
+      if (level_config_override(l, ov, at64, at32)) {
         L.gs_sched32 = ov[4];
         L.gs_first32 = ov[5];
+        for (int s = 0; s < kColours; ++s) L.gs_first32_at[s] = at32[s];
         continue;
       }
       const char* force = std::getenv("HPCG_B200_CONFIG");
@@ -1515,6 +1534,17 @@ int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config) {
   config[4] = L.mv_order;
   config[5] = L.tuned ? 1 : 0;
   config[6] = L.gs_first32;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_level_first_config(const hpcg_b200_problem* p, int level, int* fp64, int* fp32) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  const Level& L = p->lev[level];
+  for (int s = 0; s < kColours; ++s) {
+    if (fp64) fp64[s] = L.gs_first_at[s] >= 0 ? L.gs_first_at[s] : L.gs_first;
+    if (fp32) fp32[s] = L.gs_first32_at[s] >= 0 ? L.gs_first32_at[s] : L.gs_first32;
+  }
   return HPCG_B200_OK;
 }
 

@@ -308,6 +308,12 @@ int hpcg_b200_export_level(const hpcg_b200_problem* p, int level, int* new2old, 
  * configuration of the FP32 first-sweep phases. */
 int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config);
 
+/* The configuration of the first forward sweep's phase at each of the 8 sweep
+ * positions of one level (a phase reads 0 to 26 slots by its position, so the
+ * tuner chooses per position): fp64 for the FP64 V-cycle, fp32 for the FP32
+ * one (8 ints each, either may be NULL). */
+int hpcg_b200_level_first_config(const hpcg_b200_problem* p, int level, int* fp64, int* fp32);
+
 /* Check of the device-side bounded wait used by the bulk-copy Gauss-Seidel
  * phases (configuration 10): one thread waits `seconds` (0 < seconds <= 2) on
  * an mbarrier that nothing completes, gives up, records the fault and returns.

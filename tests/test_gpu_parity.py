@@ -209,6 +209,39 @@ def test_level_config_override_rejects_bad_values(binding, monkeypatch):
         D.free()
 
 
+def test_level_config_override_per_position(binding, monkeypatch):
+    """HPCG_B200_LEVEL_CONFIG's first-sweep fields may give one configuration
+    per sweep position; hpcg_b200_level_first_config reports them, and the
+    string the binding builds from a tuned problem sets the same choices."""
+    monkeypatch.setenv("HPCG_B200_LEVEL_CONFIG", "10,1/2/3/4/5/6/7/10,7,0,10,5;1,1,1,0,1,1;1,1,1,0,1,1;1,1,1,0,1,1")
+    D = binding.Problem.generate(32)
+    try:
+        x = np.zeros(32 ** 3)
+        D.ComputeMG(x, x.copy())
+        f64, f32 = D.level_first_config(0)
+        assert f64 == [1, 2, 3, 4, 5, 6, 7, 10]
+        assert D.level_config(0)["gs_first"] == 1 and D.level_first_config(1)[0] == [1] * 8
+    finally:
+        D.free()
+    monkeypatch.delenv("HPCG_B200_LEVEL_CONFIG")
+    T = binding.Problem.generate(32)
+    try:
+        y = np.zeros(32 ** 3)
+        T.ComputeMG(y, y.copy())
+        T.CG_mixed(y, y.copy(), 1, 0.0)
+        s = T.level_config_string()
+        monkeypatch.setenv("HPCG_B200_LEVEL_CONFIG", s)
+        R = binding.Problem.generate(32)
+        try:
+            R.ComputeMG(y, y.copy())
+            R.CG_mixed(y, y.copy(), 1, 0.0)
+            assert R.level_config_string() == s
+        finally:
+            R.free()
+    finally:
+        T.free()
+
+
 def test_spmv_matches_reference_golden(oracle, case16):
     P, D, _, _ = case16
     g = np.load(os.path.join(GOLD, "golden_16.npz"))
