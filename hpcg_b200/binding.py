@@ -39,6 +39,7 @@ EXPORTS = (
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
     "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
     "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest", "hpcg_b200_level_first_config",
+    "hpcg_b200_set_host_reuse",
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
@@ -109,6 +110,7 @@ def lib():
         l.hpcg_b200_batch_form.argtypes = [vp, C.POINTER(i)]
         l.hpcg_b200_grid_wait_selftest.argtypes = [i, d]
         l.hpcg_b200_level_first_config.argtypes = [vp, i, vp, vp]
+        l.hpcg_b200_set_host_reuse.argtypes = [vp, i]
         l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
         l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
@@ -354,6 +356,11 @@ class Problem:
         _check(lib().hpcg_b200_level_config(self._h, level, out.ctypes.data), "hpcg_b200_level_config")
         keys = ("gs", "gs_first", "gs32", "spmv", "spmv_order", "tuned", "gs32_first")
         return dict(zip(keys, (int(v) for v in out)))
+
+    def set_host_reuse(self, enable):
+        """hpcg_b200_set_host_reuse: whether CG may skip sending an unchanged
+        host b and a zero host x."""
+        _check(lib().hpcg_b200_set_host_reuse(self._h, int(bool(enable))), "hpcg_b200_set_host_reuse")
 
     def level_first_config(self, level):
         """The first sweep's configuration at each of the 8 sweep positions:

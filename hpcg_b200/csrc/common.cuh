@@ -245,6 +245,7 @@ struct hpcg_b200_problem {
   // and whether b still holds it (every other load into b clears the flag)
   double* b_kept_host;
   bool b_kept;
+  int host_reuse;  // hpcg_b200_cg may skip sending an unchanged b and a zero x (hpcg_b200_set_host_reuse)
 };
 
 namespace hb {

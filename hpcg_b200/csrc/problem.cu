@@ -40,6 +40,8 @@ hpcg_b200_problem* new_problem(int device, Context* c) {
   p->device = device;
   p->ctx = c;
   p->symgs_mode = HPCG_B200_SYMGS_COLOUR;
+  const char* reuse = std::getenv("HPCG_B200_HOST_REUSE");
+  p->host_reuse = reuse && reuse[0] == '0' ? 0 : 1;
   for (int l = 0; l < kMaxLevels; ++l) p->lev[l] = Level();
   return p;
 }
@@ -705,6 +707,13 @@ int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27
     L.col32 = nullptr;
     drop_coarse_graph(p, 1);  // it holds the old copy's addresses
   }
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_set_host_reuse(hpcg_b200_problem* p, int enable) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  p->host_reuse = enable != 0;
+  p->b_kept = false;
   return HPCG_B200_OK;
 }
 

@@ -1312,15 +1312,8 @@ int store_vector(hpcg_b200_problem* p, int level, const double* src, double* dst
 // bit for bit, against a host copy kept with the problem), and zeroes x on the
 // device when the host x is all zero bits, instead of sending it. Both checks
 // read host memory on several threads, which outruns a copy from pageable
-// memory. HPCG_B200_HOST_REUSE=0 sends both every call.
-
-bool host_reuse_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("HPCG_B200_HOST_REUSE");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
+// memory. hpcg_b200_set_host_reuse (or HPCG_B200_HOST_REUSE=0 at creation)
+// sends both every call.
 
 bool host_same_bits(const double* a, const double* b, int64_t n) {
   std::atomic<bool> same{true};
@@ -1353,7 +1346,7 @@ int load_cg_rhs(hpcg_b200_problem* p, const double* b) {
   bool dev = false;
   HB_TRY(locate_ptr(b, p->device, &dev, "b"));
   const int n = p->lev[0].n;
-  if (dev || !host_reuse_enabled()) return load_vector(p, 0, b, p->b);
+  if (dev || !p->host_reuse) return load_vector(p, 0, b, p->b);
   if (p->b_kept && host_same_bits(p->b_kept_host, b, n)) return HPCG_B200_OK;
   if (!p->b_kept_host) p->b_kept_host = new (std::nothrow) double[n];  // no host memory: send every call
   if (p->b_kept_host)
@@ -1369,7 +1362,7 @@ int load_cg_guess(hpcg_b200_problem* p, const double* x) {
   bool dev = false;
   HB_TRY(locate_ptr(x, p->device, &dev, "x"));
   const Level& L = p->lev[0];
-  if (!dev && host_reuse_enabled() && host_all_zero_bits(x, L.n)) {
+  if (!dev && p->host_reuse && host_all_zero_bits(x, L.n)) {
     HB_CK(cudaMemsetAsync(p->x, 0, sizeof(double) * L.pitch, p->ctx->stream));
     return HPCG_B200_OK;
   }

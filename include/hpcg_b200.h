@@ -96,6 +96,15 @@ int hpcg_b200_set_diagonal(hpcg_b200_problem* p, const double* diagonal);
  * present and ignored). */
 int hpcg_b200_set_values(hpcg_b200_problem* p, int level, const double* values27);
 
+/* Whether hpcg_b200_cg may skip moving its host inputs when it can tell they
+ * are unchanged (default on; HPCG_B200_HOST_REUSE=0 at creation turns it off):
+ * a host b equal bit for bit to the b it sent last is not sent again (compared
+ * on host threads against a copy the problem keeps), and an all-zero host x is
+ * zeroed on the device instead of sent. The reference's timed loop
+ * (src/main.cpp:334-340) passes the same b and a zeroed x to every set. No
+ * reference counterpart. */
+int hpcg_b200_set_host_reuse(hpcg_b200_problem* p, int enable);
+
 /* Selects the SYMGS ordering used by hpcg_b200_symgs / _mg / _cg. */
 int hpcg_b200_set_symgs_mode(hpcg_b200_problem* p, int mode);
 
