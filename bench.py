@@ -85,7 +85,8 @@ def profile_case(n):
     P.CG(b, x, 3, 0.0, True)
     torch.cuda.synchronize()
     print(json.dumps({"case": n, "configs": [P.level_config(l) for l in range(4)],
-                      "column_forms": [P.level_pack_width(l) for l in range(4)]}))
+                      "column_forms": [P.level_pack_width(l) for l in range(4)],
+                      "level_config": P.level_config_string()}))
     P.free()
     return 0
 
