@@ -663,7 +663,7 @@ def b200_arm(args, rank, world, local_rank):
                 "spmv_l0": round(sp_ms / (args.iters * args.steps), 3),
                 "restrict_l0": round(rs_ms / (args.iters * args.steps), 3),
                 "iteration": round(ms / (args.iters * args.steps), 3)},
-            "gpu_launches": gpu_launches_per_set(args.iters, rtz_pass=gs_packed) * args.steps,
+            "gpu_launches": gpu_launches_per_set(args.iters, rtz_pass=gs_packed and gs_pack != 3) * args.steps,
             "clocks": clk,
         }
         if e2e:

@@ -114,9 +114,11 @@ struct BulkShape {
 // few warps to cover that latency: with 8-bit offsets (31 KB FP64 stages,
 // 17 KB FP32 ones) measured at 512^3, three FP64 groups instead of two took a
 // phase from 0.93 to 0.80 ms and four FP32 groups instead of three from 11.4
-// to 10.0 ms per iteration (five: 10.2); a third SpMV group was slower (5.84
-// to 6.46 ms), so the SpMV keeps two. A shape whose stages do not fit (32-bit
-// columns) gets fewer groups.
+// to 10.0 ms per iteration (five: 10.2). With the diagonal form (28 KB FP64
+// stages), same box and run, a third SpMV group took the SpMV from 6.14 to
+// 5.52 ms and the restriction from 0.80 to 0.73 ms, while a fourth FP64 phase
+// group changed nothing. A shape whose stages do not fit (32-bit columns) gets
+// fewer groups.
 #ifndef HB_GS64_GROUPS
 #define HB_GS64_GROUPS 3
 #endif
@@ -124,7 +126,7 @@ struct BulkShape {
 #define HB_GS32_GROUPS 4
 #endif
 #ifndef HB_SPMV_GROUPS
-#define HB_SPMV_GROUPS 2
+#define HB_SPMV_GROUPS 3
 #endif
 #ifndef HB_BULK_RING
 #define HB_BULK_RING 2

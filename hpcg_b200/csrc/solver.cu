@@ -516,10 +516,12 @@ int mg_level(hpcg_b200_problem* p, int l, const double* r, double* x, double* rt
 // The CG's r'z comes out of the post-smoother (colour mode, more than one level).
 // r'z from the post-smoother's partials (CG.cpp:110/113 fused into the phase
 // that writes each colour's final value), except when level 0 runs the
-// bulk-copy phases on packed columns: there the phases that also write
-// partials measured about 12% slower than the plain ones at the same bytes
-// (0.8 ms per 512^3 iteration), more than a separate r'z pass over r and z
-// (2.1 GB), so the CG runs that pass instead (0.5 ms per iteration faster).
+// bulk-copy phases on 8- or 16-bit offset records: there the phases that also
+// write partials measured about 12% slower than the plain ones at the same
+// bytes (two consumer groups, 16-bit offsets: 0.8 ms per 512^3 iteration),
+// more than a separate r'z pass over r and z (2.1 GB), so the CG runs that
+// pass instead. With the diagonal form (three groups) the fused partials are
+// the faster way: 32.16 against 32.79 ms per 512^3 iteration, same box.
 // Read after tuning. Measurement knob HPCG_B200_RTZ: "fused" or "pass" forces
 // one way (colour mode with more than one level only).
 bool rtz_fused(const hpcg_b200_problem* P) {
@@ -530,7 +532,7 @@ bool rtz_fused(const hpcg_b200_problem* P) {
     return !e ? 0 : std::strcmp(e, "fused") == 0 ? 1 : std::strcmp(e, "pass") == 0 ? 2 : 0;
   }();
   if (force) return force == 1;
-  return !(L.gs_sched == kBulkCfg && L.colp);
+  return !(L.gs_sched == kBulkCfg && L.colp && L.pack != kPackDiag);
 }
 
 // Autotuner: per level, times each kernel configuration (load schedule x
