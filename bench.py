@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--decomposed", action="store_true",
                     help="run the decomposed (halo + allreduce) arm even on one GPU (a one-rank grid)")
     ap.add_argument("--case", type=int, default=0, metavar="N",
-                    help="the small profiling case instead of the bench: an N^3 problem, two V-cycles and a "
-                         "3-iteration CG, every kernel launched on the stream (the ncu summaries in profiles/)")
+                    help="the small profiling case instead of the bench: an N^3 problem, two V-cycles, a "
+                         "3-iteration CG and a 3-iteration CG around the FP32 V-cycle, every kernel launched on "
+                         "the stream (the ncu summaries in profiles/)")
     return ap.parse_args()
 
 
@@ -83,6 +84,8 @@ def profile_case(n):
     P.get_rhs(b)
     x = torch.zeros_like(r)
     P.CG(b, x, 3, 0.0, True)
+    x.zero_()
+    P.CG_mixed(b, x, 3, 0.0)
     torch.cuda.synchronize()
     print(json.dumps({"case": n, "configs": [P.level_config(l) for l in range(4)],
                       "column_forms": [P.level_pack_width(l) for l in range(4)],

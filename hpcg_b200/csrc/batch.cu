@@ -406,22 +406,24 @@ __global__ void __launch_bounds__(kThreads) k_b_finalize(BScal* sc, const double
 // problem computes the same bits as with one launch per step on the register
 // kernels.
 //
-// The barrier: a counter that only grows during a launch (the loop's condition
-// kernel zeroes it between launches). Every block's thread 0 adds its arrival
-// with a release reduction and waits until the counter reaches the number of
-// arrivals that barrier completes: barrier i of the launch waits for
-// (i + 1) x blocks. Each wait gives up after kBatchWaitNs of global time: it
-// records fault code 5 in the context's fault word and the block leaves the
-// kernel. A block that left stops arriving,
+// The barrier: every block's thread 0 reads the generation word, arrives on
+// the counter, and the last to arrive zeroes the counter and advances the
+// generation; the others wait for the generation to move. The two words sit on
+// separate 128-byte lines, so the waiting blocks' polls do not queue behind the
+// arrivals. Each wait gives up after kBatchWaitNs of global time: it records
+// fault code 5 in the context's fault word and the block leaves the kernel. A block that left stops arriving,
 // so every other block's next wait runs out too and the launch ends; the
 // loop's condition kernel reads the fault word and ends the loop, and the
 // host's stream synchronisation returns HPCG_B200_ERR_TIMEOUT.
 constexpr unsigned long long kBatchWaitNs = 1000000000ull;  // 1 s per wait
 
-// The barrier's state (device memory): arrivals so far in this launch.
+// The barrier's state (device memory): arrivals, and the generation on a line
+// of its own.
 struct BBar {
   unsigned count;
-  unsigned pad;
+  unsigned pad0[31];
+  unsigned gen;
+  unsigned pad1[31];
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -430,20 +432,23 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
-// true once the counter has reached `target` (every block of the grid has
-// arrived at this barrier); false if the wait gave up (the caller leaves the
-// kernel)
-__device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned target, unsigned* fault,
+// true once every one of the `expected` blocks has arrived; false if the wait
+// gave up (the caller leaves the kernel)
+__device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned expected, unsigned* fault,
                                              unsigned long long limit_ns = kBatchWaitNs) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
+    const unsigned g = ld_acquire_u32(&bar->gen);
     __threadfence();  // this block's writes are visible before its arrival
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&bar->count) : "memory");
-    if (ld_acquire_u32(&bar->count) < target) {
+    if (atomicAdd(&bar->count, 1u) + 1u == expected) {
+      bar->count = 0;  // nobody touches the counter until the generation moves
+      __threadfence();
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bar->gen), "r"(g + 1u) : "memory");
+    } else {
       const unsigned long long t0 = global_ns();
-      while (ld_acquire_u32(&bar->count) < target) {
+      while (ld_acquire_u32(&bar->gen) == g) {
         if (global_ns() - t0 > limit_ns) {
           record_fault(fault, 5);
           ok = 0;
@@ -486,11 +491,10 @@ struct BIter {
 // iteration() below, in one launch).
 __global__ void __launch_bounds__(kThreads) k_b_iteration(BIter a) {
   const unsigned nb = gridDim.x;
-  unsigned target = 0;  // arrivals that the next barrier completes
   if (*(volatile unsigned*)a.fault) return;  // an earlier launch gave up: do nothing
   if (!a.vcycle_only) {
     b_to32(a.vec, a.vtiles, a.nvt, a.sc);
-    if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+    if (!grid_barrier(a.bar, nb, a.fault)) return;
   }
   for (int i = 0; i < a.nsteps; ++i) {
     const DStep st = a.steps[i];
@@ -500,21 +504,21 @@ __global__ void __launch_bounds__(kThreads) k_b_iteration(BIter a) {
       b_restrict(a.res_items, a.tiles + st.tile_off, st.ntiles, a.sc);
     else
       b_prolong(a.res_items, a.tiles + st.tile_off, st.ntiles, a.sc);
-    if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+    if (!grid_barrier(a.bar, nb, a.fault)) return;
   }
   if (a.vcycle_only) return;
   b_to64_dots(a.vec, a.vtiles, a.nvt, a.sc, a.partials);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBRtz, a.ctl, a.m);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_update_p(a.vec, a.vtiles, a.nvt, a.sc, a.ctl);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_spmv<true>(a.vec, a.vtiles, a.nvt, 1, a.sc, a.partials);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBPap, a.ctl, a.m);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_update_xr(a.vec, a.vtiles, a.nvt, a.sc, a.partials);
-  if (!grid_barrier(a.bar, target += nb, a.fault)) return;
+  if (!grid_barrier(a.bar, nb, a.fault)) return;
   b_finalize(a.sc, a.partials, a.nvt, a.vrange, kBNormr, a.ctl, a.m);
 }
 
@@ -1027,7 +1031,10 @@ int hpcg_b200_batch_create(int count, const int* nx, const int* ny, const int* n
         cudaGetLastError();
         per_sm = 0;
       }
-      B->persist_grid = c->sms * std::min(per_sm, kBlocksPerSm);
+      // measurement knob HPCG_B200_BATCH_PERSIST_BLOCKS: resident blocks per SM
+      const char* pb = std::getenv("HPCG_B200_BATCH_PERSIST_BLOCKS");
+      const int want = pb && *pb ? std::atoi(pb) : kBlocksPerSm;
+      B->persist_grid = c->sms * std::max(0, std::min({per_sm, kBlocksPerSm, want}));
     }
     if (!st && cudaMallocHost(&B->sc_host, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_NOMEM;
     if (!st && cudaMemset(B->sc, 0, sizeof(BScal) * count) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
