@@ -543,7 +543,9 @@ def b200_arm(args, rank, world, local_rank):
     # with each level's column index as stored (8-bit or 16-bit offsets, or
     # 32-bit columns)
     packs = tuple(P.level_pack_width(l) for l in range(4))
-    bytes_iter = metrics.iteration_bytes(n, n, n, vb=8, pack=packs)
+    # r'z rides on the post-smoother except on 8-bit / 16-bit offset records
+    rtz_fused = not (P.level_config(0)["gs"] == 10 and packs[0] in (1, 2))
+    bytes_iter = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused)
     hbm_gbs = bytes_iter * args.iters * args.steps / (ms * 1e-3) / 1e9  # per GPU
 
     # end to end through the C ABI with pinned host vectors
@@ -596,7 +598,7 @@ def b200_arm(args, rank, world, local_rank):
         # the floor of the time ratio: the two forms' algorithmic bytes per
         # iteration (both bandwidth-bound at about the same efficiency)
         packs = tuple(P.level_pack_width(l) for l in range(4))
-        b64 = metrics.iteration_bytes(n, n, n, vb=8, pack=packs)
+        b64 = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused)
         b32 = metrics.iteration_bytes(n, n, n, vb=4, pack=packs)
         mixed["byte_floor_ratio"] = round(b32 / b64, 4)
         mixed["bytes_per_iter"] = {"fp64": b64, "fp32_vcycle": b32, "column_offset_bytes": list(packs)}

@@ -130,7 +130,7 @@ def first_sweep_bytes(rows, vb=8):
 
 
 
-def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False):
+def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False, rtz_fused=None):
     """Algorithmic HBM bytes of one CG iteration as this library runs it, kernel
     by kernel (the floor its kernels move when each streams its data once):
 
@@ -149,10 +149,12 @@ def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False)
     * post-smoother: 15 phases, 15/8 N_l F_l;
     * coarsest level: one symmetric sweep (first sweep + 7 phases);
     * top level, always FP64: the CG SpMV fused with p'Ap (spmv_bytes with
-      level 0's index) and the vector kernels: 80 B/row in the FP64 form
-      (r'z pass 16, p and x update 40, r update 24) and 96 B/row around the
-      FP32 V-cycle (z widened with both flexible dots 28, p and x update 40, r
-      update with r narrowed 28).
+      level 0's index) and the vector kernels: 64 B/row in the FP64 form
+      (p and x update 40, r update 24) plus 16 B/row for an r'z pass of its
+      own where the post-smoother does not accumulate r'z (level 0 on 8-bit
+      or 16-bit offset records; rtz_fused=None derives that from pack[0]),
+      and 96 B/row around the FP32 V-cycle (z widened with both flexible dots
+      28, p and x update 40, r update with r narrowed 28).
 
     With parts=True also returns the per-term split (GB)."""
     lv = level_sizes(nx, ny, nz, nlevels)
@@ -170,7 +172,9 @@ def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False)
         total += b
     n0 = lv[0][0]
     sp = spmv_bytes(n0, 8, pack[0])
-    vec = (80.0 if vb == 8 else 96.0) * n0
+    if rtz_fused is None:
+        rtz_fused = pack[0] not in (1, 2)
+    vec = (96.0 if vb != 8 else 64.0 if rtz_fused else 80.0) * n0
     split["spmv"] = sp / 1e9
     split["vectors"] = vec / 1e9
     total += sp + vec

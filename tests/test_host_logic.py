@@ -134,7 +134,8 @@ def test_flop_and_byte_models(oracle):
 def test_iteration_byte_model():
     """metrics.iteration_bytes, the floor the library's kernels move per CG
     iteration: the index width enters only through the bulk-copy kernels'
-    records (27.875 / 54.875 / 108 B per row), the FP32 V-cycle halves the
+    records (27.875 / 54.875 / 108 B per row; 4.25 for the diagonal form),
+    an r'z pass only where the post-smoother does not fuse it, the FP32 V-cycle halves the
     V-cycle's value and vector bytes but not the FP64 SpMV and CG vectors."""
     from hpcg_b200 import metrics
     assert metrics.index_bytes_per_row(1) == 27.875 and metrics.index_bytes_per_row(2) == 54.875
@@ -143,6 +144,10 @@ def test_iteration_byte_model():
     assert b[1] < b[2] < b[0]
     assert abs(b[2] / 1e9 - 232.97) < 0.01  # 16-bit offsets, every level
     assert abs(b[1] / 1e9 - 217.46) < 0.01  # 8-bit offsets, every level
+    # the diagonal form's post-smoother accumulates r'z: no 16 B/row pass of its own
+    d = metrics.iteration_bytes(512, 512, 512, 8, (3,) * 4)
+    assert abs(d / 1e9 - 201.74) < 0.01
+    assert metrics.iteration_bytes(512, 512, 512, 8, (3,) * 4, rtz_fused=False) - d == 16 * 512 ** 3
     t, parts = metrics.iteration_bytes(512, 512, 512, 4, (1,) * 4, parts=True)
     assert abs(sum(parts.values()) * 1e9 - t) < 1.0
     assert parts["spmv"] == metrics.spmv_bytes(512 ** 3, 8, 1) / 1e9 and parts["vectors"] == 96 * 512 ** 3 / 1e9
