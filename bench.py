@@ -698,14 +698,19 @@ def b200_arm(args, rank, world, local_rank):
     return 0
 
 
-def shard_launches_per_set(iters, nlevels=4):
-    """Kernels one rank launches for one sharded CG call (its own kernels only)."""
+def shard_launches_per_set(iters, nlevels=4, halo=True, rtz_fused=True):
+    """Kernels one rank launches for one sharded CG call (its own kernels only).
+    halo: the rank has neighbours (a halo pack before each exchange);
+    rtz_fused: r'z comes from the post-smoother (its store and the rank fold)
+    instead of a dot kernel of its own (dot, store, fold)."""
+    pack = 1 if halo else 0
     # per non-coarsest level: first sweep (15 phases), halo pack, restriction,
     # prolongation, halo pack, post sweep (15 phases); coarsest: 15 phases
-    per_mg = (15 + 1 + 1 + 1 + 1 + 15) * (nlevels - 1) + 15
-    # r'z (dot, store, rank fold), p update (k > 1), halo pack, SpMV + store + fold, x/r update + store + fold
-    per_iter = per_mg + 3 + 1 + 1 + 3 + 3
-    return iters * per_iter - 1 + 3 + (1 + 3)  # k = 1 copies; loads/stores; preamble pack + SpMV/residual/folds
+    per_mg = (15 + pack + 1 + 1 + pack + 15) * (nlevels - 1) + 15
+    # r'z, p update with the previous x update, halo pack, SpMV + store + fold, r update + store + fold
+    per_iter = per_mg + (2 if rtz_fused else 3) + 1 + pack + 3 + 3
+    # k = 1 copies p instead; the last x update; loads/stores; preamble pack + SpMV, residual, store, fold
+    return iters * per_iter - 1 + 1 + 3 + (pack + 4)
 
 
 def shard_arm(args, rank, world, local_rank):
@@ -782,8 +787,13 @@ def shard_arm(args, rank, world, local_rank):
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
-        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow)
+        gs_cfg = P.level_config(0)["gs"]
+        gs_pack = P.level_pack_width(0) if gs_cfg == 10 else 0
+        gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow, pack=gs_pack)
         achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
+        kernel = (f"k_gs_bulk<double,double,false> (level 0 of rank 0, configuration 10"
+                  f"{f', column form {gs_pack}' if gs_pack else ''})" if gs_cfg == 10 else
+                  f"k_gs_phase<double,double,false> (level 0 of rank 0, configuration {gs_cfg})")
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -797,9 +807,10 @@ def shard_arm(args, rank, world, local_rank):
             "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None, "traffic": None,
-                         "kernel": "k_gs_phase<double,double,false> (level 0, rank 0)",
+                         "kernel": kernel,
                          "peak_kind": peak_kind, "launches": gs_launch},
-            "gpu_launches": shard_launches_per_set(args.iters) * args.steps,
+            "gpu_launches": shard_launches_per_set(args.iters, halo=world > 1,
+                                                   rtz_fused=not (gs_cfg == 10 and gs_pack in (1, 2))) * args.steps,
             "clocks": clk,
         }
         if e2e:

@@ -768,19 +768,12 @@ __global__ void k_finalize_ranks(const double* __restrict__ vals, int nvals, int
   apply_fin(op, acc, 0.0, s, out);
 }
 
-// p = z + beta p (CG.cpp:115 as WAXPBY(1, z, beta, p)), beta from the device scalars.
-__global__ void __launch_bounds__(kThreads) k_update_p(int n, const double* __restrict__ z, double* p,
-                                                       const Scalars* __restrict__ s) {
-  const double beta = s->beta;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = z[i] + beta * p[i];
-}
-
-// p = z + beta p with the previous iteration's x update folded in: x = x +
-// alpha p (CG.cpp:121, alpha still the previous iteration's) reads the p that
-// this kernel reads anyway, so the x/r update that follows the SpMV need not
-// read p again. The same operations on the same values as k_update_p after
-// k_update_xr. first (iteration 1): p = z (CG.cpp:109), x untouched.
+// p = z + beta p (CG.cpp:115 as WAXPBY(1, z, beta, p)) with the previous
+// iteration's x update folded in: x = x + alpha p (CG.cpp:121, alpha still the
+// previous iteration's) reads the p that this kernel reads anyway, so the r
+// update that follows the SpMV need not read p. The same operations on the
+// same values as x = x + alpha p after the SpMV and p = z + beta p here.
+// first (iteration 1): p = z (CG.cpp:109), x untouched.
 __device__ __forceinline__ void update_px(int n, const double* __restrict__ z, double* p, double* x,
                                           const Scalars* __restrict__ s, bool first) {
   const double beta = s->beta, alpha = s->alpha;
@@ -850,23 +843,6 @@ __global__ void k_cg_setup(Scalars* s, int max_iter, double tol) {
     s->tol = tol;
     s->iter = 0;
   }
-}
-
-// x = x + alpha p; r = r + (-alpha) Ap (CG.cpp:121-122); partials of r'r (CG.cpp:123).
-__global__ void __launch_bounds__(kThreads) k_update_xr(int n, double* x, const double* __restrict__ p, double* r,
-                                                        const double* __restrict__ Ap, const Scalars* __restrict__ s,
-                                                        double* __restrict__ partials) {
-  const double alpha = s->alpha, malpha = -s->alpha;
-  const int stride = gridDim.x * blockDim.x;
-  double acc = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    x[i] = x[i] + alpha * p[i];
-    const double ri = r[i] + malpha * Ap[i];
-    r[i] = ri;
-    acc += ri * ri;
-  }
-  const double sum = block_sum(acc);
-  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
 }
 
 // Implicit adjoint, value part: with lambda solving A' lambda = dL/dx (A is

@@ -324,13 +324,13 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
     }
     HB_TRY(reduce(C, k == 1 ? kFinRtzFirst : kFinRtz));
     HB_TRY(timer.stop(part));
-    HB_TRY(timer.start(2, &part));  // p = z or p = z + beta p (:109 / :115)
+    HB_TRY(timer.start(2, &part));  // p = z or p = z + beta p (:109 / :115), with x of iteration k - 1
     for (int i = 0; i < nl; ++i) {
       const int n = C->ranks[i]->lev[0].n;
       if (k == 1) {
         HB_CK(cudaMemcpyAsync(ps[i], zs[i], sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));  // :109
       } else {
-        HB_TRY(launch_update_p(c, n, zs[i], ps[i]));  // :115
+        HB_TRY(launch_update_px(c, n, zs[i], ps[i], xs[i]));  // :115, and :121 of k - 1
       }
     }
     HB_TRY(timer.stop(part));
@@ -345,10 +345,10 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
     HB_TRY(timer.start(1, &part));  // pAp (:119)
     HB_TRY(reduce(C, kFinPap));  // alpha = rtz / pAp (:120)
     HB_TRY(timer.stop(part));
-    HB_TRY(timer.start(2, &part));  // x and r updates (:121-123), r'r partials with them
+    HB_TRY(timer.start(2, &part));  // r update (:122-123), r'r partials with it; x waits for the next p update
     for (int i = 0; i < nl; ++i) {
       hpcg_b200_problem* P = C->ranks[i];
-      HB_TRY(store_partial(C, i, launch_update_xr(c, P->lev[0].n, P->x, P->p, P->r, P->Ap)));  // :121-123
+      HB_TRY(store_partial(C, i, launch_update_r(c, P->lev[0].n, P->r, P->Ap)));  // :122-123
     }
     HB_TRY(timer.stop(part));
     HB_TRY(timer.start(1, &part));  // normr = sqrt(r'r) (:124)
@@ -357,6 +357,11 @@ int cg_ranks(Comm* C, int max_iter, double tol, bool prec, int* niters, double* 
     HB_TRY(read_scal(c));
     normr = std::sqrt(c->scal_host->normr2);
     *niters = k;
+  }
+  if (*niters > 0) {  // the last iteration's x update (:121)
+    HB_TRY(timer.start(2, &part));
+    for (int i = 0; i < nl; ++i) HB_TRY(launch_update_x(c, C->ranks[i]->lev[0].n, xs[i], ps[i]));
+    HB_TRY(timer.stop(part));
   }
   *normr_out = normr;
   *normr0_out = normr0;

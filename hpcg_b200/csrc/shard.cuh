@@ -56,8 +56,10 @@ int reduction_blocks(const Context* c, int64_t n);
 // written to c->partials (or a negative status)
 int launch_residual(Context* c, int n, const double* b, const double* Ap, double* r);  // r = b - Ap, r'r
 int launch_dot(Context* c, int n, const double* x, const double* y);                   // x'y
-int launch_update_p(Context* c, int n, const double* z, double* p);                    // p = z + beta p
-int launch_update_xr(Context* c, int n, double* x, const double* p, double* r, const double* Ap);  // x, r, r'r
+// x = x + alpha p with the previous iteration's alpha, then p = z + beta p
+int launch_update_px(Context* c, int n, const double* z, double* p, double* x);
+int launch_update_r(Context* c, int n, double* r, const double* Ap);  // r = r - alpha Ap, r'r
+int launch_update_x(Context* c, int n, double* x, const double* p);   // x = x + alpha p (after the loop)
 // k_finalize over c->partials / k_finalize_ranks over per-rank values
 int launch_finalize(Context* c, int nparts, int op, double* out);
 int launch_finalize_ranks(Context* c, const double* vals, int nvals, int op, double* out);

@@ -1246,17 +1246,23 @@ int launch_dot(Context* c, int n, const double* x, const double* y) {
   return e ? e : nb;
 }
 
-int launch_update_p(Context* c, int n, const double* z, double* p) {
-  k_update_p<<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, z, p, c->scal);
+int launch_update_px(Context* c, int n, const double* z, double* p, double* x) {
+  k_update_px<<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, z, p, x, c->scal);
   HB_CK(cudaGetLastError());
   return HPCG_B200_OK;
 }
 
-int launch_update_xr(Context* c, int n, double* x, const double* p, double* r, const double* Ap) {
+int launch_update_r(Context* c, int n, double* r, const double* Ap) {
   const int nb = red_blocks(c, n);
-  k_update_xr<<<nb, kThreads, 0, c->stream>>>(n, x, p, r, Ap, c->scal, c->partials);
-  const int e = neg_status("launch_update_xr");
+  k_update_r<<<nb, kThreads, 0, c->stream>>>(n, r, Ap, c->scal, c->partials);
+  const int e = neg_status("launch_update_r");
   return e ? e : nb;
+}
+
+int launch_update_x(Context* c, int n, double* x, const double* p) {
+  k_update_x<<<grid_for(c, n, kThreads, kPerSm), kThreads, 0, c->stream>>>(n, x, p, c->scal, 0);
+  HB_CK(cudaGetLastError());
+  return HPCG_B200_OK;
 }
 
 int launch_finalize(Context* c, int nparts, int op, double* out) {
