@@ -432,13 +432,17 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
                 "column_offset_bytes": pack}}
 
 
-def gpu_launches_per_set(iters, nlevels=4, rtz_pass=False):
+def gpu_launches_per_set(iters, nlevels=4, rtz_pass=False, wave=(0, 0, 0, 0)):
     """Kernels the library launches for one CG call (its own kernels only).
     rtz_pass: r'z runs as its own dot kernel (level 0 on the packed bulk-copy
-    phases) instead of coming out of the post-smoother."""
-    mg = 15 * 2 + 2  # per non-coarsest level: pre and post symmetric sweeps (15 colour phases each),
-    # residual-restriction, prolongation
-    per_mg = mg * (nlevels - 1) + 15
+    phases) instead of coming out of the post-smoother. wave[l]: level l runs
+    its sweeps from nonzero x as one wavefront launch each (the pre-smoother's
+    8 first-sweep phases, then 1 + 1 + 1 launches instead of 7 + 8 + 7)."""
+    def sweeps(l):
+        return 8 + 3 if l < len(wave) and wave[l] else 15 * 2
+    # per non-coarsest level: pre and post symmetric sweeps, residual-restriction, prolongation
+    coarsest = 8 + 1 if nlevels - 1 < len(wave) and wave[nlevels - 1] else 15  # one symmetric sweep from zero
+    per_mg = sum(sweeps(l) + 2 for l in range(nlevels - 1)) + coarsest
     # r'z finalize (its partials come out of the post-smoother, or out of a dot
     # kernel), p update with the previous iteration's x update (k > 1), SpMV +
     # finalize, r update + finalize
@@ -513,6 +517,7 @@ def b200_arm(args, rank, world, local_rank):
     sp_ms, sp_launch, sp_rows = B.profile_read(B.PROF_SPMV, dev)
     gf_ms, gf_launch, gf_rows = B.profile_read(B.PROF_GS_FIRST, dev)
     rs_ms, rs_launch, rs_rows = B.profile_read(B.PROF_RESTRICT, dev)
+    ws_ms, ws_launch, ws_rows = B.profile_read(B.PROF_GS_SWEEP, dev)
     B.profile(False, dev)
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
@@ -545,7 +550,8 @@ def b200_arm(args, rank, world, local_rank):
     packs = tuple(P.level_pack_width(l) for l in range(4))
     # r'z rides on the post-smoother except on 8-bit / 16-bit offset records
     rtz_fused = not (P.level_config(0)["gs"] == 10 and packs[0] in (1, 2))
-    bytes_iter = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused)
+    waves = tuple(P.level_wavefront(l) for l in range(4))
+    bytes_iter = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused, wave=waves)
     hbm_gbs = bytes_iter * args.iters * args.steps / (ms * 1e-3) / 1e9  # per GPU
 
     # end to end through the C ABI with pinned host vectors
@@ -598,7 +604,7 @@ def b200_arm(args, rank, world, local_rank):
         # the floor of the time ratio: the two forms' algorithmic bytes per
         # iteration (both bandwidth-bound at about the same efficiency)
         packs = tuple(P.level_pack_width(l) for l in range(4))
-        b64 = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused)
+        b64 = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused, wave=waves)
         b32 = metrics.iteration_bytes(n, n, n, vb=4, pack=packs)
         mixed["byte_floor_ratio"] = round(b32 / b64, 4)
         mixed["bytes_per_iter"] = {"fp64": b64, "fp32_vcycle": b32, "column_offset_bytes": list(packs)}
@@ -630,8 +636,25 @@ def b200_arm(args, rank, world, local_rank):
         tr = committed_traffic()
         traffic = None
         if (tr and tr.get("n") == n and tr.get("config") == gs_cfg and int(tr.get("pack", 0)) == gs_pack
-                and gs_launch):
+                and gs_launch and tr.get("form", "phase") == "phase"):
             traffic = tr.get("bytes_per_launch")
+        # level 0's sweeps as wavefront launches: then the dominant kernel
+        ws_bytes = metrics.wave_sweep_bytes(ws_rows, nrow, pack=pack0) if ws_launch else 0.0
+        wave_line = None
+        if ws_launch:
+            wave_line = {"launches": ws_launch, "avg_ms": round(ws_ms / ws_launch, 4),
+                         "gbs": round(ws_bytes / (ws_ms * 1e-3) / 1e9, 1) if ws_ms else None,
+                         "bytes_per_row": metrics.wave_sweep_bytes(nrow, nrow, pack=pack0) / nrow,
+                         "levels": list(waves)}
+        phase_ms = gs_ms  # the level-0 phases launched one by one (kernel_ms_per_iter)
+        if ws_launch and ws_ms > gs_ms:
+            gs_bytes, gs_ms, gs_launch = ws_bytes, ws_ms, ws_launch
+            achieved = ws_bytes / (ws_ms * 1e-3) / 1e9 if ws_ms > 0 else None
+            kernel = (f"k_gs_wave<double,{pack0}> (a whole level-0 sweep per launch, wavefront over z pairs, "
+                      f"column form {pack0})")
+            traffic = None
+            if (tr and tr.get("n") == n and tr.get("form") == "wave" and int(tr.get("pack", 0)) == pack0):
+                traffic = tr.get("bytes_per_launch")
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -663,14 +686,18 @@ def b200_arm(args, rank, world, local_rank):
                      if sp_ms else None, "column_offset_bytes": mv_pack},
             "first_sweep_gbs": round(metrics.first_sweep_bytes(gf_rows) / (gf_ms * 1e-3) / 1e9, 1) if gf_ms else None,
             "kernel_ms_per_iter": {
-                "gs_full_l0": round(gs_ms / (args.iters * args.steps), 3),
+                "gs_full_l0": round(phase_ms / (args.iters * args.steps), 3),
                 "gs_first_l0": round(gf_ms / (args.iters * args.steps), 3),
                 "spmv_l0": round(sp_ms / (args.iters * args.steps), 3),
                 "restrict_l0": round(rs_ms / (args.iters * args.steps), 3),
+                "gs_sweeps_l0": round(ws_ms / (args.iters * args.steps), 3) if wave_line else 0.0,
                 "iteration": round(ms / (args.iters * args.steps), 3)},
-            "gpu_launches": gpu_launches_per_set(args.iters, rtz_pass=gs_packed and gs_pack != 3) * args.steps,
+            "gpu_launches": gpu_launches_per_set(args.iters, rtz_pass=gs_packed and gs_pack != 3,
+                                                 wave=waves) * args.steps,
             "clocks": clk,
         }
+        if wave_line:
+            line["wavefront_sweeps"] = wave_line
         if e2e:
             line["e2e"] = e2e
         if mixed:

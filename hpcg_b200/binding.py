@@ -39,7 +39,7 @@ EXPORTS = (
     "hpcg_b200_profile_read", "hpcg_b200_dot_noalloc", "hpcg_b200_adjoint", "hpcg_b200_cg_multi", "hpcg_b200_mg_multi",
     "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
     "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest", "hpcg_b200_level_first_config",
-    "hpcg_b200_set_host_reuse",
+    "hpcg_b200_set_host_reuse", "hpcg_b200_level_wavefront", "hpcg_b200_wave_wait_selftest",
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
@@ -111,6 +111,8 @@ def lib():
         l.hpcg_b200_grid_wait_selftest.argtypes = [i, d]
         l.hpcg_b200_level_first_config.argtypes = [vp, i, vp, vp]
         l.hpcg_b200_set_host_reuse.argtypes = [vp, i]
+        l.hpcg_b200_level_wavefront.argtypes = [vp, i, C.POINTER(i)]
+        l.hpcg_b200_wave_wait_selftest.argtypes = [vp, d]
         l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
         l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
@@ -371,15 +373,26 @@ class Problem:
                "hpcg_b200_level_first_config")
         return [int(v) for v in a], [int(v) for v in b]
 
+    def level_wavefront(self, level):
+        """hpcg_b200_level_wavefront: 1 if the level's sweeps from nonzero x run
+        as one wavefront launch each, else 0."""
+        on = C.c_int(0)
+        _check(lib().hpcg_b200_level_wavefront(self._h, level, C.byref(on)), "hpcg_b200_level_wavefront")
+        return int(on.value)
+
+    def wave_wait_selftest(self, limit_seconds):
+        """hpcg_b200_wave_wait_selftest: the status code (not raised)."""
+        return int(lib().hpcg_b200_wave_wait_selftest(self._h, float(limit_seconds)))
+
     def level_config_string(self):
         """HPCG_B200_LEVEL_CONFIG that repeats this problem's tuned choices (the
-        first sweeps per sweep position)."""
+        first sweeps per sweep position, and the wavefront-sweep choice)."""
         parts = []
         for lv in range(self.nlevels):
             c = self.level_config(lv)
             f64, f32 = self.level_first_config(lv)
             parts.append(",".join([str(c["gs"]), "/".join(map(str, f64)), str(c["spmv"]), str(c["spmv_order"]),
-                                   str(c["gs32"]), "/".join(map(str, f32))]))
+                                   str(c["gs32"]), "/".join(map(str, f32)), str(self.level_wavefront(lv))]))
         return ";".join(parts)
 
     def export_level(self, level):
@@ -560,7 +573,7 @@ class Batch:
             pass
 
 
-PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT, PROF_GS32_FULL, PROF_GS32_FIRST = 0, 1, 2, 3, 4, 5
+PROF_GS_FULL, PROF_GS_FIRST, PROF_SPMV, PROF_RESTRICT, PROF_GS32_FULL, PROF_GS32_FIRST, PROF_GS_SWEEP = range(7)
 
 
 def stream(device=0):

@@ -426,9 +426,13 @@ struct BBar {
   unsigned pad1[31];
 };
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+// A load of the generation word from L2 without acquire semantics: an acquire
+// at GPU scope also discards the SM's L1 contents, and a block polling on an
+// SM where other blocks still work would take their cached lines away with
+// every poll. The waiter orders itself once, with the fence after the loop.
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
@@ -440,7 +444,7 @@ __device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned expected, unsig
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
-    const unsigned g = ld_acquire_u32(&bar->gen);
+    const unsigned g = ld_relaxed_u32(&bar->gen);  // cannot move before this block arrives
     __threadfence();  // this block's writes are visible before its arrival
     if (atomicAdd(&bar->count, 1u) + 1u == expected) {
       bar->count = 0;  // nobody touches the counter until the generation moves
@@ -449,7 +453,7 @@ __device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned expected, unsig
     } else {
       const unsigned long long t0 = global_ns();
       unsigned pause = 32;  // polls back off to one per ~0.5 us: fewer loads on the line while steps run
-      while (ld_acquire_u32(&bar->gen) == g) {
+      while (ld_relaxed_u32(&bar->gen) == g) {
         if (global_ns() - t0 > limit_ns) {
           record_fault(fault, 5);
           ok = 0;
@@ -459,7 +463,7 @@ __device__ __forceinline__ bool grid_barrier(BBar* bar, unsigned expected, unsig
         pause = pause < 512 ? pause * 2 : 512;
       }
     }
-    __threadfence();
+    __threadfence();  // with the load that saw the new generation: the other blocks' writes are visible
   }
   __syncthreads();
   return ok != 0;

@@ -101,8 +101,9 @@ struct BulkShape {
   static constexpr int col_bytes = PW == 0 ? kSlots * kBulkRows * (int)sizeof(int) : pack_rec(PW < 0 ? 2 : PW);
   static constexpr int tx_bytes = value_bytes + col_bytes;  // bytes landing in a stage per fill (PW >= 0)
   static constexpr int stage_bytes = (tx_bytes + 127) / 128 * 128;
-  // stages + barriers + slack to align the stages to 128 bytes (tensor copies)
-  static constexpr int smem = stages * stage_bytes + 2 * stages * (int)sizeof(uint64_t) + 128;
+  // stages + per stage two barriers and the tile's first row + slack to align
+  // the stages to 128 bytes (tensor copies)
+  static constexpr int smem = stages * stage_bytes + 3 * stages * (int)sizeof(uint64_t) + 128;
   static_assert(smem <= 227 * 1024, "shared memory of one block");
   static_assert(threads <= 1024, "threads of one block");
   static_assert(PW >= -1 && PW <= kPackDiag, "column form");
@@ -139,7 +140,7 @@ struct BulkShape {
 #endif
 template <typename T, int PW>
 __host__ __device__ constexpr int fit_groups(int want, int ring) {
-  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * ring * want + 16 * ring * want + 128 > 227 * 1024)
+  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * ring * want + 24 * ring * want + 128 > 227 * 1024)
     --want;
   return want;
 }
@@ -270,7 +271,9 @@ struct TileSrc {
 // every tile of its group, t its index in the group (row t / LANES of the tile,
 // lane t % LANES), with the tile's values sv[k * kBulkRows + row] and columns
 // on chip: sc[k * kBulkRows + row], or the packed record at sc
-// (stage_col<Shape::pack> reads any of them).
+// (stage_col<Shape::pack> reads any of them). The tile's first row q0 comes
+// from the producer through the stage (it computed src(tile) for the copies),
+// so the consumers' loads wait on no index arithmetic of their own.
 template <typename T, typename Shape, typename Src, typename Skip, typename RowFn>
 __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, RowFn row, unsigned* fault,
                                                const CUtensorMap* tm_val, const CUtensorMap* tm_col) {
@@ -284,6 +287,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
   unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * SB);
   uint64_t* empty = full + S;
+  int64_t* first = reinterpret_cast<int64_t*>(empty + S);  // q0 of the tile in each stage
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
@@ -321,6 +325,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
           record_fault(fault, 1);
           ok = 0;
         } else {
+          first[s] = ts.q0;  // released to the consumers by the arrival below
           mbar_expect_tx(&full[s], Shape::value_bytes + rec_bytes);
         }
       }
@@ -368,7 +373,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
           record_fault(fault, 3);
           break;
         }
-        row(tile, src(tile).q0, reinterpret_cast<const T*>(smem + s * SB),
+        row(tile, first[s], reinterpret_cast<const T*>(smem + s * SB),
             reinterpret_cast<const int*>(smem + s * SB + VB), t);
         mbar_arrive(&empty[s]);
       }

@@ -175,6 +175,8 @@ struct BulkMaps {
   bool ok = false;                // encoded (false: the encoder is unavailable)
 };
 
+struct WaveUnit;
+
 struct Level {
   ColourGrid g;
   int n = 0;                 // rows
@@ -217,6 +219,15 @@ struct Level {
   // 27 bases and offsets of `pack` bytes), nullptr (pack 0) if they do not pack
   unsigned char* colp = nullptr;
   int pack = 0;
+  // wavefront sweeps (wave.cuh): the unit tables of the forward and the
+  // backward sweep (device), their unit counts, tiles per unit, the per-unit
+  // counters of finished tiles; wf: the sweeps that do not start from x = 0
+  // run as one launch each (tuned, or HPCG_B200_WAVE)
+  WaveUnit* wf_unit[2] = {nullptr, nullptr};
+  int wf_units[2] = {0, 0};
+  int wf_tpu = 0;
+  unsigned* wf_done = nullptr;
+  int wf = 0;
 };
 
 struct Context;
@@ -304,7 +315,8 @@ enum ProfKind : int {
   kProfRestrict = 3, // residual + restriction, level 0 -> 1
   kProfGs32Full = 4,   // FP32 V-cycle: Gauss-Seidel colour phase on level 0, all 27 slots
   kProfGs32First = 5,  // FP32 V-cycle: first forward sweep on level 0
-  kProfKinds = 6,
+  kProfGsSweep = 6,    // a whole Gauss-Seidel sweep on level 0 in one launch (wave.cuh)
+  kProfKinds = 7,
 };
 
 struct Context {

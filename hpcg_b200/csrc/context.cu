@@ -262,8 +262,9 @@ int stream_sync(Context* c) {
   if (f && *f) {
     const unsigned code = *f;
     *f = 0;
-    set_error_text(code == 5 ? "a device-side wait gave up (bounded wait at the batched iteration's grid barrier)"
-                             : "a device-side wait gave up (bounded mbarrier wait of the bulk-copy pipeline)");
+    set_error_text(code == 5   ? "a device-side wait gave up (bounded wait at the batched iteration's grid barrier)"
+                   : code == 6 ? "a device-side wait gave up (bounded wait of a wavefront sweep on its dependencies)"
+                               : "a device-side wait gave up (bounded mbarrier wait of the bulk-copy pipeline)");
     return HPCG_B200_ERR_TIMEOUT;
   }
   return HPCG_B200_OK;

@@ -388,13 +388,15 @@ __global__ void __launch_bounds__(kThreads) k_gs_rows(const T* __restrict__ val,
 }
 
 // Storage row of the t-th row in slab order: z pair after z pair, inside a z
-// pair colour after colour (each one run of storage). Needs even grid dimensions.
+// pair colour after colour (each one run of storage). Needs even grid
+// dimensions. Rows are below 2^31, so the divisions are 32-bit ones.
 __device__ __forceinline__ int64_t slab_row(const ColourGrid& g, int64_t t) {
-  const int64_t per = (int64_t)(g.nx >> 1) * (g.ny >> 1);  // rows of one colour in one z pair
-  const int64_t h = t / (kColours * per);
-  const int64_t rem = t - h * kColours * per;
-  const int s = (int)(rem / per);
-  return g.start[s] + h * per + (rem - s * per);
+  const unsigned per = (unsigned)(g.nx >> 1) * (unsigned)(g.ny >> 1);  // rows of one colour in one z pair
+  const unsigned u = (unsigned)t;
+  const unsigned h = u / (kColours * per);
+  const unsigned rem = u - h * kColours * per;
+  const unsigned s = rem / per;
+  return g.start[s] + (int64_t)h * per + (rem - s * per);
 }
 
 // y = A x (ComputeSPMV_ref.cpp:61-70); DOT: also partials of x'y

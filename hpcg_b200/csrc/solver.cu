@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "kernels.cuh"
+#include "wave.cuh"
 
 namespace hb {
 
@@ -407,6 +408,139 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
   return prof_end(c, kind, ev0, r1 - r0);
 }
 
+// Unit tables of the wavefront sweeps of level L (wave.cuh), built once. A
+// level whose colour blocks do not cut into whole 128-row tiles per z pair
+// (odd sides, or (nx/2)(ny/2) not a multiple of 128) gets none (wf_tpu 0).
+// Phase j of a sweep runs `lag` z pairs behind phase j - 1 (2, or
+// HPCG_B200_WAVE_LAG): the units go in the order of h + lag * j.
+int ensure_wavefront(Level& L) {
+  if (L.wf_tpu > 0 || L.wf_units[0] < 0) return HPCG_B200_OK;
+  const ColourGrid& g = L.g;
+  const int64_t per = (int64_t)(g.nx / 2) * (g.ny / 2);
+  if (g.nx % 2 || g.ny % 2 || g.nz % 2 || per % kBulkRows || per == 0 || (int64_t)L.n != per * 4 * g.nz) {
+    L.wf_units[0] = -1;  // not eligible; not asked again
+    return HPCG_B200_OK;
+  }
+  static const int lag = [] {
+    const char* e = std::getenv("HPCG_B200_WAVE_LAG");
+    const int v = e && *e ? std::atoi(e) : 2;
+    return v < 1 ? 1 : v > 16 ? 16 : v;
+  }();
+  const int H = g.nz / 2, tpu = (int)(per / kBulkRows);
+  std::vector<WaveUnit> tab[2];
+  for (int dir = 0; dir < 2; ++dir) {
+    const int P = dir == 0 ? kColours : kColours - 1;  // the backward sweep skips the turn colour
+    std::vector<int> idx((size_t)P * H, -1);
+    for (int tau = 0; tau < H + lag * (P - 1); ++tau)
+      for (int j = 0; j < P; ++j) {
+        const int h = tau - lag * j;
+        if (h < 0 || h >= H) continue;
+        idx[(size_t)j * H + h] = (int)tab[dir].size();
+        WaveUnit u;
+        const int pos = dir == 0 ? j : kColours - 2 - j;  // sweep position of phase j
+        u.row0 = g.start[pos] + (int)(h * per);
+        u.dep[0] = u.dep[1] = u.dep[2] = -1;
+        u.dot = dir == 1 || j == P - 1;  // the phases that write each colour's final value
+        u.pad[0] = u.pad[1] = u.pad[2] = 0;
+        tab[dir].push_back(u);
+      }
+    for (int j = 1; j < P; ++j)
+      for (int h = 0; h < H; ++h) {
+        WaveUnit& u = tab[dir][idx[(size_t)j * H + h]];
+        int d = 0;
+        for (int hh = h - 1; hh <= h + 1; ++hh)
+          if (hh >= 0 && hh < H) u.dep[d++] = idx[(size_t)(j - 1) * H + hh];
+      }
+  }
+  for (int dir = 0; dir < 2; ++dir) {
+    const size_t bytes = sizeof(WaveUnit) * tab[dir].size();
+    HB_CK(cudaMalloc(&L.wf_unit[dir], bytes));
+    HB_CK(cudaMemcpy(L.wf_unit[dir], tab[dir].data(), bytes, cudaMemcpyHostToDevice));
+    L.wf_units[dir] = (int)tab[dir].size();
+  }
+  HB_CK(cudaMalloc(&L.wf_done, sizeof(unsigned) * L.wf_units[0]));
+  L.wf_tpu = tpu;
+  return HPCG_B200_OK;
+}
+
+// One whole sweep of level L (dir 0 forward, 1 backward; x entering nonzero)
+// as one cooperative launch of k_gs_wave. dot: as gs_colour's, the block
+// partials of the sweep's final-value rows (the caller's zeroed slots).
+// false: not launched (no tables, no tensor maps, or the launch was refused):
+// the caller runs the phases one by one.
+template <int PW>
+bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, int dir, double* dot,
+                   const WaveUnit* table = nullptr, int table_units = 0,
+                   unsigned long long limit_ns = kBulkWaitNs) {
+  const BulkMaps* m = bulk_maps(L);
+  if (!m) return false;
+  auto k = k_gs_wave<double, PW>;
+  using Shape = GsShape<double, PW>;
+  constexpr int smem = Shape::smem;
+  static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
+  bulk_attr(k, smem, c->device, &attr_set);
+  const int nunits = table ? table_units : L.wf_units[dir];
+  const int64_t ntiles = (int64_t)nunits * L.wf_tpu;
+  int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms);
+  if (dot && g > kDotStride) g = kDotStride;
+  if (cudaMemsetAsync(L.wf_done, 0, sizeof(unsigned) * nunits, c->stream) != cudaSuccess) {
+    set_error("wavefront counters", cudaGetLastError());
+    return false;
+  }
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(g);
+  cfg.blockDim = dim3(Shape::threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // every block resident: the sweep's waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, (const double*)L.val, cols_of<double>(L), L.pitch, rhs, x,
+                                           table ? table : (const WaveUnit*)L.wf_unit[dir], nunits, L.wf_tpu,
+                                           L.wf_done, dot, c->fault, m->val, m->col, (const unsigned char*)L.colp,
+                                           sink_of(L), limit_ns);
+  if (e != cudaSuccess) {
+    set_error("k_gs_wave", e);
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+bool wave_launch(Context* c, const Level& L, const double* rhs, double* x, int dir, double* dot) {
+  if (L.wf_tpu <= 0) return false;
+  if (L.pack == kPackDiag) return wave_launch_p<kPackDiag>(c, L, rhs, x, dir, dot);
+  if (L.pack == 1) return wave_launch_p<1>(c, L, rhs, x, dir, dot);
+  if (L.pack == 2) return wave_launch_p<2>(c, L, rhs, x, dir, dot);
+  return wave_launch_p<0>(c, L, rhs, x, dir, dot);
+}
+
+// A whole sweep as one wavefront launch, timed as kProfGsSweep on level 0.
+// false: not launched (see wave_launch).
+template <typename T, typename TR>
+bool wave_sweep(Context* c, const Level& L, const T* val, const TR* rhs, T* x, int dir, bool top, double* dot,
+                int* status) {
+  *status = HPCG_B200_OK;
+  if constexpr (sizeof(T) != 8 || sizeof(TR) != 8) {
+    return false;
+  } else {
+    if (!L.wf || L.wf_tpu <= 0 || val != L.val) return false;
+    const int kind = top ? kProfGsSweep : -1;
+    cudaEvent_t ev0 = nullptr;
+    if ((*status = prof_begin(c, kind, &ev0)) != HPCG_B200_OK) return true;
+    if (!wave_launch(c, L, rhs, x, dir, dot)) {
+      if (ev0) c->ev_pool.push_back(ev0);  // recorded around no launch: back to the pool, not timed
+      return false;
+    }
+    const int rows = L.wf_units[dir] * L.wf_tpu * kBulkRows;
+    *status = prof_end(c, kind, ev0, rows);
+    return true;
+  }
+}
+
 // One symmetric Gauss-Seidel step in colour order: forward over the sweep
 // positions, then backward. The last non-empty colour of the forward sweep is
 // not repeated at the start of the backward sweep: its rows read only other
@@ -416,18 +550,30 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
 // value (the last colour's forward phase, every other colour's backward phase)
 // also writes r'x block partials at dot + kDotStride * (sweep position); the
 // caller zeroes the kColours * kDotStride slots first.
+// With L.wf (FP64, whole-tile z pairs) each sweep that does not start from
+// x = 0 is one wavefront launch instead (wave.cuh: the same bits); its r'x
+// partials go to the slot of the forward sweep's last position, or of
+// position 0 for the backward sweep.
 template <typename T, typename TR>
 int gs_colour(Context* c, const Level& L, const T* val, const TR* rhs, T* x, bool first, bool top,
               double* dot = nullptr) {
   int last = -1;
   for (int s = 0; s < kColours; ++s)
     if (L.g.start[s + 1] > L.g.start[s]) last = s;
-  for (int s = 0; s < kColours; ++s)
-    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, first, top,
-                                dot && !first && s == last ? dot + (int64_t)kDotStride * s : nullptr)));
-  for (int s = last - 1; s >= 0; --s)
-    HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, false, top, dot ? dot + (int64_t)kDotStride * s : nullptr)));
-  return HPCG_B200_OK;
+  int st = HPCG_B200_OK;
+  if (first || !wave_sweep<T, TR>(c, L, val, rhs, x, 0, top, dot ? dot + (int64_t)kDotStride * last : nullptr, &st)) {
+    HB_TRY(st);
+    for (int s = 0; s < kColours; ++s)
+      HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, first, top,
+                                  dot && !first && s == last ? dot + (int64_t)kDotStride * s : nullptr)));
+  }
+  HB_TRY(st);
+  if (!wave_sweep<T, TR>(c, L, val, rhs, x, 1, top, dot, &st)) {
+    HB_TRY(st);
+    for (int s = last - 1; s >= 0; --s)
+      HB_TRY((launch_phase<T, TR>(c, L, val, rhs, x, s, false, top, dot ? dot + (int64_t)kDotStride * s : nullptr)));
+  }
+  return st;
 }
 
 // Wavefronts ix + 2 iy + 4 iz: every lower neighbour (in the reference's natural
@@ -547,10 +693,12 @@ bool rtz_fused(const hpcg_b200_problem* P) {
 // choices: under a profiler the tuner's timings are not the real ones). The
 // two first-sweep fields may list one configuration per sweep position,
 // separated by '/' (8 of them), as hpcg_b200_level_first_config reports them.
-// Fills v[6] and the per-position lists at64/at32 (-1: v[1] / v[5] at every
-// position) for level l; false if the variable is unset, malformed or has no
-// such level.
-bool level_config_override(int l, int v[6], int (&at64)[kColours], int (&at32)[kColours]) {
+// An optional seventh field, 0 or 1, is the level's wavefront-sweep choice
+// (hpcg_b200_level_wavefront). Fills v[6], *wf (-1 if absent) and the
+// per-position lists at64/at32 (-1: v[1] / v[5] at every position) for level
+// l; false if the variable is unset, malformed or has no such level.
+bool level_config_override(int l, int v[6], int* wf, int (&at64)[kColours], int (&at32)[kColours]) {
+  *wf = -1;
   const char* s = std::getenv("HPCG_B200_LEVEL_CONFIG");
   if (!s || !*s) return false;
   for (int i = 0; i < l; ++i) {
@@ -585,7 +733,23 @@ bool level_config_override(int l, int v[6], int (&at64)[kColours], int (&at32)[k
   const int lim[6] = {kGsConfigs, kGsConfigs, kConfigs, 3, kGsConfigs, kGsConfigs};
   for (int i = 0; i < 6; ++i)
     if (v[i] < 0 || v[i] >= lim[i]) return false;
+  if (*s == ',') {
+    char* end = nullptr;
+    const long y = std::strtol(s + 1, &end, 10);
+    if (end == s + 1 || (y != 0 && y != 1)) return false;
+    *wf = (int)y;
+  }
   return true;
+}
+
+// HPCG_B200_WAVE: "0" never runs a sweep as one wavefront launch, "1" does so
+// wherever the level allows it; unset: the autotuner times both.
+int wave_force() {
+  static const int f = [] {
+    const char* e = std::getenv("HPCG_B200_WAVE");
+    return !e || !*e ? -1 : e[0] == '0' ? 0 : 1;
+  }();
+  return f;
 }
 
 // The first-sweep choice from per-position timings t[s][cfg]: the fastest
@@ -619,13 +783,16 @@ int autotune(hpcg_b200_problem* P) {
     Level& L = P->lev[l];
     if (L.tuned) continue;
     L.tuned = true;
-    int ov[6], at64[kColours], at32[kColours];
-    if (level_config_override(l, ov, at64, at32)) {
+    int ov[6], at64[kColours], at32[kColours], wf = -1;
+    if (level_config_override(l, ov, &wf, at64, at32)) {
       L.gs_sched = ov[0];
       L.gs_first = ov[1];
       L.mv_sched = ov[2];
       L.mv_order = ov[3];
       for (int s = 0; s < kColours; ++s) L.gs_first_at[s] = at64[s];
+      if (wf < 0) wf = wave_force() > 0 ? 1 : 0;
+      if (wf) HB_TRY(ensure_wavefront(L));
+      L.wf = wf && L.wf_tpu > 0 ? 1 : 0;
       continue;
     }
     if (force && *force) {
@@ -696,6 +863,21 @@ int autotune(hpcg_b200_problem* P) {
     pick_first(t_first, L.gs_first_at, &L.gs_first);
     const char* fo = std::getenv("HPCG_B200_SPMV_ORDER");  // measurement: force the SpMV row order
     if (fo && *fo) L.mv_order = std::atoi(fo);
+    // the sweeps as wavefront launches (wave.cuh) or phase by phase: a whole
+    // symmetric step from nonzero x each way, round-robin
+    L.wf = 0;
+    if (wave_force() != 0) HB_TRY(ensure_wavefront(L));
+    if (L.wf_tpu > 0 && wave_force() > 0) {
+      L.wf = 1;
+    } else if (L.wf_tpu > 0 && wave_force() < 0) {
+      float t_wf[2] = {1e30f, 1e30f};
+      for (int rep = 0; rep < 3; ++rep)
+        for (int w = 0; w < 2; ++w) {
+          L.wf = w;
+          HB_TRY(time_it(t_wf[w], [&] { gs_colour<double, double>(c, L, L.val, rs, xs, false, false); }));
+        }
+      L.wf = t_wf[1] < t_wf[0] ? 1 : 0;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     HB_CK(cudaGetLastError());
@@ -1040,8 +1222,8 @@ int ensure_f32(hpcg_b200_problem* P) {
       HB_CK(cudaMemsetAsync(L.x32, 0, sizeof(float) * L.pitch, c->stream));
       // FP32 phases load half the bytes per instruction: tune them on their own
       // (on the level's FP32 work vectors, which every V-cycle rewrites)
-      int ov[6], at64[kColours], at32[kColours];
-      if (level_config_override(l, ov, at64, at32)) {
+      int ov[6], at64[kColours], at32[kColours], wf = -1;
+      if (level_config_override(l, ov, &wf, at64, at32)) {
         L.gs_sched32 = ov[4];
         L.gs_first32 = ov[5];
         for (int s = 0; s < kColours; ++s) L.gs_first32_at[s] = at32[s];
@@ -1535,6 +1717,51 @@ int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config) {
   config[4] = L.mv_order;
   config[5] = L.tuned ? 1 : 0;
   config[6] = L.gs_first32;
+  return HPCG_B200_OK;
+}
+
+int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!(limit_seconds > 0.0) || limit_seconds > 10.0) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  Context* c = p->ctx;
+  Level& L = p->lev[0];
+  HB_TRY(ensure_wavefront(L));
+  if (L.wf_tpu <= 0) return HPCG_B200_ERR_UNSUPPORTED;
+  // one unit that waits for itself: its counter cannot fill before its own
+  // tiles are released, so the producer's dependency wait runs out
+  WaveUnit u;
+  u.row0 = L.g.start[0];
+  u.dep[0] = 0;
+  u.dep[1] = u.dep[2] = -1;
+  u.dot = 0;
+  u.pad[0] = u.pad[1] = u.pad[2] = 0;
+  WaveUnit* d = nullptr;
+  HB_CK(cudaMalloc(&d, sizeof(WaveUnit)));
+  int st = HPCG_B200_OK;
+  if (cudaMemcpy(d, &u, sizeof(u), cudaMemcpyHostToDevice) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  // x: scratch (Ap); the unit's tiles are never released, so nothing is written
+  const unsigned long long lim = (unsigned long long)(limit_seconds * 1e9);
+  bool launched = false;
+  if (st == HPCG_B200_OK) {
+    if (L.pack == kPackDiag)
+      launched = wave_launch_p<kPackDiag>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
+    else if (L.pack == 1)
+      launched = wave_launch_p<1>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
+    else if (L.pack == 2)
+      launched = wave_launch_p<2>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
+    else
+      launched = wave_launch_p<0>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
+    st = launched ? stream_sync(c) : HPCG_B200_ERR_UNSUPPORTED;
+  }
+  cudaFree(d);
+  return st;
+}
+
+int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!on || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  *on = p->lev[level].wf;
   return HPCG_B200_OK;
 }
 

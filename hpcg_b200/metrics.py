@@ -113,6 +113,17 @@ def gs_phase_bytes(rows_in_phase, rows_in_level, vb=8, pack=0):
     return rows_in_phase * per_row + 7.0 * rows_in_phase * vb
 
 
+def wave_sweep_bytes(rows_updated, rows_in_level, vb=8, pack=0):
+    """Algorithmic bytes of Gauss-Seidel sweeps run as wavefront launches that
+    together updated `rows_updated` rows, each launch a whole sweep of a level
+    of `rows_in_level` rows (`rows_updated` / `rows_in_level` launches, rounded
+    up: a backward sweep updates 7/8 of the rows): per updated row the 27 slots,
+    the right-hand side read and x written; x read from DRAM once per sweep
+    (the other colours' x stays in L2 between the phases of the wavefront)."""
+    sweeps = -(-int(rows_updated) // int(rows_in_level)) if rows_in_level else 0
+    return rows_updated * (SLOTS * vb + index_bytes_per_row(pack) + 2 * vb) + sweeps * rows_in_level * vb
+
+
 def spmv_bytes(rows, vb=8, pack=0):
     """Algorithmic bytes of y = A x over `rows` rows: 27 values and column
     indices, x read once, y written."""
@@ -130,7 +141,8 @@ def first_sweep_bytes(rows, vb=8):
 
 
 
-def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False, rtz_fused=None):
+def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False, rtz_fused=None,
+                    wave=(0, 0, 0, 0)):
     """Algorithmic HBM bytes of one CG iteration as this library runs it, kernel
     by kernel (the floor its kernels move when each streams its data once):
 
@@ -156,6 +168,11 @@ def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False,
       and 96 B/row around the FP32 V-cycle (z widened with both flexible dots
       28, p and x update 40, r update with r narrowed 28).
 
+    Levels with wave[l] set run the sweeps that start from nonzero x (the
+    pre-smoother's backward sweep, both post-smoother sweeps) as wavefront
+    launches: per sweep the updated rows' 29 vb + I_l and x read once, N_l vb,
+    instead of 36 vb + I_l per updated row.
+
     With parts=True also returns the per-term split (GB)."""
     lv = level_sizes(nx, ny, nz, nlevels)
     split = {}
@@ -163,11 +180,14 @@ def iteration_bytes(nx, ny, nz, vb=8, pack=(1, 1, 1, 1), nlevels=4, parts=False,
     for l, (n_l, _) in enumerate(lv):
         ib = index_bytes_per_row(pack[l])
         full = 36.0 * vb + ib
-        b = first_sweep_bytes(n_l, vb) + 7.0 / 8.0 * n_l * full
+        wl = l < len(wave) and wave[l]
+        # a sweep that starts from nonzero x and updates the fraction f of the rows
+        sweep = (lambda f: f * n_l * (29.0 * vb + ib) + n_l * vb) if wl else (lambda f: f * n_l * full)
+        b = first_sweep_bytes(n_l, vb) + sweep(7.0 / 8.0)
         if l < nlevels - 1:
             b += n_l / 8.0 * (27.0 * vb + ib + 2.0 * vb + 4.0) + n_l * vb
             b += n_l / 8.0 * (8.0 + 3.0 * vb)
-            b += 15.0 / 8.0 * n_l * full
+            b += sweep(1.0) + sweep(7.0 / 8.0)
         split[f"level{l}"] = b / 1e9
         total += b
     n0 = lv[0][0]

@@ -323,6 +323,24 @@ int hpcg_b200_level_config(const hpcg_b200_problem* p, int level, int* config);
  * one (8 ints each, either may be NULL). */
 int hpcg_b200_level_first_config(const hpcg_b200_problem* p, int level, int* fp64, int* fp32);
 
+/* Whether the level runs each FP64 Gauss-Seidel sweep that starts from a
+ * nonzero x (all but the pre-smoother's first) as one wavefront launch: a
+ * cooperative kernel in which phase j of the sweep follows phase j - 1 two z
+ * pairs behind, so the neighbours' x stays in L2 across the phases; the same
+ * bits as the phases launched one by one. Chosen by the autotuner (both timed;
+ * HPCG_B200_WAVE=0 or 1 forces it) where the level's sides are even and each
+ * colour of a z pair fills whole 128-row tiles; *on receives 0 or 1. */
+int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on);
+
+/* Check of the wavefront sweep's bounded dependency wait: launches the sweep
+ * kernel on level 0 with one unit that waits for itself, so every block's wait
+ * runs out after limit_seconds (0 < limit <= 10); the blocks then release
+ * what they hold and leave. Returns HPCG_B200_ERR_TIMEOUT with the wavefront
+ * message in hpcg_b200_last_error when the wait gave up and the context is
+ * still usable, HPCG_B200_ERR_UNSUPPORTED where level 0 has no wavefront
+ * tables. Writes only the problem's scratch vector Ap. */
+int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds);
+
 /* Check of the device-side bounded wait used by the bulk-copy Gauss-Seidel
  * phases (configuration 10): one thread waits `seconds` (0 < seconds <= 2) on
  * an mbarrier that nothing completes, gives up, records the fault and returns.
@@ -349,13 +367,15 @@ void* hpcg_b200_stream(int device);
  * of the timed kernel classes; enabling resets the totals. Kinds:
  * 0 Gauss-Seidel colour phase on level 0 (all slots), 1 first forward sweep on
  * level 0, 2 CG SpMV on level 0, 3 residual+restriction from level 0, 4 and 5
- * the same two phase kinds of the FP32 V-cycle. */
+ * the same two phase kinds of the FP32 V-cycle, 6 a whole sweep on level 0 in
+ * one wavefront launch (rows: the rows it updates). */
 #define HPCG_B200_PROF_GS_FULL 0
 #define HPCG_B200_PROF_GS_FIRST 1
 #define HPCG_B200_PROF_SPMV 2
 #define HPCG_B200_PROF_RESTRICT 3
 #define HPCG_B200_PROF_GS32_FULL 4   /* FP32 V-cycle (hpcg_b200_cg_mixed): colour phase on level 0 */
 #define HPCG_B200_PROF_GS32_FIRST 5  /* FP32 V-cycle: first forward sweep on level 0 */
+#define HPCG_B200_PROF_GS_SWEEP 6    /* one-launch wavefront sweep on level 0 (forward or backward) */
 int hpcg_b200_profile(int device, int enable);
 int hpcg_b200_profile_read(int device, int kind, double* total_ms, int64_t* launches, int64_t* rows);
 
