@@ -175,7 +175,17 @@ struct BulkMaps {
   bool ok = false;                // encoded (false: the encoder is unavailable)
 };
 
-struct WaveUnit;
+// The shape of one wavefront sweep of a level (wave.cuh).
+struct WaveGeom {
+  int H;         // z pairs
+  int P;         // phases of the sweep (8 forward, 7 backward)
+  int lag;       // z pairs between consecutive phases
+  int tpu;       // tiles per unit: (nx/2)(ny/2) / kBulkRows
+  int per;       // rows per unit: (nx/2)(ny/2)
+  int dot_from;  // phases j >= dot_from add r'x to the partials (P: none)
+  int self_dep;  // >= 0: every unit waits for this virtual unit (the bounded-wait check); -1 normally
+  int start[kColours];  // first row of phase j's colour block
+};
 
 struct Level {
   ColourGrid g;
@@ -219,12 +229,12 @@ struct Level {
   // 27 bases and offsets of `pack` bytes), nullptr (pack 0) if they do not pack
   unsigned char* colp = nullptr;
   int pack = 0;
-  // wavefront sweeps (wave.cuh): the unit tables of the forward and the
-  // backward sweep (device), their unit counts, tiles per unit, the per-unit
-  // counters of finished tiles; wf: the sweeps that do not start from x = 0
-  // run as one launch each (tuned, or HPCG_B200_WAVE)
-  WaveUnit* wf_unit[2] = {nullptr, nullptr};
-  int wf_units[2] = {0, 0};
+  // wavefront sweeps (wave.cuh): the geometry of the forward and the backward
+  // sweep, tiles per unit (0: not set up yet, -1: the level does not cut into
+  // whole-tile units), the per-unit counters of finished tiles (device); wf:
+  // the sweeps that do not start from x = 0 run as one launch each (tuned, or
+  // HPCG_B200_WAVE)
+  WaveGeom wf_geom[2] = {};
   int wf_tpu = 0;
   unsigned* wf_done = nullptr;
   int wf = 0;

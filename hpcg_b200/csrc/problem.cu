@@ -370,7 +370,7 @@ int free_problem(hpcg_b200_problem* p) {
   for (int l = 0; l < kMaxLevels; ++l) {
     Level& L = p->lev[l];
     void* ptrs[] = {L.val, L.col, L.val32, L.col32, L.new2old, L.old2new, L.f2c, L.tf, L.tq, L.r, L.x, L.r32, L.x32,
-                    L.wave_rows, L.colp, L.wf_unit[0], L.wf_unit[1], L.wf_done};
+                    L.wave_rows, L.colp, L.wf_done};
     for (void* q : ptrs) dev_free(q);
     delete[] L.wave_start;
     delete L.maps;

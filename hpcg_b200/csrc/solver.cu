@@ -408,17 +408,17 @@ int launch_phase(Context* c, const Level& L, const T* val, const TR* rhs, T* x, 
   return prof_end(c, kind, ev0, r1 - r0);
 }
 
-// Unit tables of the wavefront sweeps of level L (wave.cuh), built once. A
-// level whose colour blocks do not cut into whole 128-row tiles per z pair
-// (odd sides, or (nx/2)(ny/2) not a multiple of 128) gets none (wf_tpu 0).
-// Phase j of a sweep runs `lag` z pairs behind phase j - 1 (2, or
-// HPCG_B200_WAVE_LAG): the units go in the order of h + lag * j.
+// The wavefront sweeps of level L (wave.cuh): their geometry and the per-unit
+// counters, set up once. A level whose colour blocks do not cut into whole
+// 128-row tiles per z pair (odd sides, or (nx/2)(ny/2) not a multiple of 128)
+// gets none (wf_tpu stays 0). Phase j of a sweep runs `lag` z pairs behind
+// phase j - 1 (2, or HPCG_B200_WAVE_LAG).
 int ensure_wavefront(Level& L) {
-  if (L.wf_tpu > 0 || L.wf_units[0] < 0) return HPCG_B200_OK;
+  if (L.wf_tpu != 0) return HPCG_B200_OK;
   const ColourGrid& g = L.g;
   const int64_t per = (int64_t)(g.nx / 2) * (g.ny / 2);
   if (g.nx % 2 || g.ny % 2 || g.nz % 2 || per % kBulkRows || per == 0 || (int64_t)L.n != per * 4 * g.nz) {
-    L.wf_units[0] = -1;  // not eligible; not asked again
+    L.wf_tpu = -1;  // not eligible; not asked again
     return HPCG_B200_OK;
   }
   static const int lag = [] {
@@ -426,61 +426,42 @@ int ensure_wavefront(Level& L) {
     const int v = e && *e ? std::atoi(e) : 2;
     return v < 1 ? 1 : v > 16 ? 16 : v;
   }();
-  const int H = g.nz / 2, tpu = (int)(per / kBulkRows);
-  std::vector<WaveUnit> tab[2];
   for (int dir = 0; dir < 2; ++dir) {
-    const int P = dir == 0 ? kColours : kColours - 1;  // the backward sweep skips the turn colour
-    std::vector<int> idx((size_t)P * H, -1);
-    for (int tau = 0; tau < H + lag * (P - 1); ++tau)
-      for (int j = 0; j < P; ++j) {
-        const int h = tau - lag * j;
-        if (h < 0 || h >= H) continue;
-        idx[(size_t)j * H + h] = (int)tab[dir].size();
-        WaveUnit u;
-        const int pos = dir == 0 ? j : kColours - 2 - j;  // sweep position of phase j
-        u.row0 = g.start[pos] + (int)(h * per);
-        u.dep[0] = u.dep[1] = u.dep[2] = -1;
-        u.dot = dir == 1 || j == P - 1;  // the phases that write each colour's final value
-        u.pad[0] = u.pad[1] = u.pad[2] = 0;
-        tab[dir].push_back(u);
-      }
-    for (int j = 1; j < P; ++j)
-      for (int h = 0; h < H; ++h) {
-        WaveUnit& u = tab[dir][idx[(size_t)j * H + h]];
-        int d = 0;
-        for (int hh = h - 1; hh <= h + 1; ++hh)
-          if (hh >= 0 && hh < H) u.dep[d++] = idx[(size_t)(j - 1) * H + hh];
-      }
+    WaveGeom& w = L.wf_geom[dir];
+    w.H = g.nz / 2;
+    w.P = dir == 0 ? kColours : kColours - 1;  // the backward sweep skips the turn colour
+    w.lag = lag;
+    w.tpu = (int)(per / kBulkRows);
+    w.per = (int)per;
+    // the phases that write each colour's final value add r'x: the forward
+    // sweep's last, every phase of the backward sweep
+    w.dot_from = dir == 0 ? w.P - 1 : 0;
+    w.self_dep = -1;
+    for (int j = 0; j < kColours; ++j) w.start[j] = j < w.P ? g.start[dir == 0 ? j : kColours - 2 - j] : 0;
   }
-  for (int dir = 0; dir < 2; ++dir) {
-    const size_t bytes = sizeof(WaveUnit) * tab[dir].size();
-    HB_CK(cudaMalloc(&L.wf_unit[dir], bytes));
-    HB_CK(cudaMemcpy(L.wf_unit[dir], tab[dir].data(), bytes, cudaMemcpyHostToDevice));
-    L.wf_units[dir] = (int)tab[dir].size();
-  }
-  HB_CK(cudaMalloc(&L.wf_done, sizeof(unsigned) * L.wf_units[0]));
-  L.wf_tpu = tpu;
+  HB_CK(cudaMalloc(&L.wf_done, sizeof(unsigned) * wave_units(L.wf_geom[0])));
+  L.wf_tpu = (int)(per / kBulkRows);
   return HPCG_B200_OK;
 }
 
-// One whole sweep of level L (dir 0 forward, 1 backward; x entering nonzero)
-// as one cooperative launch of k_gs_wave. dot: as gs_colour's, the block
-// partials of the sweep's final-value rows (the caller's zeroed slots).
-// false: not launched (no tables, no tensor maps, or the launch was refused):
-// the caller runs the phases one by one.
+// One sweep of level L as one cooperative launch of k_gs_wave over geometry w
+// (x entering nonzero). dot: as gs_colour's, the block partials of the sweep's
+// final-value rows (the caller's zeroed slots). false: not launched (no
+// tensor maps, or the launch was refused): the caller runs the phases one by
+// one.
 template <int PW>
-bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, int dir, double* dot,
-                   const WaveUnit* table = nullptr, int table_units = 0,
+bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, const WaveGeom& w, double* dot,
                    unsigned long long limit_ns = kBulkWaitNs) {
   const BulkMaps* m = bulk_maps(L);
   if (!m) return false;
   auto k = k_gs_wave<double, PW>;
-  using Shape = GsShape<double, PW>;
+  using Shape = WaveShape<double, PW>;
   constexpr int smem = Shape::smem;
+  constexpr int threads = wave_threads<double, PW>();
   static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
   bulk_attr(k, smem, c->device, &attr_set);
-  const int nunits = table ? table_units : L.wf_units[dir];
-  const int64_t ntiles = (int64_t)nunits * L.wf_tpu;
+  const int nunits = wave_units(w);
+  const int64_t ntiles = (int64_t)w.H * w.P * w.tpu;  // the non-empty units' tiles
   int g = (int)std::min<int64_t>(ntiles, (int64_t)c->sms);
   if (dot && g > kDotStride) g = kDotStride;
   if (cudaMemsetAsync(L.wf_done, 0, sizeof(unsigned) * nunits, c->stream) != cudaSuccess) {
@@ -490,7 +471,7 @@ bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, int
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof(cfg));
   cfg.gridDim = dim3(g);
-  cfg.blockDim = dim3(Shape::threads);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
@@ -498,8 +479,7 @@ bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, int
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, (const double*)L.val, cols_of<double>(L), L.pitch, rhs, x,
-                                           table ? table : (const WaveUnit*)L.wf_unit[dir], nunits, L.wf_tpu,
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, (const double*)L.val, cols_of<double>(L), L.pitch, rhs, x, w,
                                            L.wf_done, dot, c->fault, m->val, m->col, (const unsigned char*)L.colp,
                                            sink_of(L), limit_ns);
   if (e != cudaSuccess) {
@@ -510,12 +490,13 @@ bool wave_launch_p(Context* c, const Level& L, const double* rhs, double* x, int
   return true;
 }
 
-bool wave_launch(Context* c, const Level& L, const double* rhs, double* x, int dir, double* dot) {
+bool wave_launch(Context* c, const Level& L, const double* rhs, double* x, const WaveGeom& w, double* dot,
+                 unsigned long long limit_ns = kBulkWaitNs) {
   if (L.wf_tpu <= 0) return false;
-  if (L.pack == kPackDiag) return wave_launch_p<kPackDiag>(c, L, rhs, x, dir, dot);
-  if (L.pack == 1) return wave_launch_p<1>(c, L, rhs, x, dir, dot);
-  if (L.pack == 2) return wave_launch_p<2>(c, L, rhs, x, dir, dot);
-  return wave_launch_p<0>(c, L, rhs, x, dir, dot);
+  if (L.pack == kPackDiag) return wave_launch_p<kPackDiag>(c, L, rhs, x, w, dot, limit_ns);
+  if (L.pack == 1) return wave_launch_p<1>(c, L, rhs, x, w, dot, limit_ns);
+  if (L.pack == 2) return wave_launch_p<2>(c, L, rhs, x, w, dot, limit_ns);
+  return wave_launch_p<0>(c, L, rhs, x, w, dot, limit_ns);
 }
 
 // A whole sweep as one wavefront launch, timed as kProfGsSweep on level 0.
@@ -531,11 +512,12 @@ bool wave_sweep(Context* c, const Level& L, const T* val, const TR* rhs, T* x, i
     const int kind = top ? kProfGsSweep : -1;
     cudaEvent_t ev0 = nullptr;
     if ((*status = prof_begin(c, kind, &ev0)) != HPCG_B200_OK) return true;
-    if (!wave_launch(c, L, rhs, x, dir, dot)) {
+    const WaveGeom& w = L.wf_geom[dir];
+    if (!wave_launch(c, L, rhs, x, w, dot)) {
       if (ev0) c->ev_pool.push_back(ev0);  // recorded around no launch: back to the pool, not timed
       return false;
     }
-    const int rows = L.wf_units[dir] * L.wf_tpu * kBulkRows;
+    const int64_t rows = (int64_t)w.H * w.P * w.per;
     *status = prof_end(c, kind, ev0, rows);
     return true;
   }
@@ -1728,34 +1710,17 @@ int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds) {
   Level& L = p->lev[0];
   HB_TRY(ensure_wavefront(L));
   if (L.wf_tpu <= 0) return HPCG_B200_ERR_UNSUPPORTED;
-  // one unit that waits for itself: its counter cannot fill before its own
-  // tiles are released, so the producer's dependency wait runs out
-  WaveUnit u;
-  u.row0 = L.g.start[0];
-  u.dep[0] = 0;
-  u.dep[1] = u.dep[2] = -1;
-  u.dot = 0;
-  u.pad[0] = u.pad[1] = u.pad[2] = 0;
-  WaveUnit* d = nullptr;
-  HB_CK(cudaMalloc(&d, sizeof(WaveUnit)));
-  int st = HPCG_B200_OK;
-  if (cudaMemcpy(d, &u, sizeof(u), cudaMemcpyHostToDevice) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
-  // x: scratch (Ap); the unit's tiles are never released, so nothing is written
+  // one unit (one phase, one z pair) that waits for itself: its counter cannot
+  // fill before its own tiles are released, so every block's wait runs out
+  WaveGeom w = L.wf_geom[0];
+  w.H = 1;
+  w.P = 1;
+  w.dot_from = 1;
+  w.self_dep = 0;
+  // x: scratch (Ap), which the tiles released after the wait gave up rewrite
   const unsigned long long lim = (unsigned long long)(limit_seconds * 1e9);
-  bool launched = false;
-  if (st == HPCG_B200_OK) {
-    if (L.pack == kPackDiag)
-      launched = wave_launch_p<kPackDiag>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
-    else if (L.pack == 1)
-      launched = wave_launch_p<1>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
-    else if (L.pack == 2)
-      launched = wave_launch_p<2>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
-    else
-      launched = wave_launch_p<0>(c, L, p->zprev, p->Ap, 0, nullptr, d, 1, lim);
-    st = launched ? stream_sync(c) : HPCG_B200_ERR_UNSUPPORTED;
-  }
-  cudaFree(d);
-  return st;
+  if (!wave_launch(c, L, p->zprev, p->Ap, w, nullptr, lim)) return HPCG_B200_ERR_UNSUPPORTED;
+  return stream_sync(c);
 }
 
 int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on) {
