@@ -34,6 +34,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "HPCG GFLOP/s & HBM GB/s at 512^3; FP32-MG vs FP64 time to 1e-9 residual"
+# a level's column index as the kernels read it (hpcg_b200_level_packed): the
+# "column_form" fields of the JSON line hold these codes
+COLUMN_FORMS = {0: "32-bit columns", 1: "8-bit offsets", 2: "16-bit offsets",
+                3: "diagonal form: 27 bases and 27 x 128 sink bits per 128-row tile"}
 
 
 def parse():
@@ -429,7 +433,7 @@ def mixed_vs_fp64(P, b, lib_stream, tol, max_iter=2000, profile_iters=20):
                 "first_gbs": round(first_gbs, 1) if first_gbs else None,
                 "bytes_per_row": {"full": round(metrics.gs_phase_bytes(1, 8, vb=4, pack=pack), 3),
                                   "first_sweep": 130},
-                "column_offset_bytes": pack}}
+                "column_form": pack}}
 
 
 def gpu_launches_per_set(iters, nlevels=4, rtz_pass=False, wave=(0, 0, 0, 0)):
@@ -607,7 +611,7 @@ def b200_arm(args, rank, world, local_rank):
         b64 = metrics.iteration_bytes(n, n, n, vb=8, pack=packs, rtz_fused=rtz_fused, wave=waves)
         b32 = metrics.iteration_bytes(n, n, n, vb=4, pack=packs)
         mixed["byte_floor_ratio"] = round(b32 / b64, 4)
-        mixed["bytes_per_iter"] = {"fp64": b64, "fp32_vcycle": b32, "column_offset_bytes": list(packs)}
+        mixed["bytes_per_iter"] = {"fp64": b64, "fp32_vcycle": b32, "column_form": list(packs)}
 
     adjoint = None
     if not args.no_adjoint:
@@ -618,6 +622,17 @@ def b200_arm(args, rank, world, local_rank):
     batch = None
     if not args.no_batch:
         batch = batched(dev)
+    # the copy side's ceiling on level 0's tiles: the FP64 phases' pipeline over
+    # the whole matrix with consumers that hand each stage straight back (the
+    # fastest of three launches; outside every timed region)
+    probe = None
+    try:
+        pms, pbytes = min(P.stream_probe(0) for _ in range(3))
+        probe = {"gbs": round(pbytes / (pms * 1e-3) / 1e9, 1), "ms": round(pms, 4), "bytes": pbytes,
+                 "note": "hpcg_b200_stream_probe: level 0's values and column index, every 128-row tile "
+                         "through the Gauss-Seidel phases' copy pipeline, no consumer work"}
+    except B.HpcgError as ex:
+        probe = {"gbs": None, "error": str(ex)[:200]}
 
     line = None
     tuning = [P.level_config(l) for l in range(4)]
@@ -631,7 +646,7 @@ def b200_arm(args, rank, world, local_rank):
         gs_bytes = metrics.gs_phase_bytes(gs_rows, nrow, pack=gs_pack)
         achieved = gs_bytes / (gs_ms * 1e-3) / 1e9 if gs_ms > 0 else None
         kernel = (f"k_gs_bulk<double,double,false> (level 0, configuration {gs_cfg}"
-                  f"{f', packed columns, {8 * gs_pack}-bit offsets' if gs_pack else ''})" if gs_cfg == 10 else
+                  f"{', packed columns, ' + COLUMN_FORMS[gs_pack] if gs_pack else ''})" if gs_cfg == 10 else
                   f"k_gs_phase<double,double,false> (level 0, configuration {gs_cfg})")
         tr = committed_traffic()
         traffic = None
@@ -671,7 +686,7 @@ def b200_arm(args, rank, world, local_rank):
             "iteration": {"bytes": bytes_iter, "gbs": round(hbm_gbs, 1), "frac": round(hbm_gbs / peak, 4),
                           "model": "metrics.iteration_bytes: every kernel of a CG iteration streaming its data "
                                    "once, each level's column index as stored",
-                          "column_offset_bytes": list(packs),
+                          "column_form": list(packs),
                           "compulsory_4byte_index_bytes": metrics.compulsory_bytes(n, n, n)},
             "packed_index_bytes": [P.level_packed(l) for l in range(4)],
             "final_scaled_residual": res[1] / res[2] if res and res[2] else None,
@@ -683,7 +698,7 @@ def b200_arm(args, rank, world, local_rank):
                          "bytes_per_launch": gs_bytes / max(gs_launch, 1)},
             "spmv": {"launches": sp_launch, "avg_ms": round(sp_ms / max(sp_launch, 1), 4),
                      "gbs": round(metrics.spmv_bytes(sp_rows, pack=mv_pack) / (sp_ms * 1e-3) / 1e9, 1)
-                     if sp_ms else None, "column_offset_bytes": mv_pack},
+                     if sp_ms else None, "column_form": mv_pack},
             "first_sweep_gbs": round(metrics.first_sweep_bytes(gf_rows) / (gf_ms * 1e-3) / 1e9, 1) if gf_ms else None,
             "kernel_ms_per_iter": {
                 "gs_full_l0": round(phase_ms / (args.iters * args.steps), 3),
@@ -698,6 +713,8 @@ def b200_arm(args, rank, world, local_rank):
         }
         if wave_line:
             line["wavefront_sweeps"] = wave_line
+        if probe:
+            line["stream_probe"] = probe
         if e2e:
             line["e2e"] = e2e
         if mixed:

@@ -40,6 +40,7 @@ EXPORTS = (
     "hpcg_b200_level_config", "hpcg_b200_batch_create", "hpcg_b200_batch_problem", "hpcg_b200_batch_cg_mixed", "hpcg_b200_batch_free",
     "hpcg_b200_batch_form", "hpcg_b200_grid_wait_selftest", "hpcg_b200_level_first_config",
     "hpcg_b200_set_host_reuse", "hpcg_b200_level_wavefront", "hpcg_b200_wave_wait_selftest",
+    "hpcg_b200_stream_probe",
     "hpcg_b200_process_grid", "hpcg_b200_generate_rank", "hpcg_b200_halo_plan", "hpcg_b200_rank_info",
     "hpcg_b200_comm_unique_id", "hpcg_b200_comm_nccl", "hpcg_b200_comm_local", "hpcg_b200_comm_free",
     "hpcg_b200_shard_spmv", "hpcg_b200_shard_symgs", "hpcg_b200_shard_mg", "hpcg_b200_shard_dot", "hpcg_b200_shard_cg",
@@ -113,6 +114,7 @@ def lib():
         l.hpcg_b200_set_host_reuse.argtypes = [vp, i]
         l.hpcg_b200_level_wavefront.argtypes = [vp, i, C.POINTER(i)]
         l.hpcg_b200_wave_wait_selftest.argtypes = [vp, d]
+        l.hpcg_b200_stream_probe.argtypes = [vp, i, C.POINTER(C.c_float), C.POINTER(d)]
         l.hpcg_b200_process_grid.argtypes = [i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         l.hpcg_b200_generate_rank.argtypes = [i, i, i, i, i, i, i, i, i, C.POINTER(vp)]
         l.hpcg_b200_halo_plan.argtypes = [i, i, i, i, i, i, i, C.POINTER(i), vp, vp, vp, vp]
@@ -383,6 +385,14 @@ class Problem:
     def wave_wait_selftest(self, limit_seconds):
         """hpcg_b200_wave_wait_selftest: the status code (not raised)."""
         return int(lib().hpcg_b200_wave_wait_selftest(self._h, float(limit_seconds)))
+
+    def stream_probe(self, level=0):
+        """hpcg_b200_stream_probe: (milliseconds, bytes) of one launch of the
+        FP64 phases' copy pipeline over the level's whole matrix with consumers
+        that hand each stage straight back."""
+        ms, nb = C.c_float(0.0), C.c_double(0.0)
+        _check(lib().hpcg_b200_stream_probe(self._h, level, C.byref(ms), C.byref(nb)), "hpcg_b200_stream_probe")
+        return float(ms.value), float(nb.value)
 
     def level_config_string(self):
         """HPCG_B200_LEVEL_CONFIG that repeats this problem's tuned choices (the

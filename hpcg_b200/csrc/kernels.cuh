@@ -319,33 +319,77 @@ __global__ void __launch_bounds__(GsShape<T, PW>::threads, 1)
   const int a0 = r0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, GsShape<T, PW>>(
+  bulk_tiles<T, GsShape<T, PW>, bulk_early<T>()>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
-      [&](int64_t q0, const T* sv, const int* sc, int t) {
+      [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t q = q0 + t;
-        if (q < r0 || q >= r1) return;
-        T sum = (T)rhs[q];
-        T xd = (T)0;
+        if constexpr (sizeof...(release) > 0) {
+          // the row's values and columns into registers, the stage back to the producer
+          T a[kSlots];
+          int c[kSlots];
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) {
-          if (mask & (1u << k)) {
-            const T a = sv[k * kBulkRows + t];
-            const T xv = __ldg(x + stage_col<PW>(sc, k, t, sink));
-            sum -= a * xv;
-            if (k == kDiagSlot) xd = xv;
+          for (int k = 0; k < kSlots; ++k) {
+            if (mask & (1u << k)) {
+              a[k] = sv[k * kBulkRows + t];
+              c[k] = stage_col<PW>(sc, k, t, sink);
+            }
           }
+          const T d = sv[kDiagSlot * kBulkRows + t];
+          (release(), ...);
+          if (q < r0 || q >= r1) return;
+          T sum = (T)rhs[q];
+          T xd = (T)0;
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            if (mask & (1u << k)) {
+              const T xv = __ldg(x + c[k]);
+              sum -= a[k] * xv;
+              if (k == kDiagSlot) xd = xv;
+            }
+          }
+          if (!FIRST) sum += xd * d;
+          const T out = sum / d;
+          x[q] = out;
+          if (DOT) acc += (double)rhs[q] * (double)out;
+        } else {
+          if (q < r0 || q >= r1) return;
+          T sum = (T)rhs[q];
+          T xd = (T)0;
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            if (mask & (1u << k)) {
+              const T a = sv[k * kBulkRows + t];
+              const T xv = __ldg(x + stage_col<PW>(sc, k, t, sink));
+              sum -= a * xv;
+              if (k == kDiagSlot) xd = xv;
+            }
+          }
+          const T d = sv[kDiagSlot * kBulkRows + t];
+          if (!FIRST) sum += xd * d;
+          const T out = sum / d;
+          x[q] = out;
+          if (DOT) acc += (double)rhs[q] * (double)out;
         }
-        const T d = sv[kDiagSlot * kBulkRows + t];
-        if (!FIRST) sum += xd * d;
-        const T out = sum / d;
-        x[q] = out;
-        if (DOT) acc += (double)rhs[q] * (double)out;
       },
       fault, tm_val, tm_col, colp);
   if (DOT) {
     const double s = block_sum(acc);
     if (threadIdx.x == 0) dot[blockIdx.x] = s;
   }
+}
+
+// The FP64 Gauss-Seidel phase's copy pipeline (GsShape, the level's column
+// form PW) over every tile of a level's matrix, each stage handed straight back
+// by its consumers: the rate at which the phases' tiles stream when no
+// consumer holds a stage (hpcg_b200_stream_probe). Reads the matrix only.
+template <int PW>
+__global__ void __launch_bounds__(GsShape<double, PW>::threads, 1)
+    k_stream_probe(const double* __restrict__ val, const int* __restrict__ col, int64_t pitch, int ntiles,
+                   unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
+                   const __grid_constant__ CUtensorMap tm_col, const unsigned char* __restrict__ colp) {
+  bulk_tiles<double, GsShape<double, PW>, true>(
+      val, col, pitch, ntiles, [](int tile) { return (int64_t)tile * kBulkRows; },
+      [](int64_t, const double*, const int*, int, auto&& release) { release(); }, fault, tm_val, tm_col, colp);
 }
 
 // The FP32 V-cycle's matrix: values rounded to FP32 and the columns, moved from
@@ -518,13 +562,36 @@ __global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
   static_assert(ORDER == 0 || ORDER == 2, "storage or slab order");
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, SpmvShape<T, PW>>(
+  bulk_tiles<T, SpmvShape<T, PW>, bulk_early<T>()>(
       val, col, pitch, ntiles,
       [&](int tile) {
         return ORDER == 2 ? slab_row(g, (int64_t)tile * kBulkRows) : (int64_t)tile * kBulkRows;
       },
-      [&](int64_t q0, const T* sv, const int* sc, int t) {
+      [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t q = q0 + t;
+        if constexpr (sizeof...(release) > 0) {
+          // the row's values and columns into registers, the stage back to the producer
+          T a[kSlots];
+          int c[kSlots];
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            a[k] = sv[k * kBulkRows + t];
+            c[k] = stage_col<PW>(sc, k, t, sink);
+          }
+          (release(), ...);
+          if (q >= n) return;
+          T sum = (T)0;
+          T xq = (T)0;
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            const T xv = __ldg(x + c[k]);
+            sum += a[k] * xv;
+            if (k == kDiagSlot) xq = xv;
+          }
+          y[q] = sum;
+          if (DOT) acc += (double)xq * (double)sum;
+          return;
+        }
         if (q >= n) return;
         T sum = (T)0;
         T xq = (T)0;
@@ -603,10 +670,27 @@ __global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
   const int r1 = f0 + nc;
   const int a0 = f0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<T, SpmvShape<T, PW>>(
+  bulk_tiles<T, SpmvShape<T, PW>, bulk_early<T>()>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
-      [&](int64_t q0, const T* sv, const int* sc, int t) {
+      [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t f = q0 + t;
+        if constexpr (sizeof...(release) > 0) {
+          // the row's values and columns into registers, the stage back to the producer
+          T a[kSlots];
+          int c[kSlots];
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) {
+            a[k] = sv[k * kBulkRows + t];
+            c[k] = stage_col<PW>(sc, k, t, sink);
+          }
+          (release(), ...);
+          if (f < f0 || f >= r1) return;
+          T sum = (T)0;
+#pragma unroll
+          for (int k = 0; k < kSlots; ++k) sum += a[k] * __ldg(xf + c[k]);
+          rc[tq[f - f0]] = rf[f] - sum;
+          return;
+        }
         if (f < f0 || f >= r1) return;
         T sum = (T)0;
 #pragma unroll

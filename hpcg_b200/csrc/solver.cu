@@ -499,6 +499,34 @@ bool wave_launch(Context* c, const Level& L, const double* rhs, double* x, const
   return wave_launch_p<0>(c, L, rhs, x, w, dot, limit_ns);
 }
 
+// One launch of k_stream_probe over every tile of L (hpcg_b200_stream_probe).
+template <int PW>
+int stream_probe_p(Context* c, const Level& L, float* ms, double* bytes) {
+  const BulkMaps* m = bulk_maps(L);
+  if (!m) return HPCG_B200_ERR_UNSUPPORTED;
+  auto k = k_stream_probe<PW>;
+  using Shape = GsShape<double, PW>;
+  static std::atomic<uint64_t> attr_set{0};
+  bulk_attr(k, Shape::smem, c->device, &attr_set);
+  const int ntiles = (int)(((int64_t)L.n + kBulkRows - 1) / kBulkRows);
+  const int g = std::min(ntiles, c->sms);
+  cudaEvent_t e0, e1;
+  HB_CK(cudaEventCreate(&e0));
+  HB_CK(cudaEventCreate(&e1));
+  HB_CK(cudaEventRecord(e0, c->stream));
+  k<<<g, Shape::threads, Shape::smem, c->stream>>>(L.val, L.col, L.pitch, ntiles, c->fault, m->val, m->col,
+                                                     (const unsigned char*)L.colp);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+  int st = e == cudaSuccess ? stream_sync(c) : HPCG_B200_ERR_CUDA;
+  if (e != cudaSuccess) set_error("k_stream_probe", e);
+  if (st == HPCG_B200_OK && cudaEventElapsedTime(ms, e0, e1) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *bytes = (double)ntiles * (Shape::value_bytes + Shape::col_bytes);
+  return st;
+}
+
 // A whole sweep as one wavefront launch, timed as kProfGsSweep on level 0.
 // false: not launched (see wave_launch).
 template <typename T, typename TR>
@@ -1721,6 +1749,18 @@ int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds) {
   const unsigned long long lim = (unsigned long long)(limit_seconds * 1e9);
   if (!wave_launch(c, L, p->zprev, p->Ap, w, nullptr, lim)) return HPCG_B200_ERR_UNSUPPORTED;
   return stream_sync(c);
+}
+
+int hpcg_b200_stream_probe(hpcg_b200_problem* p, int level, float* ms, double* bytes) {
+  if (!valid(p)) return HPCG_B200_ERR_HANDLE;
+  if (!ms || !bytes || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
+  HB_CK(cudaSetDevice(p->device));
+  Context* c = p->ctx;
+  const Level& L = p->lev[level];
+  if (L.pack == kPackDiag) return stream_probe_p<kPackDiag>(c, L, ms, bytes);
+  if (L.pack == 1) return stream_probe_p<1>(c, L, ms, bytes);
+  if (L.pack == 2) return stream_probe_p<2>(c, L, ms, bytes);
+  return stream_probe_p<0>(c, L, ms, bytes);
 }
 
 int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on) {

@@ -341,6 +341,17 @@ int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on);
  * tables. Writes only the problem's scratch vector Ap. */
 int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds);
 
+/* Measurement aid, with no counterpart in the reference: one launch of the
+ * FP64 Gauss-Seidel phases' copy pipeline (the same stages, tensor copies and
+ * column records) over every 128-row tile of the level's matrix, with
+ * consumers that hand each stage straight back. *ms: its device time; *bytes:
+ * the bytes it streamed (values and column index of every tile). Their ratio is
+ * the rate at which the phases' tiles can stream when nothing holds a stage,
+ * the ceiling of the copy side of the pipeline on this level's data. Reads
+ * the matrix only. HPCG_B200_ERR_UNSUPPORTED where the level has no tensor
+ * maps. */
+int hpcg_b200_stream_probe(hpcg_b200_problem* p, int level, float* ms, double* bytes);
+
 /* Check of the device-side bounded wait used by the bulk-copy Gauss-Seidel
  * phases (configuration 10): one thread waits `seconds` (0 < seconds <= 2) on
  * an mbarrier that nothing completes, gives up, records the fault and returns.

@@ -797,6 +797,35 @@ def test_bounded_wait_gives_up_and_context_survives(oracle, binding, case16):
         binding._check(binding.lib().hpcg_b200_wait_selftest(0, 5.0), "wait_selftest")
 
 
+@pytest.mark.parametrize("packed", ["", "0"])
+def test_stream_probe_reads_the_matrix_only(binding, monkeypatch, packed):
+    """hpcg_b200_stream_probe streams every 128-row tile of a level (values
+    and column index, in the level's column form) through the phases' copy
+    pipeline and changes nothing: the bytes it reports are the tiles' bytes,
+    and a V-cycle after it gives the same bits as before."""
+    if packed:
+        monkeypatch.setenv("HPCG_B200_PACKED", packed)
+    D = binding.Problem.generate(64, 32, 48)
+    try:
+        r = np.random.default_rng(5).standard_normal(D.nrow)
+        z0 = np.zeros_like(r)
+        D.ComputeMG(r, z0)
+        for level in range(4):
+            n, pitch, _ = D.level_info(level)
+            ms, nb = D.stream_probe(level)
+            form = D.level_pack_width(level)
+            rec = {0: 27 * 128 * 4, 1: 28 * 4 + 27 * 128, 2: 28 * 4 + 27 * 256, 3: 28 * 4 + 27 * 16}[form]
+            assert nb == -(-n // 128) * (27 * 128 * 8 + rec), (level, form, nb)
+            assert ms > 0.0
+        z1 = np.zeros_like(r)
+        D.ComputeMG(r, z1)
+        assert np.array_equal(z0, z1)
+    finally:
+        D.free()
+    with pytest.raises(binding.HpcgError):
+        binding._check(binding.lib().hpcg_b200_stream_probe(None, 0, None, None), "stream_probe")
+
+
 def test_stream_vcycle_follows_coarse_value_changes(oracle, binding):
     """The loops that launch kernel by kernel run the V-cycle below level 0 as
     one captured graph. After set_values on a coarse level (which rebuilds that
