@@ -510,19 +510,21 @@ int stream_probe_p(Context* c, const Level& L, float* ms, double* bytes) {
   bulk_attr(k, Shape::smem, c->device, &attr_set);
   const int ntiles = (int)(((int64_t)L.n + kBulkRows - 1) / kBulkRows);
   const int g = std::min(ntiles, c->sms);
-  cudaEvent_t e0, e1;
-  HB_CK(cudaEventCreate(&e0));
-  HB_CK(cudaEventCreate(&e1));
-  HB_CK(cudaEventRecord(e0, c->stream));
-  k<<<g, Shape::threads, Shape::smem, c->stream>>>(L.val, L.col, L.pitch, ntiles, c->fault, m->val, m->col,
-                                                     (const unsigned char*)L.colp);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
-  int st = e == cudaSuccess ? stream_sync(c) : HPCG_B200_ERR_CUDA;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaError_t e = cudaEventCreate(&ev[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[0], c->stream);
+  if (e == cudaSuccess) {
+    k<<<g, Shape::threads, Shape::smem, c->stream>>>(L.val, L.col, L.pitch, ntiles, c->fault, m->val, m->col,
+                                                       (const unsigned char*)L.colp);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ev[1], c->stream);
+  int st = e == cudaSuccess ? stream_sync(c) : status_of(e);
   if (e != cudaSuccess) set_error("k_stream_probe", e);
-  if (st == HPCG_B200_OK && cudaEventElapsedTime(ms, e0, e1) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (st == HPCG_B200_OK && cudaEventElapsedTime(ms, ev[0], ev[1]) != cudaSuccess) st = HPCG_B200_ERR_CUDA;
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
   *bytes = (double)ntiles * (Shape::value_bytes + Shape::col_bytes);
   return st;
 }
@@ -1754,7 +1756,7 @@ int hpcg_b200_wave_wait_selftest(hpcg_b200_problem* p, double limit_seconds) {
 int hpcg_b200_stream_probe(hpcg_b200_problem* p, int level, float* ms, double* bytes) {
   if (!valid(p)) return HPCG_B200_ERR_HANDLE;
   if (!ms || !bytes || level < 0 || level >= p->nlev) return HPCG_B200_ERR_ARG;
-  HB_CK(cudaSetDevice(p->device));
+  Setter dev(p->device);
   Context* c = p->ctx;
   const Level& L = p->lev[level];
   if (L.pack == kPackDiag) return stream_probe_p<kPackDiag>(c, L, ms, bytes);
