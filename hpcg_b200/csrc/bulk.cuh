@@ -87,18 +87,32 @@ static_assert(pack_rec(1) % 16 == 0 && pack_rec(2) % 16 == 0 && pack_rec(kPackDi
 // KB (33.9 KB with 16-bit offsets, 30.5 KB with 8-bit ones) and FP32 ones 27
 // KB (20.4 / 17 KB); all stages of a block share at most 227 KB of shared
 // memory (one block per SM).
-template <typename T, int G, int RING, int LANES = 1, int PW = 0>
+// TB: kBulkRows-row blocks per tile (1, or 2 for whole-tile copies: the
+// blocks of a tile are consecutive in the blocked layout and in the packed
+// records, so a tile of TB blocks is still one copy of values and one of
+// columns, with TB times the bytes per request). A consumer group then has
+// kBulkRows x LANES x TB threads; thread t works on block t / (kBulkRows x
+// LANES) of the tile.
+template <typename T, int G, int RING, int LANES = 1, int PW = 0, int TB = 1>
 struct BulkShape {
   static constexpr int groups = G;
   static constexpr int ring = RING;
   static constexpr int lanes = LANES;
   static constexpr int pack = PW;
   static constexpr bool packed = PW != 0;
-  static constexpr int group_threads = kBulkRows * LANES;
+  static constexpr int blocks = TB;
+  static constexpr int tile_rows = kBulkRows * TB;
+  static constexpr int block_threads = kBulkRows * LANES;
+  static constexpr int group_threads = block_threads * TB;
   static constexpr int stages = groups * ring;
   static constexpr int threads = 32 + groups * group_threads;  // producer warp + consumers
-  static constexpr int value_bytes = kSlots * kBulkRows * (int)sizeof(T);
-  static constexpr int col_bytes = PW == 0 ? kSlots * kBulkRows * (int)sizeof(int) : pack_rec(PW < 0 ? 2 : PW);
+  static constexpr int block_value_bytes = kSlots * kBulkRows * (int)sizeof(T);
+  static constexpr int block_col_bytes =
+      PW == 0 ? kSlots * kBulkRows * (int)sizeof(int) : pack_rec(PW < 0 ? 2 : PW);
+  static constexpr int value_bytes = block_value_bytes * TB;
+  static constexpr int col_bytes = block_col_bytes * TB;
+  static_assert(TB == 1 || (TB == 2 && bulk_whole_tile<T>() && PW >= 0 && LANES == 1),
+                "tiles of two blocks: whole-tile copies, one record form, one thread per row");
   static constexpr int tx_bytes = value_bytes + col_bytes;  // bytes landing in a stage per fill (PW >= 0)
   static constexpr int stage_bytes = (tx_bytes + 127) / 128 * 128;
   // stages + per stage two barriers and the tile's first row + slack to align
@@ -118,13 +132,21 @@ struct BulkShape {
 // to 10.0 ms per iteration (five: 10.2). With the diagonal form (28 KB FP64
 // stages), same box and run, a third SpMV group took the SpMV from 6.14 to
 // 5.52 ms and the restriction from 0.80 to 0.73 ms, while a fourth FP64 phase
-// group changed nothing. A shape whose stages do not fit (32-bit columns) gets
-// fewer groups.
+// group changed nothing. The FP32 phases take tiles of two blocks (256 rows,
+// 28.8 KB a stage) in two groups: their consumers release a stage early, so
+// the copy side bounds them, and two-block tiles halve its requests per byte.
+// Measured at 512^3 (FP32 level-0 phases of one V-cycle): 8.52-8.56 ms against
+// 9.08-9.14 ms for one-block tiles in four groups; three two-block groups
+// 9.43, two with rings of three 8.68, one with a ring of four 11.93. A shape
+// whose stages do not fit (32-bit columns) gets fewer groups.
 #ifndef HB_GS64_GROUPS
 #define HB_GS64_GROUPS 3
 #endif
 #ifndef HB_GS32_GROUPS
-#define HB_GS32_GROUPS 4
+#define HB_GS32_GROUPS 2
+#endif
+#ifndef HB_SPMV32_GROUPS
+#define HB_SPMV32_GROUPS 4
 #endif
 #ifndef HB_SPMV_GROUPS
 #define HB_SPMV_GROUPS 3
@@ -134,6 +156,9 @@ struct BulkShape {
 #endif
 #ifndef HB_GS32_RING
 #define HB_GS32_RING HB_BULK_RING
+#endif
+#ifndef HB_GS32_TILE
+#define HB_GS32_TILE 2
 #endif
 // Whether the Gauss-Seidel phases, the SpMV and the restriction hand a stage
 // back once the row's values and columns are in registers (bulk_tiles_src's
@@ -157,9 +182,10 @@ __host__ __device__ constexpr bool bulk_early() {
 #ifndef HB_SPMV_RING
 #define HB_SPMV_RING 2
 #endif
-template <typename T, int PW>
+template <typename T, int PW, int TB = 1>
 __host__ __device__ constexpr int fit_groups(int want, int ring) {
-  while (want > 1 && BulkShape<T, 1, 2, 1, PW>::stage_bytes * ring * want + 24 * ring * want + 128 > 227 * 1024)
+  while (want > 1 && (BulkShape<T, 1, 2, 1, PW, TB>::stage_bytes * ring * want + 24 * ring * want + 128 > 227 * 1024 ||
+                      32 + want * kBulkRows * TB > 1024))
     --want;
   return want;
 }
@@ -167,11 +193,19 @@ template <typename T>
 __host__ __device__ constexpr int gs_ring() {
   return sizeof(T) == 8 ? HB_BULK_RING : HB_GS32_RING;
 }
+// blocks per tile of the Gauss-Seidel phases: FP32 with one record form (the
+// batched kernel's per-tile forms keep one block)
+template <typename T, int PW>
+__host__ __device__ constexpr int gs_blocks() {
+  return sizeof(T) == 4 && PW >= 0 ? HB_GS32_TILE : 1;
+}
 template <typename T, int PW = 0>
-using GsShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_GS64_GROUPS : HB_GS32_GROUPS, gs_ring<T>()),
-                          gs_ring<T>(), 1, PW>;
+using GsShape = BulkShape<T,
+                          fit_groups<T, PW, gs_blocks<T, PW>()>(sizeof(T) == 8 ? HB_GS64_GROUPS : HB_GS32_GROUPS,
+                                                                gs_ring<T>()),
+                          gs_ring<T>(), 1, PW, gs_blocks<T, PW>()>;
 template <typename T, int PW = 0>
-using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_GS32_GROUPS, sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING),
+using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_SPMV32_GROUPS, sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING),
                             sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING, 1, PW>;
 
 // Column of slot k of row t of a tile in a stage (sc: the stage's column area)
@@ -370,7 +404,7 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
       if constexpr (Shape::packed) {
         if (lane == 1) bulk_g2s(sc, ts.rec, rec_bytes, &full[s], policy);
       } else if constexpr (bulk_whole_tile<T>()) {
-        if (lane == 1) bulk_g2s(sc, ts.cols, kSlots * kBulkRows * sizeof(int), &full[s], policy);
+        if (lane == 1) bulk_g2s(sc, ts.cols, Shape::col_bytes, &full[s], policy);
       } else {
         if (lane == 1) tma_load_2d(sc, tm_col, (int)ts.q0, 0, &full[s], policy);
       }
@@ -401,12 +435,16 @@ __device__ __forceinline__ void bulk_tiles_src(int ntiles, Src src, Skip skip, R
           record_fault(fault, 3);
           break;
         }
+        // the thread's block of the tile: its first row, values and columns
+        const int h = t / Shape::block_threads;
+        const int64_t q0 = first[s] + (int64_t)h * kBulkRows;
+        const T* sv = reinterpret_cast<const T*>(smem + s * SB + h * Shape::block_value_bytes);
+        const int* sc = reinterpret_cast<const int*>(smem + s * SB + VB + h * Shape::block_col_bytes);
+        const int tb = t - h * Shape::block_threads;
         if constexpr (EARLY) {
-          row(tile, first[s], reinterpret_cast<const T*>(smem + s * SB),
-              reinterpret_cast<const int*>(smem + s * SB + VB), t, [&] { mbar_arrive(&empty[s]); });
+          row(tile, q0, sv, sc, tb, [&] { mbar_arrive(&empty[s]); });
         } else {
-          row(tile, first[s], reinterpret_cast<const T*>(smem + s * SB),
-              reinterpret_cast<const int*>(smem + s * SB + VB), t);
+          row(tile, q0, sv, sc, tb);
           mbar_arrive(&empty[s]);
         }
       }

@@ -315,12 +315,13 @@ __global__ void __launch_bounds__(GsShape<T, PW>::threads, 1)
               T* x, int r0, int r1, uint32_t mask_arg, double* __restrict__ dot, unsigned* fault,
               const __grid_constant__ CUtensorMap tm_val, const __grid_constant__ CUtensorMap tm_col,
               const unsigned char* __restrict__ colp, int sink) {
+  constexpr int TROWS = GsShape<T, PW>::tile_rows;  // 128, or 256 for FP32 tiles of two blocks
   const uint32_t mask = CMASK >= 0 ? (uint32_t)CMASK : mask_arg;
-  const int a0 = r0 & ~(kBulkRows - 1);
-  const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
+  const int a0 = r0 & ~(TROWS - 1);
+  const int ntiles = (r1 - a0 + TROWS - 1) / TROWS;
   double acc = 0.0;
   bulk_tiles<T, GsShape<T, PW>, bulk_early<T>()>(
-      val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
+      val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * TROWS; },
       [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t q = q0 + t;
         if constexpr (sizeof...(release) > 0) {

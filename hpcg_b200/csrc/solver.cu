@@ -75,8 +75,8 @@ bool gs_bulk_launch_p(Context* c, const Level& L, const T* val, const TR* rhs, T
   }
   static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
   bulk_attr(k, smem, c->device, &attr_set);
-  const int a0 = r0 & ~(kBulkRows - 1);
-  const int64_t tiles = ((int64_t)r1 - a0 + kBulkRows - 1) / kBulkRows;
+  const int a0 = r0 & ~(Shape::tile_rows - 1);
+  const int64_t tiles = ((int64_t)r1 - a0 + Shape::tile_rows - 1) / Shape::tile_rows;
   int g = (int)std::min<int64_t>(tiles, (int64_t)c->sms);
   if (DOT && g > kDotStride) g = kDotStride;
   // programmatic dependent launch: the phase's producer streams its first
