@@ -107,7 +107,11 @@ __global__ void __launch_bounds__(kThreads) k_b_gs(const BGs* __restrict__ items
 // two copies; the tiles of problems that have converged are skipped on both
 // sides. Same arithmetic as k_b_gs. The problems' levels may pack their
 // columns with different offset widths: each tile's record states its own.
-using BatchShape = GsShape<float, -1>;
+// Four consumer groups of one-block tiles.
+#ifndef HB_BATCH_GROUPS
+#define HB_BATCH_GROUPS 4
+#endif
+using BatchShape = BulkShape<float, fit_groups<float, -1>(HB_BATCH_GROUPS, HB_BULK_RING), HB_BULK_RING, 1, -1>;
 __global__ void __launch_bounds__(BatchShape::threads, 1)
     k_b_gs_bulk(const BGs* __restrict__ items, const BTile* __restrict__ tiles, int ntiles,
                 const BScal* __restrict__ sc, unsigned* fault) {
