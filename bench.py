@@ -64,11 +64,40 @@ def parse():
                     help="with N > 1 GPUs: N independent problems instead of one decomposed problem")
     ap.add_argument("--decomposed", action="store_true",
                     help="run the decomposed (halo + allreduce) arm even on one GPU (a one-rank grid)")
+    ap.add_argument("--vcycle", type=int, default=0, metavar="N",
+                    help="one FP32 and one FP64 V-cycle of an N^3 problem, after two of each untimed, between "
+                         "cudaProfilerStart and cudaProfilerStop, every kernel launched on the stream (a launch "
+                         "list under ncu --profile-from-start off; the ncu summaries in profiles/)")
     ap.add_argument("--case", type=int, default=0, metavar="N",
                     help="the small profiling case instead of the bench: an N^3 problem, two V-cycles, a "
                          "3-iteration CG and a 3-iteration CG around the FP32 V-cycle, every kernel launched on "
                          "the stream (the ncu summaries in profiles/)")
     return ap.parse_args()
+
+
+def profile_vcycle(n):
+    """The V-cycle launch list's workload: an n^3 problem, two FP32 and two
+    FP64 V-cycles untimed (the first tunes), then one of each between
+    cudaProfilerStart and cudaProfilerStop, in colour order on the library's
+    vectors. Prints the tuned configurations."""
+    os.environ.setdefault("HPCG_B200_GRAPH", "0")
+    import torch
+    from hpcg_b200 import binding as B
+    P = B.Problem.generate(n, n, n, 4, 0)
+    r = torch.rand(n ** 3, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    x = torch.zeros_like(r)
+    for _ in range(2):
+        P.ComputeMG_f32(r, x)
+        P.ComputeMG(r, x)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    P.ComputeMG_f32(r, x)
+    P.ComputeMG(r, x)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"vcycle": n, "level_config": P.level_config_string()}))
+    P.free()
+    return 0
 
 
 def profile_case(n):
@@ -875,6 +904,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.case:
         return profile_case(args.case)
+    if args.vcycle:
+        return profile_vcycle(args.vcycle)
     if args.impl == "reference":
         return reference_arm(args, rank)
     if (world > 1 and not args.replicas) or args.decomposed:

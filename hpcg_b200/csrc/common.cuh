@@ -232,8 +232,8 @@ struct Level {
   // wavefront sweeps (wave.cuh): the geometry of the forward and the backward
   // sweep, tiles per unit (0: not set up yet, -1: the level does not cut into
   // whole-tile units), the per-unit counters of finished tiles (device); wf:
-  // the sweeps that do not start from x = 0 run as one launch each (tuned, or
-  // HPCG_B200_WAVE)
+  // the sweeps that do not start from x = 0 run as one launch each
+  // (HPCG_B200_WAVE or the level's configuration string; off by default)
   WaveGeom wf_geom[2] = {};
   int wf_tpu = 0;
   unsigned* wf_done = nullptr;

@@ -754,12 +754,18 @@ bool level_config_override(int l, int v[6], int* wf, int (&at64)[kColours], int 
   return true;
 }
 
-// HPCG_B200_WAVE: "0" never runs a sweep as one wavefront launch, "1" does so
-// wherever the level allows it; unset: the autotuner times both.
+// HPCG_B200_WAVE: unset or "0": no sweep runs as one wavefront launch; "1":
+// every sweep does where the level allows it; "tune": the autotuner times
+// both. Off unless asked for: at 512^3 the wavefront lost on every level in
+// whole CG sets (levels 0 and 1 by timing; on levels 2 and 3 the tuner, which
+// times launch by launch, chose it in some runs, and those CG sets ran at
+// 1622 against 1647-1649 GFLOP/s with the phases, configurations otherwise
+// pinned equal).
 int wave_force() {
   static const int f = [] {
     const char* e = std::getenv("HPCG_B200_WAVE");
-    return !e || !*e ? -1 : e[0] == '0' ? 0 : 1;
+    if (!e || !*e || e[0] == '0') return 0;
+    return std::strcmp(e, "tune") == 0 ? -1 : 1;
   }();
   return f;
 }

@@ -327,9 +327,11 @@ int hpcg_b200_level_first_config(const hpcg_b200_problem* p, int level, int* fp6
  * nonzero x (all but the pre-smoother's first) as one wavefront launch: a
  * cooperative kernel in which phase j of the sweep follows phase j - 1 two z
  * pairs behind, so the neighbours' x stays in L2 across the phases; the same
- * bits as the phases launched one by one. Chosen by the autotuner (both timed;
- * HPCG_B200_WAVE=0 or 1 forces it) where the level's sides are even and each
- * colour of a z pair fills whole 128-row tiles; *on receives 0 or 1. */
+ * bits as the phases launched one by one. Off unless HPCG_B200_WAVE=1 (every
+ * level that allows it) or HPCG_B200_WAVE=tune (the autotuner times both)
+ * asks for it, or the level's configuration string sets it; a level allows it
+ * where its sides are even and each colour of a z pair fills whole 128-row
+ * tiles. *on receives 0 or 1. */
 int hpcg_b200_level_wavefront(const hpcg_b200_problem* p, int level, int* on);
 
 /* Check of the wavefront sweep's bounded dependency wait: launches the sweep
