@@ -32,10 +32,11 @@ namespace hb {
 // the context's fault word (host-mapped; stream_sync turns it into
 // HPCG_B200_ERR_TIMEOUT) and stops; before its block exits the producer waits,
 // bounded again, for the copies it issued.
-// Tiles start on multiples of kBulkRows (r0 rounded down); rows outside
-// [r0, r1) are copied and not computed. The last tile ends at r1 rounded up to
-// kBulkRows, which is within the pitch (a multiple of 256 above n).
-constexpr int kBulkRows = 128;                             // rows per tile = threads per consumer group
+// Tiles start on multiples of their rows (kBulkRows, or 2 kBulkRows for the
+// FP32 phases' two-block tiles; r0 rounded down); rows outside [r0, r1) are
+// copied and not computed. The last tile ends at r1 rounded up to its rows,
+// at most 256, which is within the pitch (a multiple of 256 above n).
+constexpr int kBulkRows = 128;                             // rows per block (tile) = threads per consumer group
 constexpr unsigned long long kBulkWaitNs = 1000000000ull;  // 1 s per wait
 // How a tile reaches shared memory. FP32 (blocked copy with kRowBlock32 ==
 // kBulkRows): a tile is one block of the layout, its values one run of memory
@@ -84,9 +85,10 @@ static_assert(pack_rec(1) % 16 == 0 && pack_rec(2) % 16 == 0 && pack_rec(kPackDi
 // states (the batched kernel, whose tiles come from several levels): staged
 // for the largest one, each fill expecting its own record's bytes. Stages are rounded up to
 // 128 bytes (tensor copies land on 128-byte boundaries): FP64 stages are 41.5
-// KB (33.9 KB with 16-bit offsets, 30.5 KB with 8-bit ones) and FP32 ones 27
-// KB (20.4 / 17 KB); all stages of a block share at most 227 KB of shared
-// memory (one block per SM).
+// KB with 32-bit columns (33.9 / 30.5 / 28.3 KB with 16-bit offsets, 8-bit
+// offsets, the diagonal form) and FP32 one-block stages 27 KB (20.4 / 17 /
+// 14.4 KB); all stages of a block share at most 227 KB of shared memory (one
+// block per SM).
 // TB: kBulkRows-row blocks per tile (1, or 2 for whole-tile copies: the
 // blocks of a tile are consecutive in the blocked layout and in the packed
 // records, so a tile of TB blocks is still one copy of values and one of
