@@ -181,8 +181,18 @@ __host__ __device__ constexpr bool bulk_early() {
 #ifndef HB_SPMV_GATHER_FIRST
 #define HB_SPMV_GATHER_FIRST 0
 #endif
+// The FP64 SpMV: three groups of one stage whose consumers hand the stage
+// back once the row is in registers (85 KB of shared memory, the rest of the
+// SM's 256 KB left to L1 for the gathers); the restriction keeps rings of two
+// without early release.
 #ifndef HB_SPMV_RING
-#define HB_SPMV_RING 2
+#define HB_SPMV_RING 1
+#endif
+#ifndef HB_SPMV_EARLY64
+#define HB_SPMV_EARLY64 1
+#endif
+#ifndef HB_RESTRICT_RING
+#define HB_RESTRICT_RING 2
 #endif
 template <typename T, int PW, int TB = 1>
 __host__ __device__ constexpr int fit_groups(int want, int ring) {
@@ -209,6 +219,14 @@ using GsShape = BulkShape<T,
 template <typename T, int PW = 0>
 using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_SPMV32_GROUPS, sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING),
                             sizeof(T) == 8 ? HB_SPMV_RING : HB_BULK_RING, 1, PW>;
+template <typename T>
+__host__ __device__ constexpr bool spmv_early() {
+  return sizeof(T) == 4 ? HB_EARLY32 != 0 : HB_SPMV_EARLY64 != 0;
+}
+template <typename T, int PW = 0>
+using RestrictShape =
+    BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS : HB_SPMV32_GROUPS, sizeof(T) == 8 ? HB_RESTRICT_RING : HB_BULK_RING),
+              sizeof(T) == 8 ? HB_RESTRICT_RING : HB_BULK_RING, 1, PW>;
 
 // Column of slot k of row t of a tile in a stage (sc: the stage's column area)
 // for the column form PW of BulkShape.

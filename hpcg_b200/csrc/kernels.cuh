@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
   static_assert(ORDER == 0 || ORDER == 2, "storage or slab order");
   const int ntiles = (n + kBulkRows - 1) / kBulkRows;
   double acc = 0.0;
-  bulk_tiles<T, SpmvShape<T, PW>, bulk_early<T>()>(
+  bulk_tiles<T, SpmvShape<T, PW>, spmv_early<T>()>(
       val, col, pitch, ntiles,
       [&](int tile) {
         return ORDER == 2 ? slab_row(g, (int64_t)tile * kBulkRows) : (int64_t)tile * kBulkRows;
@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(kThreads, cfg_minb(CFG)) k_restrict(const T* _
 // when the injected rows are one run f0 .. f0 + nc of fine rows (tf[t] = f0 + t,
 // checked on the host): the run is tiled like a phase. Same sums as k_restrict.
 template <typename T, int PW = 0>
-__global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
+__global__ void __launch_bounds__(RestrictShape<T, PW>::threads, 1)
     k_restrict_bulk(const T* __restrict__ val, const int* __restrict__ col, int64_t pitch, const T* __restrict__ rf,
                     const T* __restrict__ xf, const int* __restrict__ tq, T* __restrict__ rc, int f0, int nc,
                     unsigned* fault, const __grid_constant__ CUtensorMap tm_val,
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(SpmvShape<T, PW>::threads, 1)
   const int r1 = f0 + nc;
   const int a0 = f0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<T, SpmvShape<T, PW>, bulk_early<T>()>(
+  bulk_tiles<T, RestrictShape<T, PW>, bulk_early<T>()>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t f = q0 + t;

@@ -356,7 +356,7 @@ bool restrict_bulk_p(Context* c, const Level& L, const T* val, const T* rf, cons
     tc = &m->col;
   }
   auto k = k_restrict_bulk<T, PW>;
-  using Shape = SpmvShape<T, PW>;
+  using Shape = RestrictShape<T, PW>;
   constexpr int smem = Shape::smem;
   static std::atomic<uint64_t> attr_set{0};  // devices on which the shared-memory size is enabled
   bulk_attr(k, smem, c->device, &attr_set);
