@@ -194,6 +194,12 @@ __host__ __device__ constexpr bool bulk_early() {
 #ifndef HB_RESTRICT_RING
 #define HB_RESTRICT_RING 2
 #endif
+#ifndef HB_RESTRICT_EARLY64
+#define HB_RESTRICT_EARLY64 0
+#endif
+#ifndef HB_FIRST_EARLY64
+#define HB_FIRST_EARLY64 0
+#endif
 template <typename T, int PW, int TB = 1>
 __host__ __device__ constexpr int fit_groups(int want, int ring) {
   while (want > 1 && (BulkShape<T, 1, 2, 1, PW, TB>::stage_bytes * ring * want + 24 * ring * want + 128 > 227 * 1024 ||
@@ -222,6 +228,15 @@ using SpmvShape = BulkShape<T, fit_groups<T, PW>(sizeof(T) == 8 ? HB_SPMV_GROUPS
 template <typename T>
 __host__ __device__ constexpr bool spmv_early() {
   return sizeof(T) == 4 ? HB_EARLY32 != 0 : HB_SPMV_EARLY64 != 0;
+}
+template <typename T>
+__host__ __device__ constexpr bool restrict_early() {
+  return sizeof(T) == 4 ? HB_EARLY32 != 0 : HB_RESTRICT_EARLY64 != 0;
+}
+// the Gauss-Seidel phases: FIRST (x entering zero, masked slots) separately
+template <typename T, bool FIRST>
+__host__ __device__ constexpr bool gs_early() {
+  return bulk_early<T>() || (FIRST && sizeof(T) == 8 && HB_FIRST_EARLY64 != 0);
 }
 template <typename T, int PW = 0>
 using RestrictShape =

@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(GsShape<T, PW>::threads, 1)
   const int a0 = r0 & ~(TROWS - 1);
   const int ntiles = (r1 - a0 + TROWS - 1) / TROWS;
   double acc = 0.0;
-  bulk_tiles<T, GsShape<T, PW>, bulk_early<T>()>(
+  bulk_tiles<T, GsShape<T, PW>, gs_early<T, FIRST>()>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * TROWS; },
       [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t q = q0 + t;
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(RestrictShape<T, PW>::threads, 1)
   const int r1 = f0 + nc;
   const int a0 = f0 & ~(kBulkRows - 1);
   const int ntiles = (r1 - a0 + kBulkRows - 1) / kBulkRows;
-  bulk_tiles<T, RestrictShape<T, PW>, bulk_early<T>()>(
+  bulk_tiles<T, RestrictShape<T, PW>, restrict_early<T>()>(
       val, col, pitch, ntiles, [&](int tile) { return a0 + (int64_t)tile * kBulkRows; },
       [&](int64_t q0, const T* sv, const int* sc, int t, auto&&... release) {
         const int64_t f = q0 + t;
